@@ -1,0 +1,432 @@
+#!/usr/bin/env python
+"""Benchmark: sampler throughput (points x iterations / s) of the sub-cluster DPMM sampler.
+
+Workload (default): the large overlapping Gaussian configuration -- N = 10,000,000 points,
+D = 64, 100 true clusters, means ~ N(0, 5^2 I), covariances A A^T / D + 0.5 I, Dirichlet(2)
+weights, float32 data; NIW(kappa=1, m=0, nu=67, Psi=I), alpha = 10, 300 iterations.  Data are
+seeded synthetic draws of that generative model, generated on the device.
+
+A "step" is one sampler iteration (local_clusters_actions::group_step: parameter draws, label
+phase, sub-label + statistics phase, split and merge tests, relabels).  The sampler starts from
+initial_clusters = 100 and runs `--burnin` untimed iterations so that the timed iterations are at
+the configuration's steady state (about 100 clusters, split / merge tests active), then W warm-up
+iterations, then exactly K timed iterations bracketed by a barrier and device synchronisation,
+timed with CUDA events on the sampler's stream.  Inputs (2.56 GB) are larger than L2.
+
+--gpus N (under torchrun) runs N independent replicas, one per GPU, each on its own data set of
+the same shape (weak scaling; the path has no cross-GPU exchange in this form); value sums all
+ranks' points x iterations over the max elapsed time.
+
+--impl reference times the reference's per-point path on the host cores: the reference has no CPU
+implementation of these phases (every one dispatches to its CUDA back-end), so its FP64
+restatement (oracle/) runs in a pool of all host threads on a bounded sample per step.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "sampler points*iters/sec at N=1e7 D=64: mixed+learned vs plain FP32, NMI within 0.01"
+UNIT = "points*iters/s"
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d, "measured"
+    except Exception:
+        return dict(FALLBACK_PEAKS), "fallback"
+
+
+# ----------------------------------------------------------------------------- workload
+def c5_config(args):
+    return dict(N=args.n, D=args.d, K_true=args.k_true, alpha=10.0, nu=args.d + 3.0, kappa=1.0, iterations=300,
+                mean_sd=5.0, dirichlet=2.0)
+
+
+def generate_c5_torch(cfg, seed, device):
+    import torch
+    torch.manual_seed(seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    N, D, K = cfg["N"], cfg["D"], cfg["K_true"]
+    w = torch.distributions.Dirichlet(torch.full((K,), cfg["dirichlet"])).sample()
+    z = torch.multinomial(w.to(device), N, replacement=True, generator=g)
+    mus = torch.randn(K, D, device=device, generator=g) * cfg["mean_sd"]
+    x = torch.empty(N, D, device=device, dtype=torch.float32)
+    order = torch.argsort(z)
+    counts = torch.bincount(z, minlength=K).tolist()
+    start = 0
+    for k in range(K):
+        n = counts[k]
+        A = torch.randn(D, D, device=device, generator=g, dtype=torch.float64)
+        cov = A @ A.T / D + 0.5 * torch.eye(D, device=device, dtype=torch.float64)
+        L = torch.linalg.cholesky(cov).float()
+        e = torch.randn(n, D, device=device, generator=g)
+        x[order[start:start + n]] = e @ L.T + mus[k]
+        start += n
+    return x.contiguous(), z
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [v.strip() for v in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+def _cpu_sample_worker(payload):
+    import numpy as np
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+    x, mu, inv, logdet, w, u, mu_lr, inv_lr, ld_lr, lrw = payload
+    K = mu.shape[0]
+    t0 = time.perf_counter()
+    r = np.stack([O.gauss_loglik(x, mu[k], inv[k], logdet[k], w[k]) for k in range(K)], 1)
+    lab, _ = O.sample_labels(r, u)
+    sub, _, _ = O.gauss_sub_labels(x, lab, mu_lr, inv_lr, ld_lr, lrw, u.reshape(-1))
+    O.suff_stats(x, lab, sub, K)
+    return time.perf_counter() - t0
+
+
+def cpu_sample_payload(x_np, n, seed, K, D):
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    idx = rng.choice(x_np.shape[0], size=n, replace=False)
+    x = x_np[idx].astype(np.float64)
+    mu = rng.normal(size=(K, D)) * 5
+    inv = np.repeat(np.eye(D)[None], K, 0) * 0.8
+    logdet = np.full(K, -D * math.log(0.8))
+    w = rng.dirichlet(np.full(K, 2.0))
+    u = rng.random((n, 2))
+    u[u == 0] = 1.0
+    mu_lr = mu[:, None, :] + rng.normal(size=(K, 2, D))
+    inv_lr = np.repeat(inv[:, None], 2, 1)
+    ld_lr = np.repeat(logdet[:, None], 2, 1)
+    lrw = np.full((K, 2), 0.5)
+    return (x, mu, inv, logdet, w, u, mu_lr, inv_lr, ld_lr, lrw)
+
+
+def cpu_baseline(x_np, K, D, n=4000):
+    t = _cpu_sample_worker(cpu_sample_payload(x_np, n, 1, K, D))
+    return {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
+            "sample": f"{n} points x 1 iteration of the per-point phases (K={K}, D={D}) through the FP64 C "
+                      f"restatement (oracle/dpmm_oracle.c), 1 thread; {t:.1f} s"}
+
+
+# ----------------------------------------------------------------------------- reference arm
+def run_reference(args, rank, world):
+    import numpy as np
+    if rank != 0:
+        return 0
+    import multiprocessing as mp
+    cores = os.cpu_count() or 1
+    cfg = c5_config(args)
+    D, K = cfg["D"], cfg["K_true"]
+    per = args.ref_points_per_core
+    rng = np.random.default_rng(0)
+    x_np = (rng.normal(size=(per * cores, D)) * 5).astype(np.float32)
+    ctx = mp.get_context("spawn")
+    payloads = [cpu_sample_payload(x_np[i * per:(i + 1) * per], per, i, K, D) for i in range(cores)]
+    times = []
+    with ctx.Pool(cores) as pool:
+        for step in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            pool.map(_cpu_sample_worker, payloads)
+            dt = time.perf_counter() - t0
+            if step >= args.warmup:
+                times.append(dt)
+    n = per * cores
+    tot = sum(times)
+    value = n * len(times) / tot
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * tot / len(times), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "C5 Gaussian N=1e7 D=64 K=100 (bounded host sample per step)",
+                       "points_per_step": n, "K": K, "D": D},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": f"{n} points ({per} per process x {cores} processes) per step through "
+                                       "the label, sub-label and statistics phases of the reference's "
+                                       "per-point path, FP64 C restatement"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--burnin", type=int, default=20)
+    ap.add_argument("--n", type=int, default=10_000_000)
+    ap.add_argument("--d", type=int, default=64)
+    ap.add_argument("--k-true", type=int, default=100)
+    ap.add_argument("--mode", default="auto", choices=["auto", "fp32", "tc"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-points-per-core", type=int, default=600)
+    args = ap.parse_args()
+    assert args.warmup >= 0 and args.steps >= 1
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from dpmmsubclusters_gpu_b200 import capi
+    from dpmmsubclusters_gpu_b200.capi import check, lib
+    L = lib()
+    cfg = c5_config(args)
+    N, D = cfg["N"], cfg["D"]
+    x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[args.mode]
+
+    def make_run(iterations):
+        rd = capi.dpmm_run_desc()
+        rd.prior_type = capi.PRIOR_GAUSSIAN
+        rd.iterations = iterations
+        rd.initial_clusters = cfg["K_true"]
+        rd.burnout = 15
+        rd.alpha = cfg["alpha"]
+        rd.seed = 12345 + rank
+        rd.loglik_mode = mode
+        rd.rng_kind = capi.RNG_PHILOX
+        rd.k_max = 256
+        rd.device = local
+        m = np.zeros(D)
+        psi = np.eye(D)
+        rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
+        rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        return rd, (m, psi)
+
+    rd, keep = make_run(cfg["iterations"])
+    h = ctypes.c_void_p()
+    check(L.dpmm_sampler_create(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1, ctypes.byref(h)))
+    ctx = L.dpmm_sampler_context(h)
+    stream = torch.cuda.ExternalStream(L.dpmm_sampler_stream(h), device=f"cuda:{local}")
+    check(L.dpmm_sampler_step(h, args.burnin + args.warmup))
+    k_before = ctypes.c_int32()
+    check(L.dpmm_sampler_num_clusters(h, ctypes.byref(k_before)))
+
+    # ---- timed region
+    check(L.dpmm_phase_times(ctx, 1, None, None))
+    launches0 = L.dpmm_kernel_launch_count()
+    h2d0, d2h0 = ctypes.c_uint64(), ctypes.c_uint64()
+    L.dpmm_transfer_bytes(ctypes.byref(h2d0), ctypes.byref(d2h0))
+    ks = []
+    with ClockSampler(local) as clk:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            check(L.dpmm_sampler_step(h, 1))
+            kk = ctypes.c_int32()
+            L.dpmm_sampler_num_clusters(h, ctypes.byref(kk))
+            ks.append(kk.value)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    elapsed_ms = e0.elapsed_time(e1)
+    launches = L.dpmm_kernel_launch_count() - launches0
+    ph_ms = (ctypes.c_double * 8)()
+    ph_calls = (ctypes.c_int64 * 8)()
+    check(L.dpmm_phase_times(ctx, 0, ph_ms, ph_calls))
+    h2d1, d2h1 = ctypes.c_uint64(), ctypes.c_uint64()
+    L.dpmm_transfer_bytes(ctypes.byref(h2d1), ctypes.byref(d2h1))
+    if dist:
+        t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(t.item())
+
+    # quality of the state reached (NMI against the generating labels)
+    mi = ctypes.c_void_p()
+    check(L.dpmm_sampler_model_info(h, ctypes.byref(mi)))
+    lab = np.ctypeslib.as_array(L.dpmm_model_info_labels(mi), shape=(N,)).copy()
+    L.dpmm_model_info_free(mi)
+    check(L.dpmm_sampler_destroy(h))
+    zt = z.cpu().numpy()
+    nmi = _nmi(lab[::10], zt[::10])
+
+    value = world * N * args.steps / (elapsed_ms / 1e3)
+    pk, pk_src = peaks()
+    k_mean = float(np.mean(ks)) if ks else float(k_before.value)
+    label_ms = ph_ms[0] / max(1, ph_calls[0])
+    flops = 2.0 * N * k_mean * D * D
+    achieved = flops / (label_ms / 1e3) / 1e12 if label_ms > 0 else None
+    peak = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
+    roofline = {"kernel": "label phase (fused N x K contraction + softmax + alias draw)",
+                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "peak_source": f"bf16_tflops of {pk_src}",
+                "algorithmic": f"2*N*K*D^2 FLOP per launch, K mean {k_mean:.1f}"}
+    phases = ["labels", "sub_labels_stats", "stats", "split_hastings", "merge_hastings", "relabel", "params", "-"]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3" if mode != capi.LL_FP32 else "f32",
+            "data": "synthetic (seeded draws of the configuration's generative model, generated on device)",
+            "config": {"workload": "C5 Gaussian DPMM N=1e7 D=64 100 true clusters (means N(0,25I), "
+                                   "cov AA^T/D+0.5I, Dir(2) weights, f32); NIW k=1 m=0 nu=67 Psi=I; alpha=10",
+                       "N": N, "D": D, "initial_clusters": cfg["K_true"], "burnin_iterations": args.burnin,
+                       "clusters_in_timed_steps": ks, "loglik_mode": args.mode,
+                       "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
+                       "nmi_vs_generating_labels": nmi},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "phase_ms_per_step": {p: ph_ms[i] / args.steps for i, p in enumerate(phases) if ph_calls[i]},
+            "clocks": clk.summary()}
+    line["clocks"].pop("samples", None)
+    del x
+    torch.cuda.empty_cache()
+
+    if rank == 0 and not args.no_cpu:
+        import numpy as np2
+        rng = np2.random.default_rng(0)
+        xs = (rng.normal(size=(4000, D)) * 5).astype(np2.float32)
+        line["cpu_baseline"] = cpu_baseline(xs, cfg["K_true"], D)
+    if not args.no_e2e:
+        line["e2e"] = run_e2e(args, cfg, rank, local, world, dist, L, make_run)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_e2e(args, cfg, rank, local, world, dist, L, make_run):
+    """The same metric through the public whole-sampler call (dpmm_dp_parallel) from HOST buffers:
+    point upload, initialisation, burn-in + warm-up + timed iterations and the label download
+    are all inside the timed region (wall clock, max over ranks)."""
+    import numpy as np
+    import torch
+    from dpmmsubclusters_gpu_b200.capi import check
+    x, _ = generate_c5_torch(cfg, 2000 + rank, f"cuda:{local}")
+    xh = x.double().cpu().numpy()
+    del x
+    torch.cuda.empty_cache()
+    iters = args.burnin + args.warmup + args.steps
+    rd, keep = make_run(iters)
+    h2d0, d2h0 = ctypes.c_uint64(), ctypes.c_uint64()
+    L.dpmm_transfer_bytes(ctypes.byref(h2d0), ctypes.byref(d2h0))
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    mi = ctypes.c_void_p()
+    check(L.dpmm_dp_parallel(ctypes.byref(rd), xh.shape[0], xh.shape[1],
+                             xh.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(mi)))
+    labels = np.ctypeslib.as_array(L.dpmm_model_info_labels(mi), shape=(xh.shape[0],)).copy()
+    L.dpmm_model_info_free(mi)
+    dt = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([dt], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dt = float(t.item())
+    h2d1, d2h1 = ctypes.c_uint64(), ctypes.c_uint64()
+    L.dpmm_transfer_bytes(ctypes.byref(h2d1), ctypes.byref(d2h1))
+    assert labels.min() >= 1
+    return {"value": world * xh.shape[0] * iters / dt, "unit": UNIT,
+            "h2d_bytes_per_step": int((h2d1.value - h2d0.value) / iters),
+            "d2h_bytes_per_step": int((d2h1.value - d2h0.value) / iters),
+            "iterations": iters, "wall_s": dt,
+            "note": "dpmm_dp_parallel from host float64 points: upload, init, all iterations and label "
+                    "download in the timed region"}
+
+
+def _nmi(a, b):
+    import numpy as np
+    ua, ia = np.unique(a, return_inverse=True)
+    ub, ib = np.unique(b, return_inverse=True)
+    c = np.zeros((ua.size, ub.size))
+    np.add.at(c, (ia, ib), 1)
+    p = c / c.sum()
+    pa, pb = p.sum(1), p.sum(0)
+    h = lambda q: -np.sum(q[q > 0] * np.log(q[q > 0]))
+    nz = p > 0
+    mi = np.sum(p[nz] * np.log(p[nz] / np.outer(pa, pb)[nz]))
+    return float(2 * mi / (h(pa) + h(pb)))
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,402 @@
+"""Host-side mirror of the reference's API for the sampler path.
+
+Names, argument order and meaning follow the reference (DPMMSubClusters/):
+  prior_type                         global_params.h:11-15
+  niw_hyperparams(k, m, v, psi)      priors/niw_hyperparams.h:9-43
+  multinomial_hyper(alpha)           priors/multinomial_hyper.h:9-29
+  ModelInfo                          modelInfo.h:8-56
+  dp_parallel_sampling_class         dp_parallel_sampling.h:9-38 (both constructors,
+                                     dp_parallel, dp_parallel_from_file)
+  CudaKernel                         cudaKernel.cuh:31-138 -- the device back-end, one method per
+                                     reference method, over the C ABI (include/dpmm_capi.h)
+Points follow the reference's Eigen layout: a D x N matrix (one column per point).
+Errors raise capi.DpmmError (the reference printf()s and exit()s instead).
+"""
+from __future__ import annotations
+
+import ctypes
+import enum
+import sys
+from ctypes import byref, c_double, c_float, c_int32, c_int64, c_uint32, c_void_p
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import capi
+from .capi import check, lib
+
+DBL_MAX = sys.float_info.max
+
+
+class prior_type(enum.IntEnum):
+    Gaussian = capi.PRIOR_GAUSSIAN
+    Multinomial = capi.PRIOR_MULTINOMIAL
+
+
+class niw_hyperparams:
+    def __init__(self, k: float, m, v: float, psi):
+        self.k = float(k)
+        self.m = np.ascontiguousarray(m, dtype=np.float64).reshape(-1)
+        self.v = float(v)
+        self.psi = np.asarray(psi, dtype=np.float64).reshape(self.m.size, self.m.size)
+
+    def clone(self):
+        return niw_hyperparams(self.k, self.m.copy(), self.v, self.psi.copy())
+
+
+class multinomial_hyper:
+    def __init__(self, alpha):
+        self.alpha = np.ascontiguousarray(alpha, dtype=np.float64).reshape(-1)
+
+    def clone(self):
+        return multinomial_hyper(self.alpha.copy())
+
+
+class ModelInfo:
+    """labels (1-based, N), weights, iter_count (seconds per iteration), histories."""
+
+    def __init__(self):
+        self.labels = np.zeros(0, np.int32)
+        self.weights = np.zeros(0)
+        self.iter_count = np.zeros(0)
+        self.nmi_score_history = np.zeros(0)
+        self.likelihood_history = np.zeros(0)
+        self.cluster_count_history = np.zeros(0, np.int32)
+
+    @staticmethod
+    def _from_handle(h) -> "ModelInfo":
+        L = lib()
+        mi = ModelInfo()
+        n = L.dpmm_model_info_n(h)
+        it = L.dpmm_model_info_iterations(h)
+        nw = L.dpmm_model_info_num_weights(h)
+        mi.labels = np.ctypeslib.as_array(L.dpmm_model_info_labels(h), shape=(n,)).copy() if n else mi.labels
+        mi.weights = np.ctypeslib.as_array(L.dpmm_model_info_weights(h), shape=(nw,)).copy() if nw else mi.weights
+        if it:
+            mi.iter_count = np.ctypeslib.as_array(L.dpmm_model_info_iter_count(h), shape=(it,)).copy()
+            mi.likelihood_history = np.ctypeslib.as_array(L.dpmm_model_info_likelihood_history(h), shape=(it,)).copy()
+            mi.cluster_count_history = np.ctypeslib.as_array(L.dpmm_model_info_cluster_count_history(h),
+                                                             shape=(it,)).copy()
+            p = L.dpmm_model_info_nmi_history(h)
+            if p:
+                mi.nmi_score_history = np.ctypeslib.as_array(p, shape=(it,)).copy()
+        return mi
+
+
+def _dptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(c_double)) if a is not None else None
+
+
+def _fptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(c_float)) if a is not None else None
+
+
+def _iptr(a):
+    return a.ctypes.data_as(ctypes.POINTER(c_int32)) if a is not None else None
+
+
+def _points_major(all_data, numLabels=None) -> np.ndarray:
+    """D x N (reference layout) -> contiguous N x D float64."""
+    x = np.asarray(all_data, dtype=np.float64)
+    if x.ndim != 2:
+        raise ValueError("points must be a 2-D D x N matrix")
+    if numLabels is not None and x.shape[1] != numLabels:
+        raise ValueError(f"points matrix must be D x N with N = {numLabels}")
+    return np.ascontiguousarray(x.T)
+
+
+class dp_parallel_sampling_class:
+    """dp_parallel_sampling_class(numLabels, all_data (D x N), randomSeed, priorType) or
+    dp_parallel_sampling_class(modelDataFileName (.npy, N x D), modelParamsFileName (JSON), priorType)."""
+
+    def __init__(self, a, b, c=None, d=None, *, loglik_mode: int = capi.LL_AUTO, rng_kind: int = capi.RNG_PHILOX,
+                 k_max: int = 0, device: int = 0):
+        self._from_file = isinstance(a, str)
+        self.loglik_mode, self.rng_kind, self.k_max, self.device = loglik_mode, rng_kind, k_max, device
+        if self._from_file:
+            self.model_path, self.params_path = a, b
+            self.prior = prior_type(c if c is not None else prior_type.Gaussian)
+        else:
+            self.numLabels = int(a)
+            self.points = _points_major(b, self.numLabels)
+            self.random_seed = int(c or 0)
+            self.prior = prior_type(d if d is not None else prior_type.Gaussian)
+
+    def dp_parallel(self, local_hyper_params, alpha_param: float, iters: int = 100, init_clusters: int = 1,
+                    verbose: bool = True, draw_labels: bool = False, save_model: bool = False, burnout: int = 15,
+                    gt: Optional[Sequence[int]] = None, max_clusters: float = DBL_MAX, outlier_weight: float = 0,
+                    outlier_params=None) -> ModelInfo:
+        if self._from_file:
+            raise RuntimeError("dp_parallel needs the (numLabels, all_data, seed, prior) constructor")
+        n, dim = self.points.shape
+        rd = capi.dpmm_run_desc()
+        rd.prior_type = int(self.prior)
+        rd.iterations = iters
+        rd.initial_clusters = init_clusters
+        rd.burnout = burnout
+        rd.alpha = alpha_param
+        rd.max_clusters = max_clusters if max_clusters < DBL_MAX else 0
+        rd.outlier_weight = outlier_weight
+        rd.seed = self.random_seed
+        rd.verbose = int(verbose)
+        rd.loglik_mode = self.loglik_mode
+        rd.rng_kind = self.rng_kind
+        rd.k_max = self.k_max
+        rd.device = self.device
+        keep = []
+
+        def put(h, prefix):
+            if h is None:
+                return
+            if isinstance(h, niw_hyperparams):
+                m, psi = np.ascontiguousarray(h.m), np.ascontiguousarray(h.psi.T)   # column-major
+                keep.extend([m, psi])
+                setattr(rd, prefix + "niw_k", h.k)
+                setattr(rd, prefix + "niw_v", h.v)
+                setattr(rd, prefix + "niw_m", _dptr(m))
+                setattr(rd, prefix + "niw_psi", _dptr(psi))
+            else:
+                a = np.ascontiguousarray(h.alpha)
+                keep.append(a)
+                setattr(rd, prefix + "mult_alpha", _dptr(a))
+
+        put(local_hyper_params, "")
+        put(outlier_params, "out_")
+        if gt is not None:
+            g = np.ascontiguousarray(gt, dtype=np.int32)
+            keep.append(g)
+            rd.gt = _iptr(g)
+        h = c_void_p()
+        check(lib().dpmm_dp_parallel(byref(rd), n, dim, _dptr(self.points), byref(h)))
+        try:
+            return ModelInfo._from_handle(h)
+        finally:
+            lib().dpmm_model_info_free(h)
+
+    def dp_parallel_from_file(self, result_path: Optional[str] = None) -> ModelInfo:
+        if not self._from_file:
+            raise RuntimeError("dp_parallel_from_file needs the (npy, params, prior) constructor")
+        rd = capi.dpmm_run_desc()
+        rd.loglik_mode = self.loglik_mode
+        rd.rng_kind = self.rng_kind
+        rd.k_max = self.k_max
+        rd.device = self.device
+        h = c_void_p()
+        check(lib().dpmm_dp_parallel_from_file(self.model_path.encode(), self.params_path.encode(), int(self.prior),
+                                               byref(rd), byref(h)))
+        try:
+            if result_path:
+                check(lib().dpmm_model_info_write_json(h, result_path.encode()))
+            return ModelInfo._from_handle(h)
+        finally:
+            lib().dpmm_model_info_free(h)
+
+
+class CudaKernel:
+    """The device back-end (the reference's cudaKernel / cudaKernel_gaussian / cudaKernel_multinomial)
+    over the C ABI.  init() mirrors cudaKernel::init(numLabels, points (D x N), seed, verbose,
+    forceKernel); forceKernel 1 selects the FP32 SIMT contraction, 2 the tensor cores."""
+
+    def __init__(self, prior: int = prior_type.Gaussian, rng_kind: int = capi.RNG_PHILOX, k_max: int = 0,
+                 loglik_mode: Optional[int] = None, device: int = 0):
+        self.prior = int(prior)
+        self.rng_kind = rng_kind
+        self.k_max = k_max
+        self.loglik_mode = loglik_mode
+        self.device = device
+        self.ctx = None
+
+    # -------------------------------------------------------------- lifetime (cudaKernel.cu:537-720)
+    def init(self, numLabels: int, points, seed: int = 0, verbose: bool = False, forceKernel: int = 0,
+             points_major: bool = False):
+        x = np.ascontiguousarray(points, np.float64) if points_major else _points_major(points, numLabels)
+        self.N, self.D = x.shape
+        mode = self.loglik_mode
+        if mode is None:
+            mode = {1: capi.LL_FP32, 2: capi.LL_TC_BF16X3}.get(forceKernel, capi.LL_AUTO)
+        d = capi.dpmm_desc()
+        d.n_points, d.dim, d.prior_type = self.N, self.D, self.prior
+        d.k_max, d.rng_kind, d.seed = self.k_max, self.rng_kind, int(seed or 0)
+        d.loglik_mode, d.device, d.verbose = mode, self.device, int(verbose)
+        h = c_void_p()
+        check(lib().dpmm_create(byref(d), byref(h)))
+        self.ctx = h
+        check(lib().dpmm_upload_points(self.ctx, _dptr(x)))
+        return self
+
+    def release(self):
+        if self.ctx:
+            lib().dpmm_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    # -------------------------------------------------------------- labels (cudaKernel.cu:1093-1257)
+    @staticmethod
+    def _u(u, n):
+        if u is None:
+            return None
+        u = np.ascontiguousarray(u, dtype=np.float32).reshape(-1)
+        if u.size != n:
+            raise ValueError(f"expected {n} uniforms, got {u.size}")
+        return u
+
+    def sample_labels(self, initial_clusters: int, outlier_mod: float, uniforms=None):
+        u = self._u(uniforms, self.N)
+        check(lib().dpmm_sample_labels(self.ctx, initial_clusters, outlier_mod, _fptr(u)))
+
+    def sample_sub_labels(self, uniforms=None):
+        u = self._u(uniforms, self.N)
+        check(lib().dpmm_sample_sub_labels(self.ctx, _fptr(u)))
+
+    def set_labels(self, labels):
+        a = np.ascontiguousarray(labels, np.int32)
+        check(lib().dpmm_set_labels(self.ctx, _iptr(a)))
+
+    def set_sub_labels(self, sub):
+        a = np.ascontiguousarray(sub, np.int32)
+        check(lib().dpmm_set_sub_labels(self.ctx, _iptr(a)))
+
+    def get_labels(self) -> np.ndarray:
+        out = np.empty(self.N, np.int32)
+        check(lib().dpmm_get_labels(self.ctx, _iptr(out)))
+        return out
+
+    def get_sub_labels(self) -> np.ndarray:
+        out = np.empty(self.N, np.int32)
+        check(lib().dpmm_get_sub_labels(self.ctx, _iptr(out)))
+        return out
+
+    def get_sub_labels_count(self):
+        l, r = c_int32(), c_int32()
+        check(lib().dpmm_get_sub_labels_count(self.ctx, byref(l), byref(r)))
+        return l.value, r.value
+
+    # -------------------------------------------------------------- parameters
+    def set_gaussian_params(self, mu, inv_sigma, logdet_sigma, weights, mu_lr=None, inv_sigma_lr=None,
+                            logdet_sigma_lr=None, lr_weights=None, factors=False):
+        """mu (K, D); inv_sigma (K, D, D) -- or precision factors W with inv_sigma = W W^T when
+        factors=True; logdet_sigma (K,); weights (K,); *_lr with a leading (K, 2) for l / r."""
+        mu = np.ascontiguousarray(mu, np.float64)
+        K = mu.shape[0]
+        colmaj = lambda a: None if a is None else np.ascontiguousarray(np.swapaxes(np.asarray(a, np.float64), -1, -2))
+        arrs = [mu, colmaj(inv_sigma), np.ascontiguousarray(logdet_sigma, np.float64),
+                np.ascontiguousarray(weights, np.float64),
+                None if mu_lr is None else np.ascontiguousarray(mu_lr, np.float64),
+                colmaj(inv_sigma_lr),
+                None if logdet_sigma_lr is None else np.ascontiguousarray(logdet_sigma_lr, np.float64),
+                None if lr_weights is None else np.ascontiguousarray(lr_weights, np.float64)]
+        fn = lib().dpmm_set_gaussian_factors if factors else lib().dpmm_set_gaussian_params
+        check(fn(self.ctx, K, *[_dptr(a) for a in arrs]))
+        self._keep = arrs
+
+    def set_multinomial_params(self, log_theta, weights=None, log_theta_lr=None, lr_weights=None):
+        lt = np.ascontiguousarray(log_theta, np.float64)
+        K = lt.shape[0]
+        w = np.ones(K) if weights is None else np.ascontiguousarray(weights, np.float64)
+        ltlr = None if log_theta_lr is None else np.ascontiguousarray(log_theta_lr, np.float64)
+        lrw = None if lr_weights is None else np.ascontiguousarray(lr_weights, np.float64)
+        check(lib().dpmm_set_multinomial_params(self.ctx, K, _dptr(lt), _dptr(w), _dptr(ltlr), _dptr(lrw)))
+        self._keep = [lt, w, ltlr, lrw]
+
+    # -------------------------------------------------------------- phases
+    def create_clusters_labels(self, K: int, bFinal: bool = False, uniforms=None, return_loglik=False):
+        u = self._u(uniforms, 2 * self.N)
+        r = np.empty((self.N, K), np.float32) if return_loglik else None
+        check(lib().dpmm_create_clusters_labels(self.ctx, K, int(bFinal), _fptr(u), _fptr(r)))
+        return r
+
+    def create_subclusters_labels(self, K: int, uniforms=None, return_loglik=False):
+        u = self._u(uniforms, 2 * self.N)
+        r = np.empty((self.N, 2), np.float32) if return_loglik else None
+        check(lib().dpmm_create_subclusters_labels(self.ctx, K, _fptr(u), _fptr(r)))
+        return r
+
+    def create_sufficient_statistics(self, indices):
+        """-> count (n, 3), sum (n, 3, D), S (n, 3, D, D) or None, slots cluster / l / r."""
+        idx = np.ascontiguousarray(indices, np.int32)
+        n, D = idx.size, self.D
+        cnt = np.empty(3 * n, np.int64)
+        sm = np.empty(3 * n * D)
+        S = np.empty(3 * n * D * D) if self.prior == prior_type.Gaussian else None
+        check(lib().dpmm_create_sufficient_statistics(self.ctx, n, _iptr(idx), cnt.ctypes.data_as(ctypes.POINTER(c_int64)),
+                                                      _dptr(sm), _dptr(S)))
+        S = None if S is None else S.reshape(n, 3, D, D).swapaxes(-1, -2).copy()
+        return cnt.reshape(n, 3), sm.reshape(n, 3, D), S
+
+    def split_cluster_local_worker(self, index, newIndex, bits=None):
+        i = np.atleast_1d(np.asarray(index, np.int32))
+        j = np.atleast_1d(np.asarray(newIndex, np.int32))
+        b = None if bits is None else np.ascontiguousarray(bits, np.uint32)
+        check(lib().dpmm_split_clusters(self.ctx, i.size, _iptr(i), _iptr(j),
+                                        None if b is None else b.ctypes.data_as(ctypes.POINTER(c_uint32))))
+
+    def merge_clusters_worker(self, index, newIndex):
+        i = np.atleast_1d(np.asarray(index, np.int32))
+        j = np.atleast_1d(np.asarray(newIndex, np.int32))
+        check(lib().dpmm_merge_clusters(self.ctx, i.size, _iptr(i), _iptr(j)))
+
+    def reset_bad_clusters_worker(self, index, bits=None):
+        i = np.atleast_1d(np.asarray(index, np.int32))
+        b = None if bits is None else np.ascontiguousarray(bits, np.uint32)
+        check(lib().dpmm_reset_bad_clusters(self.ctx, i.size, _iptr(i),
+                                            None if b is None else b.ctypes.data_as(ctypes.POINTER(c_uint32))))
+
+    def remove_empty_clusters_worker(self, limit):
+        lim = np.atleast_1d(np.asarray(limit, np.int32))
+        check(lib().dpmm_remove_empty_clusters(self.ctx, lim.size, _iptr(lim)))
+
+    # -------------------------------------------------------------- test seams (test/myCudaKernel.h)
+    def log_likelihood_labels(self, weight, mu, inv_sigma=None, logdet_sigma=0.0, log_theta=None):
+        r = np.empty(self.N)
+        if self.prior == prior_type.Gaussian:
+            m = np.ascontiguousarray(mu, np.float64)
+            s = np.ascontiguousarray(np.asarray(inv_sigma, np.float64).T)
+            check(lib().dpmm_log_likelihood_labels_gaussian(self.ctx, _dptr(m), _dptr(s), logdet_sigma, weight, _dptr(r)))
+        else:
+            lt = np.ascontiguousarray(log_theta if log_theta is not None else mu, np.float64)
+            check(lib().dpmm_log_likelihood_labels_multinomial(self.ctx, _dptr(lt), _dptr(r)))
+        return r
+
+    def sample_log_cat_array(self, log_likelihood_array, uniforms=None):
+        a = np.asarray(log_likelihood_array, np.float64)       # N x K
+        K = a.shape[1]
+        buf = np.ascontiguousarray(a.T)                         # column-major N x K
+        u = self._u(uniforms, 2 * self.N)
+        check(lib().dpmm_sample_log_cat_array(self.ctx, K, _dptr(buf), _fptr(u)))
+
+    def sample_log_cat_array_sub_cluster(self, log_likelihood_array, indices, lr_weights, uniforms=None):
+        a = np.asarray(log_likelihood_array, np.float64)       # m x 2
+        buf = np.ascontiguousarray(a.T)
+        idx = np.ascontiguousarray(indices, np.int32)
+        lw = np.ascontiguousarray(lr_weights, np.float64)
+        u = self._u(uniforms, 2 * self.N)
+        check(lib().dpmm_sample_log_cat_array_sub_cluster(self.ctx, idx.size, _dptr(buf), _iptr(idx), _dptr(lw), _fptr(u)))
+
+    # -------------------------------------------------------------- Hastings (one launch each)
+    def set_prior(self, hyper):
+        if isinstance(hyper, niw_hyperparams):
+            m = np.ascontiguousarray(hyper.m)
+            psi = np.ascontiguousarray(hyper.psi.T)
+            check(lib().dpmm_set_prior_niw(self.ctx, hyper.k, _dptr(m), hyper.v, _dptr(psi)))
+        else:
+            a = np.ascontiguousarray(hyper.alpha)
+            check(lib().dpmm_set_prior_multinomial(self.ctx, _dptr(a)))
+
+    def split_hastings(self, K: int, alpha: float):
+        lml = np.empty(3 * K)
+        hr = np.empty(K)
+        check(lib().dpmm_split_hastings(self.ctx, K, alpha, _dptr(lml), _dptr(hr)))
+        return lml.reshape(K, 3), hr
+
+    def merge_hastings(self, K: int, alpha: float):
+        hr = np.empty(K * K)
+        check(lib().dpmm_merge_hastings(self.ctx, K, alpha, _dptr(hr)))
+        return hr.reshape(K, K)
+
+    def synchronize(self):
+        check(lib().dpmm_synchronize(self.ctx))

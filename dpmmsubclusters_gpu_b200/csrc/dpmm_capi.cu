@@ -1,0 +1,929 @@
+// dpmm_capi.cu -- the device back-end half of the C ABI (include/dpmm_capi.h): context
+// lifetime, point upload, parameter packing, and one entry point per method of the
+// reference's cudaKernel class.  Kernels live in dpmm_kernels.cu / dpmm_hastings.cu /
+// dpmm_tc.cu.
+#include <cuda_runtime.h>
+#include <curand_kernel.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "dpmm_internal.h"
+#include "linalg.h"
+
+namespace dpmm {
+
+static thread_local std::string g_last_error;
+std::atomic<uint64_t> g_launches{0}, g_h2d_bytes{0}, g_d2h_bytes{0};
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+
+dpmm_status fail(dpmm_status s, const std::string& msg)
+{
+    g_last_error = msg;
+    return s;
+}
+
+dpmm_status cuda_status(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return DPMM_ERR_OOM;
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return DPMM_ERR_NO_DEVICE;
+    return DPMM_ERR_CUDA;
+}
+
+int padded_dim(int d)
+{
+    int p = 4;
+    while (p < d) p <<= 1;
+    return p;
+}
+
+static int mult_padded_dim(int d) { return (d + 31) / 32 * 32; }
+
+template <typename T>
+static dpmm_status dev_alloc(T** p, size_t count)
+{
+    *p = nullptr;
+    if (count == 0) return DPMM_OK;
+    cudaError_t e = cudaMalloc((void**)p, sizeof(T) * count);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return cuda_status(e, "cudaMalloc");
+    }
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- point conversion kernels
+template <typename T>
+__global__ void k_col_sums(const T* __restrict__ x, int64_t N, int D, double* __restrict__ out)
+{
+    // block b sums rows [b*R, (b+1)*R) for every column, then atomically adds (FP64)
+    const int64_t R = 4096;
+    const int64_t r0 = (int64_t)blockIdx.x * R;
+    for (int d = threadIdx.x; d < D; d += blockDim.x) {
+        double s = 0;
+        for (int64_t r = r0; r < min(N, r0 + R); ++r) s += (double)x[r * D + d];
+        atomicAdd(&out[d], s);
+    }
+}
+
+template <typename T>
+__global__ void k_convert_points(const T* __restrict__ x, int64_t N, int D, int Dp, const double* __restrict__ shift,
+                                 float* __restrict__ out)
+{
+    int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (e >= N * Dp) return;
+    int64_t n = e / Dp;
+    int d = (int)(e % Dp);
+    float v = 0.f;
+    if (d < D) v = (float)((double)x[n * D + d] - (shift ? shift[d] : 0.0));
+    out[e] = v;
+}
+
+__global__ void k_count_nonfinite(const float* __restrict__ x, int64_t n, int32_t* __restrict__ bad)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n && !isfinite(x[i])) atomicAdd(bad, 1);
+}
+
+}  // namespace dpmm
+
+using namespace dpmm;
+
+// ----------------------------------------------------------------- status / version
+extern "C" const char* dpmm_status_string(dpmm_status s)
+{
+    switch (s) {
+        case DPMM_OK: return "ok";
+        case DPMM_ERR_INVALID_ARG: return "invalid argument";
+        case DPMM_ERR_OOM: return "out of memory";
+        case DPMM_ERR_CUDA: return "CUDA error";
+        case DPMM_ERR_NOT_PD: return "matrix not positive definite";
+        case DPMM_ERR_TIMEOUT: return "device wait timed out";
+        case DPMM_ERR_NUMERIC: return "non-finite value";
+        case DPMM_ERR_STATE: return "call out of order";
+        case DPMM_ERR_IO: return "I/O or parse error";
+        case DPMM_ERR_NO_DEVICE: return "no CUDA device";
+    }
+    return "unknown status";
+}
+
+extern "C" const char* dpmm_last_error(void) { return g_last_error.c_str(); }
+
+extern "C" int dpmm_capi_version(void) { return DPMM_CAPI_VERSION; }
+
+extern "C" uint64_t dpmm_kernel_launch_count(void) { return g_launches.load(); }
+
+extern "C" void dpmm_transfer_bytes(uint64_t* h2d, uint64_t* d2h)
+{
+    if (h2d) *h2d = g_h2d_bytes.load();
+    if (d2h) *d2h = g_d2h_bytes.load();
+}
+
+extern "C" dpmm_status dpmm_phase_times(dpmm_ctx* c, int enable, double* ms, int64_t* calls)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    for (int i = 0; i < PH_COUNT; ++i) {
+        if (ms) ms[i] = c->phase_ms[i];
+        if (calls) calls[i] = c->phase_calls[i];
+    }
+    if (enable >= 0) {
+        c->timing = enable != 0;
+        for (int i = 0; i < PH_COUNT; ++i) { c->phase_ms[i] = 0; c->phase_calls[i] = 0; }
+    }
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- lifetime
+static void free_ctx(dpmm_ctx* c)
+{
+    if (!c) return;
+    if (c->device >= 0) cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void* bufs[] = {c->d_x, c->d_gshift, c->d_labels, c->d_sub, c->d_curand, c->d_Wt, c->d_b, c->d_c, c->d_lrw,
+                    c->d_mu, c->d_perm, c->d_blk_hist, c->d_seg, c->d_chunk, c->d_nchunks, c->d_part, c->d_stats,
+                    c->d_u, c->d_bits, c->d_remap, c->d_aux, c->d_r64, c->d_dbl_scratch, c->d_prior, c->d_lml,
+                    c->d_split_hr, c->d_merge_hr, c->d_post_logdet};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    if (c->h_pinned) cudaFreeHost(c->h_pinned);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
+{
+    if (!desc || !out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    if (desc->n_points <= 0 || desc->n_points > (int64_t)INT32_MAX - 1) return fail(DPMM_ERR_INVALID_ARG, "n_points out of range");
+    if (desc->dim <= 0) return fail(DPMM_ERR_INVALID_ARG, "dim must be positive");
+    if (desc->prior_type != DPMM_PRIOR_GAUSSIAN && desc->prior_type != DPMM_PRIOR_MULTINOMIAL)
+        return fail(DPMM_ERR_INVALID_ARG, "unknown prior_type");
+    if (desc->prior_type == DPMM_PRIOR_GAUSSIAN && desc->dim > kMaxGaussDim)
+        return fail(DPMM_ERR_INVALID_ARG, "Gaussian dimension above 128 is not supported");
+    if (desc->prior_type == DPMM_PRIOR_MULTINOMIAL && desc->dim > kMaxMultDim)
+        return fail(DPMM_ERR_INVALID_ARG, "multinomial dimension above 4096 is not supported");
+    if (desc->rng_kind != DPMM_RNG_PHILOX && desc->rng_kind != DPMM_RNG_CURAND_XORWOW)
+        return fail(DPMM_ERR_INVALID_ARG, "unknown rng_kind");
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return fail(DPMM_ERR_NO_DEVICE, "no CUDA device available");
+    if (desc->device < 0 || desc->device >= ndev) return fail(DPMM_ERR_INVALID_ARG, "device ordinal out of range");
+
+    dpmm_ctx* c = new dpmm_ctx();
+    c->device = desc->device;
+    c->N = desc->n_points;
+    c->D = desc->dim;
+    c->prior = desc->prior_type;
+    c->Dp = c->prior == DPMM_PRIOR_GAUSSIAN ? padded_dim(c->D) : mult_padded_dim(c->D);
+    c->k_max = desc->k_max > 0 ? desc->k_max : 256;
+    c->rng_kind = desc->rng_kind;
+    c->seed = desc->seed;
+    c->ll_mode = desc->loglik_mode;
+    c->verbose = desc->verbose;
+    c->shift.assign(c->D, 0.0);
+    dpmm_status st = DPMM_OK;
+    auto chk = [&](dpmm_status s) {
+        if (st == DPMM_OK) st = s;
+    };
+    if (cudaSetDevice(c->device) != cudaSuccess) {
+        free_ctx(c);
+        return fail(DPMM_ERR_NO_DEVICE, "cudaSetDevice failed");
+    }
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        free_ctx(c);
+        return fail(DPMM_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+    const int64_t N = c->N;
+    const int Dp = c->Dp, KM = c->k_max;
+    const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    c->nblk_hist = (int)((N + 2047) / 2048);
+    c->max_chunks = (int)(N / kChunk) + KM + 1;
+    const int T = Dp * (Dp + 1) / 2;
+    const int SL = gauss ? 1 + Dp + T : 1 + Dp;
+    c->stat_len = gauss ? 1 + c->D + c->D * c->D : 1 + c->D;
+    chk(dev_alloc(&c->d_x, (size_t)N * Dp));
+    chk(dev_alloc(&c->d_gshift, (size_t)c->D));
+    chk(dev_alloc(&c->d_labels, (size_t)N));
+    chk(dev_alloc(&c->d_sub, (size_t)N));
+    chk(dev_alloc(&c->d_perm, (size_t)N));
+    chk(dev_alloc(&c->d_u, (size_t)2 * N));
+    chk(dev_alloc(&c->d_bits, (size_t)N));
+    chk(dev_alloc(&c->d_r64, (size_t)N));
+    if (gauss) {
+        chk(dev_alloc(&c->d_Wt, (size_t)3 * KM * Dp * Dp));
+        chk(dev_alloc(&c->d_b, (size_t)3 * KM * Dp));
+    }
+    chk(dev_alloc(&c->d_c, (size_t)3 * KM));
+    chk(dev_alloc(&c->d_lrw, (size_t)2 * KM));
+    chk(dev_alloc(&c->d_mu, (size_t)3 * KM * Dp));
+    chk(dev_alloc(&c->d_blk_hist, (size_t)c->nblk_hist * (KM + 1)));
+    chk(dev_alloc(&c->d_seg, (size_t)KM + 2));
+    chk(dev_alloc(&c->d_chunk, (size_t)3 * c->max_chunks));
+    chk(dev_alloc(&c->d_nchunks, (size_t)1));
+    chk(dev_alloc(&c->d_part, (size_t)c->max_chunks * 2 * SL));
+    chk(dev_alloc(&c->d_stats, (size_t)3 * KM * c->stat_len));
+    chk(dev_alloc(&c->d_remap, (size_t)KM + 2));
+    chk(dev_alloc(&c->d_aux, (size_t)KM + 16));
+    chk(dev_alloc(&c->d_dbl_scratch, (size_t)std::max(2 + c->D + c->D * c->D, 4 * KM) + 64));
+    chk(dev_alloc(&c->d_prior, (size_t)(gauss ? c->D + c->D * c->D : c->D)));
+    chk(dev_alloc(&c->d_lml, (size_t)3 * KM));
+    chk(dev_alloc(&c->d_split_hr, (size_t)KM));
+    chk(dev_alloc(&c->d_merge_hr, (size_t)KM * KM));
+    chk(dev_alloc(&c->d_post_logdet, (size_t)3 * KM));
+    if (c->rng_kind == DPMM_RNG_CURAND_XORWOW) chk(dev_alloc(&c->d_curand, (size_t)N));
+    if (st == DPMM_OK) {
+        c->h_pinned_bytes = std::max({sizeof(double) * 3 * KM * (size_t)c->stat_len, sizeof(double) * (size_t)KM * KM,
+                                      sizeof(float) * 3 * KM * ((size_t)Dp * Dp + 2 * Dp + 2)});
+        if (cudaMallocHost((void**)&c->h_pinned, c->h_pinned_bytes) != cudaSuccess) {
+            c->h_pinned = nullptr;
+            st = fail(DPMM_ERR_OOM, "cudaMallocHost failed");
+        }
+    }
+    if (st == DPMM_OK) {
+        cudaMemsetAsync(c->d_x, 0, sizeof(float) * (size_t)N * Dp, c->stream);
+        cudaMemsetAsync(c->d_labels, 0, sizeof(int32_t) * N, c->stream);
+        cudaMemsetAsync(c->d_sub, 0, sizeof(int32_t) * N, c->stream);
+        cudaMemsetAsync(c->d_gshift, 0, sizeof(double) * c->D, c->stream);
+        cudaMemsetAsync(c->d_mu, 0, sizeof(float) * 3 * KM * Dp, c->stream);
+        if (gauss) {
+            cudaMemsetAsync(c->d_Wt, 0, sizeof(float) * 3 * KM * (size_t)Dp * Dp, c->stream);
+            cudaMemsetAsync(c->d_b, 0, sizeof(float) * 3 * KM * Dp, c->stream);
+        }
+        if (c->d_curand) st = launch_init_curand(c);
+    }
+    if (st == DPMM_OK) {
+        cudaError_t e2 = cudaStreamSynchronize(c->stream);
+        if (e2 != cudaSuccess) st = cuda_status(e2, "dpmm_create");
+    }
+    if (st != DPMM_OK) {
+        std::string msg = g_last_error;
+        free_ctx(c);
+        g_last_error = msg;
+        return st;
+    }
+    *out = c;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_destroy(dpmm_ctx* ctx)
+{
+    free_ctx(ctx);
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_synchronize(dpmm_ctx* c)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- points
+template <typename T>
+static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
+{
+    if (!c || !points) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    const int64_t N = c->N;
+    const int D = c->D;
+    T* tmp = nullptr;
+    DPMM_TRY(dev_alloc(&tmp, (size_t)N * D));
+    // cudaMemcpyDefault: the points may live in host or device memory
+    cudaError_t e = cudaMemcpyAsync(tmp, points, sizeof(T) * (size_t)N * D, cudaMemcpyDefault, c->stream);
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, points) == cudaSuccess && pa.type != cudaMemoryTypeDevice)
+        g_h2d_bytes += sizeof(T) * (size_t)N * D;
+    cudaGetLastError();
+    const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    if (e == cudaSuccess && gauss) {
+        // FP64 column means (the shift)
+        cudaMemsetAsync(c->d_gshift, 0, sizeof(double) * D, c->stream);
+        k_col_sums<T><<<(unsigned)((N + 4095) / 4096), 128, 0, c->stream>>>(tmp, N, D, c->d_gshift);
+        e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess) {
+            std::vector<double> sums(D);
+            e = cudaMemcpy(sums.data(), c->d_gshift, sizeof(double) * D, cudaMemcpyDeviceToHost);
+            for (int d = 0; d < D; ++d) c->shift[d] = sums[d] / (double)N;
+            if (e == cudaSuccess)
+                e = cudaMemcpy(c->d_gshift, c->shift.data(), sizeof(double) * D, cudaMemcpyHostToDevice);
+        }
+    }
+    if (e == cudaSuccess) {
+        const int64_t total = N * c->Dp;
+        k_convert_points<T><<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(
+            tmp, N, D, c->Dp, gauss ? c->d_gshift : nullptr, c->d_x);
+        cudaMemsetAsync(c->d_aux, 0, sizeof(int32_t), c->stream);
+        k_count_nonfinite<<<(unsigned)((total + 255) / 256), 256, 0, c->stream>>>(c->d_x, total, c->d_aux);
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(tmp);
+    if (e != cudaSuccess) return cuda_status(e, "dpmm_upload_points");
+    int32_t bad = 0;
+    DPMM_CUDA_TRY(cudaMemcpy(&bad, c->d_aux, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (bad) return fail(DPMM_ERR_NUMERIC, "points contain NaN or Inf");
+    c->points_ready = true;
+    c->perm_K = -1;
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_upload_points(dpmm_ctx* c, const double* points) { return upload_points_t(c, points); }
+extern "C" dpmm_status dpmm_upload_points_f32(dpmm_ctx* c, const float* points) { return upload_points_t(c, points); }
+
+// ----------------------------------------------------------------- labels
+static dpmm_status stage_uniforms(dpmm_ctx* c, const float* u, int64_t n, const float** d_u)
+{
+    *d_u = nullptr;
+    if (!u) return DPMM_OK;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_u, u, sizeof(float) * n, cudaMemcpyHostToDevice, c->stream));
+    g_h2d_bytes += sizeof(float) * n;
+    *d_u = c->d_u;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sample_labels(dpmm_ctx* c, int initial_clusters, double outlier_mod, const float* u)
+{
+    if (!c || initial_clusters < 1) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    const float* du;
+    DPMM_TRY(stage_uniforms(c, u, c->N, &du));
+    DPMM_TRY(launch_labels_init(c, initial_clusters, outlier_mod, du));
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sample_sub_labels(dpmm_ctx* c, const float* u)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    const float* du;
+    DPMM_TRY(stage_uniforms(c, u, c->N, &du));
+    DPMM_TRY(launch_sub_labels_init(c, du));
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_labels(dpmm_ctx* c, const int32_t* labels)
+{
+    if (!c || !labels) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_labels, labels, sizeof(int32_t) * c->N, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->perm_K = -1;
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_sub_labels(dpmm_ctx* c, const int32_t* sub)
+{
+    if (!c || !sub) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_sub, sub, sizeof(int32_t) * c->N, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_get_labels(dpmm_ctx* c, int32_t* labels)
+{
+    if (!c || !labels) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(labels, c->d_labels, sizeof(int32_t) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    g_d2h_bytes += sizeof(int32_t) * c->N;
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_get_sub_labels(dpmm_ctx* c, int32_t* sub)
+{
+    if (!c || !sub) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(sub, c->d_sub, sizeof(int32_t) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_get_sub_labels_count(dpmm_ctx* c, int32_t* l, int32_t* r)
+{
+    if (!c || !l || !r) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    return launch_sub_count(c, l, r);
+}
+
+// ----------------------------------------------------------------- cluster parameters
+// Pack one Gaussian slot: Wt[j][i] = W(i, j), b = W^T (mu - shift), c = -logdet/2 (+ log w), mu - shift.
+static void pack_gauss_slot(dpmm_ctx* c, int slot, const double* mu, const std::vector<double>& W, double cval,
+                            float* hWt, float* hb, float* hc, float* hmu)
+{
+    const int D = c->D, Dp = c->Dp;
+    float* wt = hWt + (size_t)slot * Dp * Dp;
+    std::fill(wt, wt + (size_t)Dp * Dp, 0.f);
+    for (int j = 0; j < D; ++j)
+        for (int i = 0; i < D; ++i) wt[(size_t)j * Dp + i] = (float)W[(size_t)j * D + i];
+    for (int j = 0; j < Dp; ++j) {
+        double s = 0;
+        if (j < D)
+            for (int i = 0; i < D; ++i) s += W[(size_t)j * D + i] * (mu[i] - c->shift[i]);
+        hb[(size_t)slot * Dp + j] = (float)s;
+        hmu[(size_t)slot * Dp + j] = j < D ? (float)(mu[j] - c->shift[j]) : 0.f;
+    }
+    hc[slot] = (float)cval;
+}
+
+static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, const double* mat, bool is_factor,
+                                       const double* logdet, const double* weights, const double* mu_lr,
+                                       const double* mat_lr, const double* logdet_lr, const double* lr_weights)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (c->prior != DPMM_PRIOR_GAUSSIAN) return fail(DPMM_ERR_STATE, "context is not Gaussian");
+    if (K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [1, k_max]");
+    if (!mu || !mat || !logdet || !weights) return fail(DPMM_ERR_INVALID_ARG, "null cluster parameter");
+    const int D = c->D, Dp = c->Dp;
+    float* hWt = reinterpret_cast<float*>(c->h_pinned);
+    float* hb = hWt + (size_t)3 * K * Dp * Dp;
+    float* hc = hb + (size_t)3 * K * Dp;
+    float* hmu = hc + 3 * K;
+    std::vector<float> hlrw(2 * K, 0.f);
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));   // the pinned stage may still be in flight
+    std::vector<double> W;
+    for (int k = 0; k < K; ++k) {
+        for (int s = 0; s < 3; ++s) {
+            const bool sub = s > 0;
+            if (sub && !mu_lr) {
+                // no sub-cluster parameters: zero slots (sub-label phase then needs them set later)
+                std::fill(hWt + (size_t)(3 * k + s) * Dp * Dp, hWt + (size_t)(3 * k + s + 1) * Dp * Dp, 0.f);
+                std::fill(hb + (size_t)(3 * k + s) * Dp, hb + (size_t)(3 * k + s + 1) * Dp, 0.f);
+                std::fill(hmu + (size_t)(3 * k + s) * Dp, hmu + (size_t)(3 * k + s + 1) * Dp, 0.f);
+                hc[3 * k + s] = 0.f;
+                continue;
+            }
+            const int idx = sub ? 2 * k + (s - 1) : k;
+            const double* m = sub ? mu_lr + (size_t)idx * D : mu + (size_t)k * D;
+            const double* A = sub ? mat_lr + (size_t)idx * D * D : mat + (size_t)k * D * D;
+            const double ld = sub ? logdet_lr[idx] : logdet[k];
+            if (is_factor) {
+                W.assign(A, A + (size_t)D * D);
+            } else if (!la::cholesky(A, D, W)) {
+                return fail(DPMM_ERR_NOT_PD, "inv_sigma of cluster " + std::to_string(k) + (sub ? " (sub)" : "") +
+                                                 " is not positive definite");
+            }
+            double cval = -ld / 2;
+            if (!sub) cval += std::log(weights[k]);
+            if (!std::isfinite(cval) && !(cval < 0)) return fail(DPMM_ERR_NUMERIC, "non-finite log-likelihood constant");
+            pack_gauss_slot(c, 3 * k + s, m, W, cval, hWt, hb, hc, hmu);
+            if (sub) hlrw[idx] = lr_weights ? (float)std::log(lr_weights[idx]) : 0.f;
+        }
+    }
+    // relocate packed arrays to their device buffers
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_Wt, hWt, sizeof(float) * 3 * K * (size_t)Dp * Dp, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_b, hb, sizeof(float) * 3 * K * (size_t)Dp, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c, hc, sizeof(float) * 3 * K, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, hmu, sizeof(float) * 3 * K * (size_t)Dp, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hlrw.data(), sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
+    g_h2d_bytes += sizeof(float) * 3 * (size_t)K * ((size_t)Dp * Dp + 2 * Dp + 1) + sizeof(float) * 2 * K;
+    c->K_params = K;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_gaussian_params(dpmm_ctx* c, int K, const double* mu, const double* inv_sigma,
+                                                const double* logdet_sigma, const double* weights, const double* mu_lr,
+                                                const double* inv_sigma_lr, const double* logdet_sigma_lr,
+                                                const double* lr_weights)
+{
+    return upload_gauss_params(c, K, mu, inv_sigma, false, logdet_sigma, weights, mu_lr, inv_sigma_lr, logdet_sigma_lr,
+                               lr_weights);
+}
+
+extern "C" dpmm_status dpmm_set_gaussian_factors(dpmm_ctx* c, int K, const double* mu, const double* w,
+                                                 const double* logdet_sigma, const double* weights, const double* mu_lr,
+                                                 const double* w_lr, const double* logdet_sigma_lr,
+                                                 const double* lr_weights)
+{
+    return upload_gauss_params(c, K, mu, w, true, logdet_sigma, weights, mu_lr, w_lr, logdet_sigma_lr, lr_weights);
+}
+
+extern "C" dpmm_status dpmm_set_multinomial_params(dpmm_ctx* c, int K, const double* log_theta, const double* weights,
+                                                   const double* log_theta_lr, const double* lr_weights)
+{
+    (void)weights;
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (c->prior != DPMM_PRIOR_MULTINOMIAL) return fail(DPMM_ERR_STATE, "context is not multinomial");
+    if (K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [1, k_max]");
+    if (!log_theta) return fail(DPMM_ERR_INVALID_ARG, "null log_theta");
+    const int D = c->D, Dp = c->Dp;
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    float* hmu = reinterpret_cast<float*>(c->h_pinned);
+    float* hc = hmu + (size_t)3 * K * Dp;
+    std::vector<float> hlrw(2 * K, 0.f);
+    for (int k = 0; k < K; ++k)
+        for (int s = 0; s < 3; ++s) {
+            const double* src = s == 0 ? log_theta + (size_t)k * D
+                                       : (log_theta_lr ? log_theta_lr + (size_t)(2 * k + s - 1) * D : nullptr);
+            float* dst = hmu + (size_t)(3 * k + s) * Dp;
+            for (int d = 0; d < Dp; ++d) dst[d] = (src && d < D) ? (float)src[d] : 0.f;
+            hc[3 * k + s] = 0.f;
+            if (s > 0) hlrw[2 * k + s - 1] = lr_weights ? (float)std::log(lr_weights[2 * k + s - 1]) : 0.f;
+        }
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, hmu, sizeof(float) * 3 * K * (size_t)Dp, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c, hc, sizeof(float) * 3 * K, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hlrw.data(), sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
+    c->K_params = K;
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- phases
+static dpmm_status check_ready(dpmm_ctx* c, int K)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (!c->points_ready) return fail(DPMM_ERR_STATE, "points not uploaded");
+    if (K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [1, k_max]");
+    if (K > c->K_params) return fail(DPMM_ERR_STATE, "cluster parameters not set for K clusters");
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final_, const float* u, float* loglik_out)
+{
+    DPMM_TRY(check_ready(c, K));
+    const float* du = nullptr;
+    if (!final_) DPMM_TRY(stage_uniforms(c, u, 2 * c->N, &du));
+    float* d_rout = nullptr;
+    if (loglik_out) DPMM_TRY(dev_alloc(&d_rout, (size_t)c->N * K));
+    dpmm_status s;
+    const bool use_tc = c->ll_mode != DPMM_LL_FP32 && tc_supported(c, K);
+    PhaseTimer pt(c, PH_LABELS);
+    if (c->ll_mode == DPMM_LL_TC_BF16X3 && !use_tc) {
+        s = fail(DPMM_ERR_INVALID_ARG, "tensor-core log-likelihood not available for this shape");
+    } else {
+        s = use_tc ? launch_cluster_labels_tc(c, K, final_, du, d_rout) : launch_cluster_labels(c, K, final_, du, d_rout);
+    }
+    if (s == DPMM_OK && d_rout) {
+        cudaError_t e = cudaMemcpyAsync(loglik_out, d_rout, sizeof(float) * (size_t)c->N * K, cudaMemcpyDeviceToHost,
+                                        c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s = cuda_status(e, "loglik_out copy");
+    }
+    if (d_rout) cudaFree(d_rout);
+    if (s == DPMM_OK && u) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);   // caller's uniforms staged: keep order simple
+        if (e != cudaSuccess) s = cuda_status(e, "dpmm_create_clusters_labels");
+    }
+    c->perm_K = -1;
+    c->stats_K = -1;
+    return s;
+}
+
+extern "C" dpmm_status dpmm_create_subclusters_labels(dpmm_ctx* c, int K, const float* u, float* loglik_out)
+{
+    DPMM_TRY(check_ready(c, K));
+    const float* du = nullptr;
+    DPMM_TRY(stage_uniforms(c, u, 2 * c->N, &du));
+    float* d_rout = nullptr;
+    if (loglik_out) DPMM_TRY(dev_alloc(&d_rout, (size_t)c->N * 2));
+    dpmm_status s;
+    {
+        PhaseTimer pt(c, PH_SUB_STATS);
+        s = launch_sub_labels_and_stats(c, K, du, d_rout, true);
+    }
+    if (s == DPMM_OK && d_rout) {
+        cudaError_t e = cudaMemcpyAsync(loglik_out, d_rout, sizeof(float) * (size_t)c->N * 2, cudaMemcpyDeviceToHost,
+                                        c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s = cuda_status(e, "loglik_out copy");
+    }
+    if (d_rout) cudaFree(d_rout);
+    return s;
+}
+
+extern "C" dpmm_status dpmm_create_sufficient_statistics(dpmm_ctx* c, int n, const int32_t* indices, int64_t* count,
+                                                         double* sum, double* S)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (!c->points_ready) return fail(DPMM_ERR_STATE, "points not uploaded");
+    if (n < 0 || (n > 0 && !indices)) return fail(DPMM_ERR_INVALID_ARG, "bad index list");
+    int K = 0;
+    for (int i = 0; i < n; ++i) {
+        if (indices[i] < 0 || indices[i] >= c->k_max) return fail(DPMM_ERR_INVALID_ARG, "cluster index out of range");
+        K = std::max(K, indices[i] + 1);
+    }
+    if (n == 0) return DPMM_OK;
+    // statistics are (re)computed for every current cluster, so that the Hastings launches
+    // that follow see all of them; each cluster's accumulation is shifted by its mean parameter
+    const int Keff = std::min(c->k_max, std::max(K, c->K_params));
+    if (c->stats_K < Keff) {
+        PhaseTimer pt(c, PH_STATS);
+        DPMM_TRY(launch_sub_labels_and_stats(c, Keff, nullptr, nullptr, false));
+    }
+    g_d2h_bytes += sizeof(double) * 3 * (size_t)Keff * c->stat_len;
+    const int L = c->stat_len, D = c->D;
+    double* h = c->h_pinned;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_stats, sizeof(double) * 3 * (size_t)K * L, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int q = 0; q < n; ++q) {
+        const int k = indices[q];
+        for (int s = 0; s < 3; ++s) {
+            const double* src = h + (size_t)(3 * k + s) * L;
+            if (count) count[3 * q + s] = (int64_t)llround(src[0]);
+            if (sum) std::memcpy(sum + (size_t)(3 * q + s) * D, src + 1, sizeof(double) * D);
+            if (S && c->prior == DPMM_PRIOR_GAUSSIAN)
+                std::memcpy(S + (size_t)(3 * q + s) * D * D, src + 1 + D, sizeof(double) * D * D);
+        }
+    }
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- label maintenance
+static bool has_repeats(int n, const int32_t* a, const int32_t* b)
+{
+    std::vector<int32_t> v;
+    for (int i = 0; i < n; ++i) {
+        v.push_back(a[i]);
+        if (b) v.push_back(b[i]);
+    }
+    std::sort(v.begin(), v.end());
+    return std::adjacent_find(v.begin(), v.end()) != v.end();
+}
+
+static dpmm_status stage_bits(dpmm_ctx* c, const uint32_t* bits, const uint32_t** d_bits)
+{
+    *d_bits = nullptr;
+    if (!bits) return DPMM_OK;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_bits, bits, sizeof(uint32_t) * c->N, cudaMemcpyHostToDevice, c->stream));
+    *d_bits = c->d_bits;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_split_clusters(dpmm_ctx* c, int n, const int32_t* index, const int32_t* new_index,
+                                           const uint32_t* bits)
+{
+    if (!c || n < 0 || (n > 0 && (!index || !new_index))) return fail(DPMM_ERR_INVALID_ARG, "bad split list");
+    const int tlen = c->k_max + 2;
+    for (int i = 0; i < n; ++i)
+        if (index[i] < 0 || new_index[i] < 0 || index[i] + 1 >= tlen || new_index[i] + 1 >= tlen)
+            return fail(DPMM_ERR_INVALID_ARG, "split index out of range");
+    const uint32_t* db;
+    DPMM_TRY(stage_bits(c, bits, &db));
+    const bool seq = has_repeats(n, index, new_index);
+    std::vector<int32_t> table(tlen, 0);
+    for (int i = 0; i < n; ++i) {
+        if (seq) std::fill(table.begin(), table.end(), 0);
+        table[index[i] + 1] = new_index[i] + 1;
+        if (seq || i == n - 1) DPMM_TRY(launch_relabel(c, 0, 0, table.data(), tlen, db));
+    }
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_merge_clusters(dpmm_ctx* c, int n, const int32_t* index, const int32_t* new_index)
+{
+    if (!c || n < 0 || (n > 0 && (!index || !new_index))) return fail(DPMM_ERR_INVALID_ARG, "bad merge list");
+    const int tlen = c->k_max + 2;
+    for (int i = 0; i < n; ++i)
+        if (index[i] < 0 || new_index[i] < 0 || index[i] + 1 >= tlen || new_index[i] + 1 >= tlen)
+            return fail(DPMM_ERR_INVALID_ARG, "merge index out of range");
+    const bool seq = has_repeats(n, index, new_index);
+    std::vector<int32_t> table(tlen, 0);
+    for (int i = 0; i < n; ++i) {
+        if (seq) std::fill(table.begin(), table.end(), 0);
+        table[index[i] + 1] = 1;
+        table[new_index[i] + 1] = -(index[i] + 1);
+        if (seq || i == n - 1) DPMM_TRY(launch_relabel(c, 1, 0, table.data(), tlen, nullptr));
+    }
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_reset_bad_clusters(dpmm_ctx* c, int n, const int32_t* index, const uint32_t* bits)
+{
+    if (!c || n < 0 || (n > 0 && !index)) return fail(DPMM_ERR_INVALID_ARG, "bad reset list");
+    if (n == 0) return DPMM_OK;
+    const int tlen = c->k_max + 2;
+    std::vector<int32_t> table(tlen, 0);
+    for (int i = 0; i < n; ++i) {
+        if (index[i] < 0 || index[i] + 1 >= tlen) return fail(DPMM_ERR_INVALID_ARG, "reset index out of range");
+        table[index[i] + 1] = 1;
+    }
+    const uint32_t* db;
+    DPMM_TRY(stage_bits(c, bits, &db));
+    if (has_repeats(n, index, nullptr)) {
+        // a repeated index re-randomises the same points again (one draw per listing)
+        for (int i = 0; i < n; ++i) {
+            std::fill(table.begin(), table.end(), 0);
+            table[index[i] + 1] = 1;
+            DPMM_TRY(launch_relabel(c, 2, 0, table.data(), tlen, db));
+        }
+    } else {
+        DPMM_TRY(launch_relabel(c, 2, 0, table.data(), tlen, db));
+    }
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_remove_empty_clusters(dpmm_ctx* c, int n, const int32_t* limits)
+{
+    if (!c || n < 0 || (n > 0 && !limits)) return fail(DPMM_ERR_INVALID_ARG, "bad limit list");
+    if (n == 0) return DPMM_OK;
+    const int tlen = c->k_max + 2;
+    std::vector<int32_t> table(tlen);
+    for (int v = 0; v < tlen; ++v) {
+        int x = v;
+        for (int i = 0; i < n; ++i)
+            if (x > limits[i]) x -= 1;
+        table[v] = x;
+    }
+    DPMM_TRY(launch_relabel(c, 3, 0, table.data(), tlen, nullptr));
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- test seams
+extern "C" dpmm_status dpmm_log_likelihood_labels_gaussian(dpmm_ctx* c, const double* mu, const double* inv_sigma,
+                                                           double logdet_sigma, double weight, double* r_out)
+{
+    if (!c || !mu || !inv_sigma || !r_out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_GAUSSIAN) return fail(DPMM_ERR_STATE, "context is not Gaussian");
+    if (!c->points_ready) return fail(DPMM_ERR_STATE, "points not uploaded");
+    const int D = c->D;
+    std::vector<double> prm((size_t)D + D * D + 2);
+    std::memcpy(prm.data(), mu, sizeof(double) * D);
+    std::memcpy(prm.data() + D, inv_sigma, sizeof(double) * D * D);
+    prm[D + D * D] = -(((double)D * D * std::log(2 * M_PI) + logdet_sigma) / 2);   // sigma.size() == D*D
+    prm[D + D * D + 1] = std::log(weight);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_dbl_scratch, prm.data(), sizeof(double) * prm.size(), cudaMemcpyHostToDevice,
+                                  c->stream));
+    DPMM_TRY(launch_loglik_gauss_one(c, c->d_r64));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(r_out, c->d_r64, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_log_likelihood_labels_multinomial(dpmm_ctx* c, const double* log_theta, double* r_out)
+{
+    if (!c || !log_theta || !r_out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (!c->points_ready) return fail(DPMM_ERR_STATE, "points not uploaded");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_dbl_scratch, log_theta, sizeof(double) * c->D, cudaMemcpyHostToDevice, c->stream));
+    DPMM_TRY(launch_loglik_mult_one(c, c->d_r64));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(r_out, c->d_r64, sizeof(double) * c->N, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sample_log_cat_array(dpmm_ctx* c, int K, const double* loglik, const float* u)
+{
+    if (!c || !loglik || K < 1) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    double* d_r = nullptr;
+    DPMM_TRY(dev_alloc(&d_r, (size_t)c->N * K));
+    const float* du;
+    dpmm_status s = stage_uniforms(c, u, 2 * c->N, &du);
+    cudaError_t e = cudaMemcpyAsync(d_r, loglik, sizeof(double) * c->N * K, cudaMemcpyHostToDevice, c->stream);
+    if (s == DPMM_OK && e != cudaSuccess) s = cuda_status(e, "copy");
+    if (s == DPMM_OK) s = launch_sample_log_cat(c, K, d_r, du);
+    if (s == DPMM_OK) {
+        e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s = cuda_status(e, "dpmm_sample_log_cat_array");
+    }
+    cudaFree(d_r);
+    c->perm_K = -1;
+    c->stats_K = -1;
+    return s;
+}
+
+extern "C" dpmm_status dpmm_sample_log_cat_array_sub_cluster(dpmm_ctx* c, int m, const double* loglik,
+                                                             const int32_t* indices, const double* lr_weights,
+                                                             const float* u)
+{
+    if (!c || m < 0 || (m > 0 && (!loglik || !indices || !lr_weights))) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    if (m == 0) return DPMM_OK;
+    double* d_r = nullptr;
+    int32_t* d_idx = nullptr;
+    DPMM_TRY(dev_alloc(&d_r, (size_t)2 * m + 2));
+    dpmm_status s = dev_alloc(&d_idx, (size_t)m);
+    const float* du = nullptr;
+    if (s == DPMM_OK) s = stage_uniforms(c, u, 2 * c->N, &du);
+    if (s == DPMM_OK) {
+        cudaError_t e = cudaMemcpyAsync(d_r, loglik, sizeof(double) * 2 * m, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_r + 2 * m, lr_weights, sizeof(double) * 2, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_idx, indices, sizeof(int32_t) * m, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) s = cuda_status(e, "copy");
+    }
+    if (s == DPMM_OK) s = launch_sample_log_cat_sub(c, m, d_r, d_idx, d_r + 2 * m, du);
+    if (s == DPMM_OK) {
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) s = cuda_status(e, "dpmm_sample_log_cat_array_sub_cluster");
+    }
+    cudaFree(d_r);
+    if (d_idx) cudaFree(d_idx);
+    c->stats_K = -1;
+    return s;
+}
+
+// ----------------------------------------------------------------- priors + Hastings
+extern "C" dpmm_status dpmm_set_prior_niw(dpmm_ctx* c, double k, const double* m, double v, const double* psi)
+{
+    if (!c || !m || !psi) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_GAUSSIAN) return fail(DPMM_ERR_STATE, "context is not Gaussian");
+    const int D = c->D;
+    std::vector<double> L;
+    if (!la::cholesky(psi, D, L)) return fail(DPMM_ERR_NOT_PD, "prior psi is not positive definite");
+    c->prior_logdet = la::logdet_from_chol(L, D);
+    c->prior_k = k;
+    c->prior_v = v;
+    std::vector<double> h((size_t)D + D * D);
+    std::memcpy(h.data(), m, sizeof(double) * D);
+    std::memcpy(h.data() + D, psi, sizeof(double) * D * D);
+    DPMM_CUDA_TRY(cudaMemcpy(c->d_prior, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    c->prior_set = true;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_prior_multinomial(dpmm_ctx* c, const double* alpha)
+{
+    if (!c || !alpha) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_MULTINOMIAL) return fail(DPMM_ERR_STATE, "context is not multinomial");
+    DPMM_CUDA_TRY(cudaMemcpy(c->d_prior, alpha, sizeof(double) * c->D, cudaMemcpyHostToDevice));
+    c->prior_set = true;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_split_hastings(dpmm_ctx* c, int K, double alpha, double* lml, double* split_log_hr)
+{
+    if (!c || K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    {
+        PhaseTimer pt(c, PH_SPLIT_HR);
+        DPMM_TRY(launch_split_hastings(c, K, alpha));
+    }
+    if (lml) DPMM_CUDA_TRY(cudaMemcpyAsync(lml, c->d_lml, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost, c->stream));
+    if (split_log_hr)
+        DPMM_CUDA_TRY(cudaMemcpyAsync(split_log_hr, c->d_split_hr, sizeof(double) * K, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_merge_hastings(dpmm_ctx* c, int K, double alpha, double* merge_log_hr)
+{
+    if (!c || K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    {
+        PhaseTimer pt(c, PH_MERGE_HR);
+        DPMM_TRY(launch_merge_hastings(c, K, alpha));
+    }
+    if (merge_log_hr)
+        DPMM_CUDA_TRY(cudaMemcpyAsync(merge_log_hr, c->d_merge_hr, sizeof(double) * (size_t)K * K,
+                                      cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- all-points statistics
+namespace dpmm {
+
+__global__ void k_fill_i32(int32_t* __restrict__ a, int64_t n, int32_t v)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = v;
+}
+
+dpmm_status launch_fill_labels(dpmm_ctx* c, int32_t value)
+{
+    k_fill_i32<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->d_labels, c->N, value);
+    DPMM_CUDA_TRY(cudaGetLastError());
+    c->perm_K = -1;
+    c->stats_K = -1;
+    return DPMM_OK;
+}
+
+// Statistics of every point (slot 0 of a one-cluster reduction over the label-ordered
+// machinery); the labels are saved and restored around it.  Points need sub-labels in {1, 2}.
+dpmm_status all_points_stats(dpmm_ctx* c, int64_t* count, double* sum, double* S)
+{
+    int32_t* saved = reinterpret_cast<int32_t*>(c->d_bits);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(saved, c->d_labels, sizeof(int32_t) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    const int kp = c->K_params;
+    DPMM_TRY(launch_fill_labels(c, 1));
+    // shift of the accumulation: the mean parameter slot 0 is replaced by zeros for the call
+    std::vector<float> zero(c->Dp, 0.f), keep(c->Dp);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(keep.data(), c->d_mu, sizeof(float) * c->Dp, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, zero.data(), sizeof(float) * c->Dp, cudaMemcpyHostToDevice, c->stream));
+    c->K_params = std::max(kp, 1);
+    int32_t idx = 0;
+    int64_t cnt[3];
+    const int D = c->D;
+    std::vector<double> sm(3 * (size_t)D), SS(c->prior == DPMM_PRIOR_GAUSSIAN ? 3 * (size_t)D * D : 0);
+    c->stats_K = -1;
+    dpmm_status st = dpmm_create_sufficient_statistics(c, 1, &idx, cnt, sm.data(), SS.empty() ? nullptr : SS.data());
+    c->K_params = kp;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, keep.data(), sizeof(float) * c->Dp, cudaMemcpyHostToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_labels, saved, sizeof(int32_t) * c->N, cudaMemcpyDeviceToDevice, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->perm_K = -1;
+    c->stats_K = -1;
+    DPMM_TRY(st);
+    if (count) *count = cnt[0];
+    if (sum) std::memcpy(sum, sm.data(), sizeof(double) * D);
+    if (S && !SS.empty()) std::memcpy(S, SS.data(), sizeof(double) * D * D);
+    return DPMM_OK;
+}
+
+}  // namespace dpmm

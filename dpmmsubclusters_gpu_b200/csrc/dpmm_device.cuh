@@ -1,0 +1,174 @@
+// dpmm_device.cuh -- device helpers shared by the kernels: uniforms (caller-supplied,
+// Philox4x32-10, or the cuRAND XORWOW device API in compat mode) and the Walker alias
+// draw with the reference's exact construction order.
+#pragma once
+
+#include <curand_kernel.h>
+#include <stdint.h>
+
+#include "dpmm_internal.h"
+
+namespace dpmm {
+
+// Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy as 1, 2, 3",
+// SC'11): ten rounds of the 4x32 bijection keyed by a 64-bit key, with the multipliers and
+// Weyl key increments published in that paper.
+struct Philox4 {
+    uint32_t v[4];
+};
+
+__device__ __forceinline__ Philox4 philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                                 uint32_t k0, uint32_t k1)
+{
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0 = __umulhi(M0, c0), lo0 = M0 * c0;
+        uint32_t hi1 = __umulhi(M1, c2), lo1 = M1 * c2;
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+        k0 += W0;
+        k1 += W1;
+    }
+    Philox4 o;
+    o.v[0] = c0; o.v[1] = c1; o.v[2] = c2; o.v[3] = c3;
+    return o;
+}
+
+// 24 random bits -> float in (0, 1] (the range curand_uniform returns)
+__device__ __forceinline__ float u01_from_bits(uint32_t x)
+{
+    return (float)((x >> 8) + 1u) * (1.0f / 16777216.0f);
+}
+
+__device__ __forceinline__ Philox4 philox_point(const RngArgs& r, int64_t pt)
+{
+    return philox4x32_10((uint32_t)pt, (uint32_t)((uint64_t)pt >> 32), (uint32_t)r.ctr,
+                         (uint32_t)(r.ctr >> 32), (uint32_t)r.seed, (uint32_t)(r.seed >> 32));
+}
+
+// Two uniforms for point pt (the two curand_uniform() calls of cudaKernel.cu:115-116).
+__device__ __forceinline__ void draw_uniform2(const RngArgs& r, int64_t pt, float& u1, float& u2)
+{
+    if (r.ucaller) {
+        u1 = r.ucaller[2 * pt];
+        u2 = r.ucaller[2 * pt + 1];
+    } else if (r.kind == DPMM_RNG_CURAND_XORWOW) {
+        curandStateXORWOW st = r.states[pt];
+        u1 = curand_uniform(&st);
+        u2 = curand_uniform(&st);
+        r.states[pt] = st;
+    } else {
+        Philox4 o = philox_point(r, pt);
+        u1 = u01_from_bits(o.v[0]);
+        u2 = u01_from_bits(o.v[1]);
+    }
+}
+
+// One uniform for point pt (initial label draws, cudaKernel.cu:144-170).
+__device__ __forceinline__ float draw_uniform1(const RngArgs& r, int64_t pt)
+{
+    if (r.ucaller) return r.ucaller[pt];
+    if (r.kind == DPMM_RNG_CURAND_XORWOW) {
+        curandStateXORWOW st = r.states[pt];
+        float u = curand_uniform(&st);
+        r.states[pt] = st;
+        return u;
+    }
+    return u01_from_bits(philox_point(r, pt).v[0]);
+}
+
+// 32 random bits for point pt (the curand() of cudaKernel.cu:210, :252).
+__device__ __forceinline__ uint32_t draw_bits(const RngArgs& r, const uint32_t* bits, int64_t pt)
+{
+    if (bits) return bits[pt];
+    if (r.kind == DPMM_RNG_CURAND_XORWOW) {
+        curandStateXORWOW st = r.states[pt];
+        uint32_t v = curand(&st);
+        r.states[pt] = st;
+        return v;
+    }
+    return philox_point(r, pt).v[2];
+}
+
+// Column chosen by the first uniform: (int)(u1 * (n - 1 + 0.999999) + 1) evaluated in double
+// exactly as cudaKernel.cu:115 does (float uniform promoted to double).  For u1 in (0, 1] the
+// column is already in [1, n]; the clamp only keeps a caller's out-of-range uniform inside the table.
+__device__ __forceinline__ int alias_column(int n, float u1)
+{
+    int col = (int)((double)u1 * ((double)(n - 1) + 0.999999) + 1.0);
+    return col < 1 ? 1 : (col > n ? n : col);
+}
+
+// Walker alias construction + draw in the order of cudaKernel.cu:27-124.  The arrays are
+// accessed through an accessor so the same code serves shared-memory tables interleaved
+// across the points of a tile (index * stride + lane) and small per-thread arrays.
+// Preconditions: y(1..n) = p_i * n.  Indices 0..n+1 are used.  Returns the 1-based label.
+template <typename T, typename IdxT, typename Acc>
+__device__ __forceinline__ int alias_draw(int n, Acc acc, float u1, float u2)
+{
+    T* __restrict__ y = acc.y;
+    IdxT* __restrict__ a = acc.a;
+    IdxT* __restrict__ b = acc.b;
+    const int s = acc.stride;
+    for (int i = 0; i <= n + 1; ++i) {
+        a[i * s] = (IdxT)i;
+        b[i * s] = (IdxT)i;
+    }
+    y[0] = (T)0;
+    y[(n + 1) * s] = (T)2;
+    int i = 0, j = n + 1, t;
+    for (;;) {
+        do { i++; } while (y[(int)b[i * s] * s] < (T)1);
+        do { j--; } while ((T)1 <= y[(int)b[j * s] * s]);
+        if (j <= i) break;
+        t = b[i * s]; b[i * s] = b[j * s]; b[j * s] = (IdxT)t;
+    }
+    i = j;
+    j++;
+    while (0 < i) {
+        while (y[(int)b[j * s] * s] <= (T)1) j++;
+        if (n < j) break;
+        const int bj = b[j * s], bi = b[i * s];
+        y[bj * s] = y[bj * s] - ((T)1 - y[bi * s]);
+        a[bi * s] = (IdxT)bj;
+        if (y[bj * s] < (T)1) {
+            b[i * s] = (IdxT)bj;
+            b[j * s] = (IdxT)bi;
+            j++;
+        } else {
+            i--;
+        }
+    }
+    const int col = alias_column(n, u1);
+    int label = col;
+    if (y[col * s] < (T)u2) label = a[col * s];
+    return label;
+}
+
+template <typename T, typename IdxT>
+struct AliasAcc {
+    T* y;
+    IdxT* a;
+    IdxT* b;
+    int stride;
+};
+
+// Two-category draw used by the sub-cluster phase: the general construction with n = 2 on
+// a 4-entry table, with the reference's float->double promotions replaced by float maths.
+__device__ __forceinline__ int alias_draw2(float p1, float p2, float u1, float u2)
+{
+    float y[4];
+    uint8_t a[4], b[4];
+    y[1] = p1 * 2.0f;
+    y[2] = p2 * 2.0f;
+    AliasAcc<float, uint8_t> acc{y, a, b, 1};
+    return alias_draw<float, uint8_t>(2, acc, u1, u2);
+}
+
+}  // namespace dpmm

@@ -1,0 +1,199 @@
+// dpmm_internal.h -- context layout shared by the CUDA translation units and the C++ host
+// driver.  Not part of the public ABI (include/dpmm_capi.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/dpmm_capi.h"
+
+struct curandStateXORWOW;
+
+namespace dpmm {
+
+// Largest padded dimension of the Gaussian kernels (x held in registers per thread).
+constexpr int kMaxGaussDim = 128;
+// Largest dimension of the multinomial kernels (count vectors).
+constexpr int kMaxMultDim = 4096;
+// Points per chunk of the segmented (per-cluster) passes.
+constexpr int kChunk = 4096;
+
+int padded_dim(int d);  // 4, 8, 16, 32, 64, 128 (Gaussian); d rounded up to 32 (multinomial)
+
+// Thread-local error message for dpmm_last_error().
+void set_error(const std::string& msg);
+dpmm_status fail(dpmm_status s, const std::string& msg);
+dpmm_status cuda_status(cudaError_t e, const char* what);
+
+#define DPMM_CUDA_TRY(expr)                                              \
+    do {                                                                 \
+        cudaError_t _e = (expr);                                         \
+        if (_e != cudaSuccess) return ::dpmm::cuda_status(_e, #expr);    \
+    } while (0)
+
+// process-wide diagnostics: kernels launched, bytes copied host->device / device->host
+extern std::atomic<uint64_t> g_launches, g_h2d_bytes, g_d2h_bytes;
+
+#define DPMM_LAUNCHED()                                                        \
+    do {                                                                       \
+        ::dpmm::g_launches.fetch_add(1, std::memory_order_relaxed);            \
+        DPMM_CUDA_TRY(cudaGetLastError());                                     \
+    } while (0)
+
+enum Phase { PH_LABELS = 0, PH_SUB_STATS = 1, PH_STATS = 2, PH_SPLIT_HR = 3, PH_MERGE_HR = 4, PH_RELABEL = 5,
+             PH_PARAMS = 6, PH_COUNT = 8 };
+
+#define DPMM_TRY(expr)                         \
+    do {                                       \
+        dpmm_status _s = (expr);               \
+        if (_s != DPMM_OK) return _s;          \
+    } while (0)
+
+// How a phase obtains its uniforms.
+struct RngArgs {
+    int kind;                      // dpmm_rng_kind
+    uint64_t seed;
+    uint64_t ctr;                  // Philox draw counter (one per phase call)
+    curandStateXORWOW* states;     // per point (compat mode)
+    const float* ucaller;          // device copy of caller uniforms (or nullptr)
+};
+
+}  // namespace dpmm
+
+// Device-side state of one sampler.  All buffers are allocated at dpmm_create at capacity.
+struct dpmm_ctx {
+    int device = 0;
+    int64_t N = 0;
+    int D = 0;
+    int Dp = 0;                    // padded dimension used by the kernels
+    int prior = 0;
+    int k_max = 0;
+    int rng_kind = 0;
+    uint64_t seed = 0;
+    uint64_t philox_ctr = 0;
+    int ll_mode = 0;
+    int verbose = 0;
+    bool points_ready = false;
+    bool tc_ok = false;            // tensor-core kernel usable for this shape
+    cudaStream_t stream = nullptr;
+
+    // points: N x Dp row-major FP32.  Gaussian points are stored shifted by `shift`
+    // (their FP64 mean), which leaves every log-likelihood unchanged and keeps the FP32
+    // contraction and the scatter accumulation away from cancellation.
+    float* d_x = nullptr;
+    std::vector<double> shift;
+    double* d_gshift = nullptr;    // shift on the device (D doubles)
+
+    int32_t* d_labels = nullptr;
+    int32_t* d_sub = nullptr;
+    curandStateXORWOW* d_curand = nullptr;
+
+    // cluster parameters: 3 slots per cluster (3k: cluster, 3k+1: l, 3k+2: r)
+    int K_params = 0;
+    float* d_Wt = nullptr;         // [3*k_max][Dp][Dp], Wt[j][i] = W(i, j)  (Gaussian)
+    float* d_b = nullptr;          // [3*k_max][Dp], b = W^T (mu - shift)   (Gaussian)
+    float* d_c = nullptr;          // [3*k_max]: -logdet/2 + log w (slot 3k), -logdet/2 (sub slots);
+                                   // 0 for the multinomial prior (no weight term)
+    float* d_lrw = nullptr;        // [2*k_max] log lr_weights
+    float* d_mu = nullptr;         // [3*k_max][Dp], mu - shift (Gaussian) / log theta (multinomial)
+    std::vector<float> h_param_stage;
+
+    // label-ordered permutation of the points and the per-cluster chunk table
+    int nblk_hist = 0;
+    int32_t* d_perm = nullptr;
+    int32_t* d_blk_hist = nullptr; // [nblk_hist][k_max]
+    int32_t* d_seg = nullptr;      // [k_max + 1] segment starts
+    int32_t* d_chunk = nullptr;    // [max_chunks][3] (cluster, start, len)
+    int32_t* d_nchunks = nullptr;
+    int max_chunks = 0;
+    int perm_K = -1;               // K the permutation was built for (-1: stale)
+
+    // statistics: chunk partials (FP64) and per-slot results in original coordinates
+    double* d_part = nullptr;      // [max_chunks][2][stat_len]
+    double* d_stats = nullptr;     // [3*k_max][stat_len]: count, sum[D], S[D*D] (col-major)
+    int stat_len = 0;              // 1 + D + D*D (Gaussian) / 1 + D (multinomial)
+    int stats_K = -1;
+
+    // uniforms / random bits supplied by the caller, staged on the device
+    float* d_u = nullptr;          // 2N
+    uint32_t* d_bits = nullptr;    // N
+    int32_t* d_remap = nullptr;    // [k_max + 2] relabel table
+    int32_t* d_aux = nullptr;      // small scratch (counts)
+    double* d_r64 = nullptr;       // N doubles (FP64 test seams)
+    double* d_dbl_scratch = nullptr; // k_max-sized FP64 scratch
+
+    // priors + Hastings (FP64)
+    bool prior_set = false;
+    double prior_k = 0, prior_v = 0;
+    double prior_logdet = 0;       // log det psi0 (NIW)
+    double* d_prior = nullptr;     // NIW: m[D], psi[D*D]; multinomial: alpha[D]
+    double* d_lml = nullptr;       // [3*k_max]
+    double* d_split_hr = nullptr;  // [k_max]
+    double* d_merge_hr = nullptr;  // [k_max*k_max]
+    double* d_post_logdet = nullptr; // [3*k_max]
+    double* h_pinned = nullptr;    // pinned staging for D2H of results
+    size_t h_pinned_bytes = 0;
+
+    // events for phase timing (bench): device time per phase while `timing` is set
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool timing = false;
+    double phase_ms[dpmm::PH_COUNT] = {0};
+    int64_t phase_calls[dpmm::PH_COUNT] = {0};
+};
+
+namespace dpmm {
+// Records device time of one phase on the context's stream when timing is enabled.
+struct PhaseTimer {
+    dpmm_ctx* c;
+    int ph;
+    PhaseTimer(dpmm_ctx* ctx, int phase) : c(ctx), ph(phase)
+    {
+        if (c && c->timing) cudaEventRecord(c->ev0, c->stream);
+    }
+    ~PhaseTimer()
+    {
+        if (!c || !c->timing) return;
+        cudaEventRecord(c->ev1, c->stream);
+        if (cudaEventSynchronize(c->ev1) == cudaSuccess) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            c->phase_ms[ph] += ms;
+            c->phase_calls[ph] += 1;
+        }
+    }
+};
+}  // namespace dpmm
+
+namespace dpmm {
+// kernel launchers (dpmm_kernels.cu)
+dpmm_status launch_init_curand(dpmm_ctx* c);
+dpmm_status launch_labels_init(dpmm_ctx* c, int initial_clusters, double outlier_mod, const float* d_u);
+dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u);
+dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
+dpmm_status build_permutation(dpmm_ctx* c, int K);
+dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw);
+dpmm_status launch_stats_finalize(dpmm_ctx* c, int K);
+dpmm_status launch_relabel(dpmm_ctx* c, int mode, int K, const int32_t* h_table, int table_len,
+                           const uint32_t* d_bits);
+dpmm_status launch_sub_count(dpmm_ctx* c, int32_t* h_l, int32_t* h_r);
+dpmm_status launch_loglik_gauss_one(dpmm_ctx* c, double* d_r);
+dpmm_status launch_loglik_mult_one(dpmm_ctx* c, double* d_r);
+dpmm_status launch_sample_log_cat(dpmm_ctx* c, int K, const double* d_r, const float* d_u);
+dpmm_status launch_sample_log_cat_sub(dpmm_ctx* c, int m, const double* d_r, const int32_t* d_idx,
+                                      const double* d_lrw, const float* d_u);
+// Hastings (dpmm_hastings.cu)
+dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha);
+dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha);
+// tensor-core label kernel (dpmm_tc.cu); returns DPMM_ERR_INVALID_ARG when the shape is unsupported
+bool tc_supported(const dpmm_ctx* c, int K);
+dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
+
+RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
+// statistics of all points together (niw::create_sufficient_statistics over the whole data set)
+dpmm_status all_points_stats(dpmm_ctx* c, int64_t* count, double* sum, double* S);
+dpmm_status launch_fill_labels(dpmm_ctx* c, int32_t value);
+}  // namespace dpmm

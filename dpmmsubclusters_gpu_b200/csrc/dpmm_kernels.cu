@@ -1,0 +1,1001 @@
+// dpmm_kernels.cu -- SIMT kernels of the per-iteration path (the "plain FP32 form") and the
+// integer passes shared by every form: label-ordered permutation, fused sub-label draw +
+// segmented sufficient statistics, relabel passes, test seams.
+//
+// Reference correspondence (DPMMSubClusters/):
+//   k_gauss_labels_simt   cudaKernel_gaussian.cu:82-113 + cudaKernel.cu:374-403, 805-829, 27-124
+//                         (one kernel: K log-likelihood columns, softmax, alias draw / argmax)
+//   k_mult_labels_simt    cudaKernel_multinomial.cu:22-35, 60-76 + the same softmax/draw
+//   k_hist/k_scan/k_scatter  replace find_indices (cudaKernel.cu:189-200): a stable counting
+//                         sort of the points by label instead of K atomic compactions
+//   k_gauss_sub_stats     cudaKernel.cu:1299-1398 + cudaKernel_gaussian.cu:43-79 (sub-labels)
+//                         fused with cudaKernel.cu:844-941 + cudaKernel_gaussian.cu:126-168
+//   k_relabel             cudaKernel.cu:172-263 (split / merge / reset / remove)
+#include <algorithm>
+#include <vector>
+
+#include "dpmm_device.cuh"
+
+namespace dpmm {
+
+RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller)
+{
+    RngArgs r;
+    r.kind = c->rng_kind;
+    r.seed = c->seed;
+    r.ctr = c->philox_ctr++;
+    r.states = c->d_curand;
+    r.ucaller = d_ucaller;
+    return r;
+}
+
+static inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
+
+// ----------------------------------------------------------------------------- init draws
+__global__ void k_init_curand(curandStateXORWOW* st, uint64_t seed, int64_t n)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) curand_init(seed, (unsigned long long)i, 0, &st[i]);   // cudaKernel.cu:19-25
+}
+
+dpmm_status launch_init_curand(dpmm_ctx* c)
+{
+    k_init_curand<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(c->d_curand, c->seed, c->N);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+__global__ void k_labels_init(RngArgs r, int64_t n, int ic, int outlier, int32_t* labels)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float u = draw_uniform1(r, i);
+    // cudaKernel.cu:158-161
+    labels[i] = (int)((double)u * ((double)(ic - 1) + 0.999999) + 1.0 + (outlier ? 1.0 : 0.0));
+}
+
+__global__ void k_sub_labels_init(RngArgs r, int64_t n, int32_t* sub)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float u = draw_uniform1(r, i);
+    sub[i] = (int)((double)u * (2.0 - 1.0 + 0.999999) + 1.0);   // cudaKernel.cu:144-147
+}
+
+dpmm_status launch_labels_init(dpmm_ctx* c, int ic, double outlier_mod, const float* d_u)
+{
+    RngArgs r = rng_args(c, d_u);
+    k_labels_init<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(r, c->N, ic, outlier_mod > 0 ? 1 : 0, c->d_labels);
+    DPMM_LAUNCHED();
+    c->perm_K = -1;
+    return DPMM_OK;
+}
+
+dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u)
+{
+    RngArgs r = rng_args(c, d_u);
+    k_sub_labels_init<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(r, c->N, c->d_sub);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- label phase
+// Shared epilogue: r values of one point (stride P in shared memory) -> label.
+template <int P>
+__device__ __forceinline__ int draw_from_r(float* sr, uint16_t* sa, uint16_t* sb, int p, int K, int final_,
+                                           const RngArgs& rng, int64_t pt)
+{
+    if (final_) {
+        // update_labels_by_max_index_kernel (cudaKernel.cu:405-424): first maximum wins
+        float best = sr[p];
+        int arg = 0;
+        for (int k = 1; k < K; ++k) {
+            float v = sr[k * P + p];
+            if (best < v) { best = v; arg = k; }
+        }
+        return arg + 1;
+    }
+    // build_log_likelihood_array_kernel (cudaKernel.cu:374-403): max, exp, normalise
+    float mx = sr[p];
+    for (int k = 1; k < K; ++k) mx = fmaxf(mx, sr[k * P + p]);
+    float sum = 0.f;
+    for (int k = 0; k < K; ++k) {
+        float e = __expf(sr[k * P + p] - mx);
+        sr[k * P + p] = e;
+        sum += e;
+    }
+    const float inv = 1.0f / sum;
+    const float fk = (float)K;
+    // y[k+1] = p_k * K, written from the top so y[k+1] never overwrites an unread e[k+1]
+    for (int k = K - 1; k >= 0; --k) sr[(k + 1) * P + p] = (sr[k * P + p] * inv) * fk;
+    float u1, u2;
+    draw_uniform2(rng, pt, u1, u2);
+    AliasAcc<float, uint16_t> acc{sr + p, sa + p, sb + p, P};
+    return alias_draw<float, uint16_t>(K, acc, u1, u2);
+}
+
+// Gaussian label phase, FP32 SIMT: one thread per point, x in registers, each cluster's
+// precision factor (transposed) broadcast from shared memory.
+//   z_j = sum_i W(i,j) x_i - b_j,   r_k = c_k - 0.5 * sum_j z_j^2
+template <int DP, int P>
+__global__ void __launch_bounds__(P) k_gauss_labels_simt(
+    const float* __restrict__ x, int64_t N, const float* __restrict__ Wt, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, int K, int final_, RngArgs rng, int32_t* __restrict__ labels,
+    float* __restrict__ r_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* sW = reinterpret_cast<float*>(smem);          // DP*DP
+    float* sbv = sW + DP * DP;                            // DP
+    float* sx = sbv + DP;                                 // P*(DP+1)
+    float* sr = sx + P * (DP + 1);                        // (K+2)*P
+    uint16_t* sa = reinterpret_cast<uint16_t*>(sr + (size_t)(K + 2) * P);
+    uint16_t* sb = sa + (size_t)(K + 2) * P;
+
+    const int p = threadIdx.x;
+    const int64_t pt0 = (int64_t)blockIdx.x * P;
+    const int64_t pt = pt0 + p;
+    const bool valid = pt < N;
+
+    // stage the tile's points (contiguous rows) with coalesced loads
+    const int64_t rows = min((int64_t)P, N - pt0);
+    for (int e = p; e < P * DP; e += P) {
+        int pp = e / DP, i = e % DP;
+        sx[pp * (DP + 1) + i] = pp < rows ? x[(pt0 + pp) * DP + i] : 0.f;
+    }
+    __syncthreads();
+    float xr[DP];
+#pragma unroll
+    for (int i = 0; i < DP; ++i) xr[i] = sx[p * (DP + 1) + i];
+
+    for (int k = 0; k < K; ++k) {
+        __syncthreads();
+        const float4* src = reinterpret_cast<const float4*>(Wt + (size_t)3 * k * DP * DP);
+        float4* dst = reinterpret_cast<float4*>(sW);
+        for (int e = p; e < DP * DP / 4; e += P) dst[e] = src[e];
+        for (int e = p; e < DP; e += P) sbv[e] = bvec[(size_t)3 * k * DP + e];
+        __syncthreads();
+        float q = 0.f;
+#pragma unroll 2
+        for (int j = 0; j < DP; j += 2) {
+            const float4* w0 = reinterpret_cast<const float4*>(sW + j * DP);
+            const float4* w1 = reinterpret_cast<const float4*>(sW + (j + 1) * DP);
+            float z0 = -sbv[j], z1 = -sbv[j + 1];
+            float z0b = 0.f, z1b = 0.f;
+#pragma unroll
+            for (int i4 = 0; i4 < DP / 4; ++i4) {
+                float4 a = w0[i4], b = w1[i4];
+                z0 = fmaf(a.x, xr[4 * i4 + 0], z0);
+                z1 = fmaf(b.x, xr[4 * i4 + 0], z1);
+                z0b = fmaf(a.y, xr[4 * i4 + 1], z0b);
+                z1b = fmaf(b.y, xr[4 * i4 + 1], z1b);
+                z0 = fmaf(a.z, xr[4 * i4 + 2], z0);
+                z1 = fmaf(b.z, xr[4 * i4 + 2], z1);
+                z0b = fmaf(a.w, xr[4 * i4 + 3], z0b);
+                z1b = fmaf(b.w, xr[4 * i4 + 3], z1b);
+            }
+            z0 += z0b;
+            z1 += z1b;
+            q = fmaf(z0, z0, q);
+            q = fmaf(z1, z1, q);
+        }
+        const float r = cvec[3 * k] - 0.5f * q;
+        sr[k * P + p] = r;
+        if (r_out && valid) r_out[pt * K + k] = r;
+    }
+    if (!valid) return;
+    labels[pt] = draw_from_r<P>(sr, sa, sb, p, K, final_, rng, pt);
+}
+
+// Multinomial label phase, FP32 SIMT: tiled dot products r[p][k] = sum_d x[p][d] * logtheta[k][d]
+// (64 points x 64 clusters per pass, 256 threads, 4x4 register tile), then the same draw.
+template <int P>
+__global__ void __launch_bounds__(256) k_mult_labels_simt(
+    const float* __restrict__ x, int64_t N, int Dp, const float* __restrict__ logtheta,
+    int K, int final_, RngArgs rng, int32_t* __restrict__ labels, float* __restrict__ r_out)
+{
+    constexpr int KG = 64, DC = 32;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* sX = reinterpret_cast<float*>(smem);          // P x (DC+1)
+    float* sT = sX + P * (DC + 1);                        // KG x (DC+1)
+    float* sr = sT + KG * (DC + 1);                       // (K+2)*P
+    uint16_t* sa = reinterpret_cast<uint16_t*>(sr + (size_t)(K + 2) * P);
+    uint16_t* sb = sa + (size_t)(K + 2) * P;
+
+    const int tid = threadIdx.x;
+    const int64_t pt0 = (int64_t)blockIdx.x * P;
+    const int64_t rows = min((int64_t)P, N - pt0);
+    const int tp = tid / 16, tk = tid % 16;              // 16 x 16 thread grid, 4 x 4 outputs each
+
+    for (int g = 0; g < K; g += KG) {
+        float acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+        for (int d0 = 0; d0 < Dp; d0 += DC) {
+            __syncthreads();
+            for (int e = tid; e < P * DC; e += 256) {
+                int pp = e / DC, dd = e % DC;
+                sX[pp * (DC + 1) + dd] = pp < rows ? x[(pt0 + pp) * Dp + d0 + dd] : 0.f;
+            }
+            for (int e = tid; e < KG * DC; e += 256) {
+                int kk = e / DC, dd = e % DC;
+                sT[kk * (DC + 1) + dd] = (g + kk) < K ? logtheta[(size_t)3 * (g + kk) * Dp + d0 + dd] : 0.f;
+            }
+            __syncthreads();
+#pragma unroll 8
+            for (int dd = 0; dd < DC; ++dd) {
+                float xv[4], tv[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) xv[a] = sX[(tp + 16 * a) * (DC + 1) + dd];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) tv[b] = sT[(tk + 16 * b) * (DC + 1) + dd];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(xv[a], tv[b], acc[a][b]);
+            }
+        }
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                int pp = tp + 16 * a, kk = g + tk + 16 * b;
+                if (kk < K) {
+                    sr[kk * P + pp] = acc[a][b];
+                    if (r_out && pp < rows) r_out[(pt0 + pp) * K + kk] = acc[a][b];
+                }
+            }
+    }
+    __syncthreads();
+    if (tid >= P || tid >= rows) return;
+    const int64_t pt = pt0 + tid;
+    labels[pt] = draw_from_r<P>(sr, sa, sb, tid, K, final_, rng, pt);
+}
+
+template <int DP, int P>
+static dpmm_status launch_gauss_labels_t(dpmm_ctx* c, int K, int final_, RngArgs r, float* d_rout)
+{
+    size_t sm = sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)(K + 2) * P) +
+                sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
+    auto kern = k_gauss_labels_simt<DP, P>;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<blocks_for(c->N, P), P, sm, c->stream>>>(c->d_x, c->N, c->d_Wt, c->d_b, c->d_c, K, final_, r,
+                                                     c->d_labels, d_rout);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+static size_t gauss_label_smem(int DP, int P, int K)
+{
+    return sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)(K + 2) * P) +
+           sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
+}
+
+template <int DP>
+static dpmm_status launch_gauss_labels_dp(dpmm_ctx* c, int K, int final_, RngArgs r, float* d_rout)
+{
+    const size_t cap = 220 * 1024;
+    if (gauss_label_smem(DP, 128, K) <= cap) return launch_gauss_labels_t<DP, 128>(c, K, final_, r, d_rout);
+    if (gauss_label_smem(DP, 64, K) <= cap) return launch_gauss_labels_t<DP, 64>(c, K, final_, r, d_rout);
+    if (gauss_label_smem(DP, 32, K) <= cap) return launch_gauss_labels_t<DP, 32>(c, K, final_, r, d_rout);
+    return fail(DPMM_ERR_INVALID_ARG, "too many clusters for the label kernel's shared-memory table");
+}
+
+dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout)
+{
+    RngArgs r = rng_args(c, d_u);
+    if (c->prior == DPMM_PRIOR_GAUSSIAN) {
+        switch (c->Dp) {
+            case 4: return launch_gauss_labels_dp<4>(c, K, final_, r, d_rout);
+            case 8: return launch_gauss_labels_dp<8>(c, K, final_, r, d_rout);
+            case 16: return launch_gauss_labels_dp<16>(c, K, final_, r, d_rout);
+            case 32: return launch_gauss_labels_dp<32>(c, K, final_, r, d_rout);
+            case 64: return launch_gauss_labels_dp<64>(c, K, final_, r, d_rout);
+            case 128: return launch_gauss_labels_dp<128>(c, K, final_, r, d_rout);
+            default: return fail(DPMM_ERR_INVALID_ARG, "unsupported padded dimension");
+        }
+    }
+    constexpr int P = 64;
+    size_t sm = sizeof(float) * (P * 33 + 64 * 33 + (size_t)(K + 2) * P) + sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
+    if (sm > 220 * 1024) return fail(DPMM_ERR_INVALID_ARG, "too many clusters for the multinomial label kernel");
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(k_mult_labels_simt<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_mult_labels_simt<P><<<blocks_for(c->N, P), 256, sm, c->stream>>>(c->d_x, c->N, c->Dp, c->d_mu, K, final_, r,
+                                                                       c->d_labels, d_rout);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- permutation
+// Stable counting sort of the points by label.  Bin K collects labels outside 1..K.
+constexpr int kHistBlock = 2048;   // points per histogram block (256 threads x 8)
+
+__device__ __forceinline__ int label_bin(int32_t lab, int K) { return (lab >= 1 && lab <= K) ? lab - 1 : K; }
+
+__global__ void k_hist(const int32_t* __restrict__ labels, int64_t N, int K, int32_t* __restrict__ blk_hist)
+{
+    extern __shared__ int32_t sh[];
+    for (int k = threadIdx.x; k <= K; k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kHistBlock;
+    for (int it = 0; it < kHistBlock / 256; ++it) {
+        int64_t pt = base + it * 256 + threadIdx.x;
+        if (pt < N) atomicAdd(&sh[label_bin(labels[pt], K)], 1);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k <= K; k += blockDim.x) blk_hist[(size_t)blockIdx.x * (K + 1) + k] = sh[k];
+}
+
+// one block per bin: exclusive scan over histogram blocks, in place; total into seg_tmp[k]
+__global__ void k_scan_bins(int32_t* __restrict__ blk_hist, int nblk, int K, int32_t* __restrict__ total)
+{
+    const int k = blockIdx.x;
+    __shared__ int32_t warp_sums[32];
+    __shared__ int32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int b0 = 0; b0 < nblk; b0 += blockDim.x) {
+        int b = b0 + threadIdx.x;
+        int v = b < nblk ? blk_hist[(size_t)b * (K + 1) + k] : 0;
+        // block-wide inclusive scan
+        int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        int s = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int t = __shfl_up_sync(0xffffffffu, s, o);
+            if (lane >= o) s += t;
+        }
+        if (lane == 31) warp_sums[w] = s;
+        __syncthreads();
+        if (w == 0) {
+            int ws = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int t = __shfl_up_sync(0xffffffffu, ws, o);
+                if (lane >= o) ws += t;
+            }
+            warp_sums[lane] = ws;
+        }
+        __syncthreads();
+        int incl = s + (w > 0 ? warp_sums[w - 1] : 0);
+        if (b < nblk) blk_hist[(size_t)b * (K + 1) + k] = carry + incl - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry += incl;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) total[k] = carry;
+}
+
+// single block: segment starts and the chunk table (cluster, start, len) of <= kChunk points
+__global__ void k_segments(const int32_t* __restrict__ total, int K, int32_t* __restrict__ seg,
+                           int32_t* __restrict__ chunk, int32_t* __restrict__ nchunks, int max_chunks)
+{
+    if (threadIdx.x != 0) return;
+    int32_t acc = 0, nc = 0;
+    for (int k = 0; k <= K; ++k) {
+        seg[k] = acc;
+        int32_t t = total[k];
+        if (k < K) {
+            for (int32_t s = 0; s < t && nc < max_chunks; s += kChunk) {
+                chunk[3 * nc + 0] = k;
+                chunk[3 * nc + 1] = acc + s;
+                chunk[3 * nc + 2] = min(kChunk, t - s);
+                ++nc;
+            }
+        }
+        acc += t;
+    }
+    seg[K + 1] = acc;
+    *nchunks = nc;
+}
+
+__global__ void k_scatter(const int32_t* __restrict__ labels, int64_t N, int K, const int32_t* __restrict__ blk_off,
+                          const int32_t* __restrict__ seg, int32_t* __restrict__ perm)
+{
+    extern __shared__ int32_t sh[];
+    int32_t* run = sh;                 // K+1
+    int32_t* wcnt = sh + (K + 1);      // 8 x (K+1)
+    for (int k = threadIdx.x; k < 9 * (K + 1); k += blockDim.x) sh[k] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t base = (int64_t)blockIdx.x * kHistBlock;
+    for (int it = 0; it < kHistBlock / 256; ++it) {
+        const int64_t pt = base + it * 256 + threadIdx.x;
+        const int bin = pt < N ? label_bin(labels[pt], K) : -1;
+        const unsigned peers = __match_any_sync(0xffffffffu, bin);
+        const int rank = __popc(peers & lt);
+        if (rank == 0 && bin >= 0) wcnt[w * (K + 1) + bin] = __popc(peers);
+        __syncthreads();
+        if (bin >= 0) {
+            int before = run[bin];
+            for (int v = 0; v < w; ++v) before += wcnt[v * (K + 1) + bin];
+            perm[seg[bin] + blk_off[(size_t)blockIdx.x * (K + 1) + bin] + before + rank] = (int32_t)pt;
+        }
+        __syncthreads();
+        if (rank == 0 && bin >= 0) {
+            atomicAdd(&run[bin], __popc(peers));
+            wcnt[w * (K + 1) + bin] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+dpmm_status build_permutation(dpmm_ctx* c, int K)
+{
+    const int nblk = blocks_for(c->N, kHistBlock);
+    if (nblk > c->nblk_hist || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "permutation capacity exceeded");
+    k_hist<<<nblk, 256, sizeof(int32_t) * (K + 1), c->stream>>>(c->d_labels, c->N, K, c->d_blk_hist);
+    DPMM_LAUNCHED();
+    int32_t* total = c->d_aux + 8;   // K+1 entries
+    k_scan_bins<<<K + 1, 1024, 0, c->stream>>>(c->d_blk_hist, nblk, K, total);
+    DPMM_LAUNCHED();
+    k_segments<<<1, 32, 0, c->stream>>>(total, K, c->d_seg, c->d_chunk, c->d_nchunks, c->max_chunks);
+    DPMM_LAUNCHED();
+    size_t sm = sizeof(int32_t) * 9 * (K + 1);
+    if (sm > 48 * 1024) DPMM_CUDA_TRY(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_scatter<<<nblk, 256, sm, c->stream>>>(c->d_labels, c->N, K, c->d_blk_hist, c->d_seg, c->d_perm);
+    DPMM_LAUNCHED();
+    c->perm_K = K;
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- sub-labels + stats
+// Upper-triangle pair count of the scatter matrix
+__host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
+
+// Gaussian: one block per chunk of one cluster (points in permutation order).  Draws the
+// sub-labels (unless draw == 0, in which case the current sub-labels are used) and accumulates
+// per sub-cluster: count, sum(x - s) and the upper triangle of sum (x - s)(x - s)^T, shift
+// s = the cluster's mean parameter.  FP32 products, FP32 runs of 32 points, FP64 totals.
+template <int DP, int TP>
+__global__ void __launch_bounds__(256) k_gauss_sub_stats(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const float* __restrict__ Wt, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, const float* __restrict__ lrw, const float* __restrict__ muv, int draw,
+    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part)
+{
+    constexpr int T = tri(DP);
+    constexpr int E = (T + 255) / 256;       // scatter entries per thread
+    constexpr int SL = 1 + DP + T;            // partial record length per sub-cluster
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* sWl = reinterpret_cast<float*>(smem);   // DP*DP
+    float* sWr = sWl + DP * DP;                    // DP*DP
+    float* sbl = sWr + DP * DP;                    // DP
+    float* sbr = sbl + DP;                         // DP
+    float* ss = sbr + DP;                          // DP (shift)
+    float* sx = ss + DP;                           // TP*(DP+1)
+    int32_t* ssub = reinterpret_cast<int32_t*>(sx + TP * (DP + 1));   // TP
+    uint16_t* spair = reinterpret_cast<uint16_t*>(ssub + TP);         // T (i<<8 | j)
+
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    const int tid = threadIdx.x;
+
+    if (draw) {
+        const float4* wl = reinterpret_cast<const float4*>(Wt + (size_t)(3 * k + 1) * DP * DP);
+        const float4* wr = reinterpret_cast<const float4*>(Wt + (size_t)(3 * k + 2) * DP * DP);
+        for (int e = tid; e < DP * DP / 4; e += 256) {
+            reinterpret_cast<float4*>(sWl)[e] = wl[e];
+            reinterpret_cast<float4*>(sWr)[e] = wr[e];
+        }
+        for (int e = tid; e < DP; e += 256) {
+            sbl[e] = bvec[(size_t)(3 * k + 1) * DP + e];
+            sbr[e] = bvec[(size_t)(3 * k + 2) * DP + e];
+        }
+    }
+    for (int e = tid; e < DP; e += 256) ss[e] = muv[(size_t)(3 * k) * DP + e];
+    for (int e = tid; e < T; e += 256) {
+        // row-major upper triangle: (i, j), i <= j
+        int i = 0, rem = e;
+        while (rem >= DP - i) { rem -= DP - i; ++i; }
+        spair[e] = (uint16_t)((i << 8) | (i + rem));
+    }
+    const float cl = draw ? cvec[3 * k + 1] : 0.f, cr = draw ? cvec[3 * k + 2] : 0.f;
+    const float wl = draw ? lrw[2 * k] : 0.f, wr = draw ? lrw[2 * k + 1] : 0.f;
+
+    float accf[2][E];
+    double accd[2][E];
+#pragma unroll
+    for (int s = 0; s < 2; ++s)
+#pragma unroll
+        for (int m = 0; m < E; ++m) { accf[s][m] = 0.f; accd[s][m] = 0.0; }
+    // sums: threads [0, DP) -> l, [DP, 2DP) -> r
+    float sumf = 0.f;
+    double sumd = 0.0;
+    int cnt_l = 0, cnt_r = 0;
+
+    for (int t0 = 0; t0 < len; t0 += TP) {
+        const int nt = min(TP, len - t0);
+        __syncthreads();
+        for (int e = tid; e < TP * DP; e += 256) {
+            int pp = e / DP, i = e % DP;
+            sx[pp * (DP + 1) + i] = pp < nt ? x[(size_t)perm[start + t0 + pp] * DP + i] : 0.f;
+        }
+        __syncthreads();
+        if (tid < nt) {
+            const int64_t pt = perm[start + t0 + tid];
+            int sv;
+            if (draw) {
+                float ql = 0.f, qr = 0.f;
+                const float* xp = sx + tid * (DP + 1);
+                for (int j = 0; j < DP; ++j) {
+                    const float* wl = sWl + j * DP;
+                    const float* wr = sWr + j * DP;
+                    float zl = -sbl[j], zr = -sbr[j];
+#pragma unroll 8
+                    for (int i = 0; i < DP; ++i) {
+                        float xv = xp[i];
+                        zl = fmaf(wl[i], xv, zl);
+                        zr = fmaf(wr[i], xv, zr);
+                    }
+                    ql = fmaf(zl, zl, ql);
+                    qr = fmaf(zr, zr, qr);
+                }
+                float rl = cl - 0.5f * ql, rr = cr - 0.5f * qr;
+                if (r_out) { r_out[2 * pt] = rl; r_out[2 * pt + 1] = rr; }
+                // + log lr_weights, then the 2-way softmax (cudaKernel.cu:352-372)
+                rl += wl;
+                rr += wr;
+                float mx = fmaxf(rl, rr);
+                float el = __expf(rl - mx), er = __expf(rr - mx);
+                float s = el + er;
+                float u1, u2;
+                draw_uniform2(rng, pt, u1, u2);
+                sv = alias_draw2(el / s, er / s, u1, u2);
+                sub[pt] = sv;
+            } else {
+                sv = sub[pt];
+            }
+            ssub[tid] = sv;
+        }
+        __syncthreads();
+        for (int e = tid; e < nt * DP; e += 256) {
+            int pp = e / DP, i = e % DP;
+            sx[pp * (DP + 1) + i] -= ss[i];
+        }
+        __syncthreads();
+        for (int pp = 0; pp < nt; ++pp) {
+            const int sv = ssub[pp];
+            if (sv != 1 && sv != 2) continue;
+            const float* xp = sx + pp * (DP + 1);
+            if (sv == 1) {
+                ++cnt_l;
+#pragma unroll
+                for (int m = 0; m < E; ++m) {
+                    int e = tid + 256 * m;
+                    if (e < T) {
+                        uint16_t pr = spair[e];
+                        int i = pr >> 8, j = pr & 0xff;
+                        accf[0][m] = fmaf(xp[i], xp[j], accf[0][m]);
+                    }
+                }
+                if (tid < DP) sumf += xp[tid];
+            } else {
+                ++cnt_r;
+#pragma unroll
+                for (int m = 0; m < E; ++m) {
+                    int e = tid + 256 * m;
+                    if (e < T) {
+                        uint16_t pr = spair[e];
+                        int i = pr >> 8, j = pr & 0xff;
+                        accf[1][m] = fmaf(xp[i], xp[j], accf[1][m]);
+                    }
+                }
+                if (tid >= DP && tid < 2 * DP) sumf += xp[tid - DP];
+            }
+            if ((pp & 31) == 31) {
+#pragma unroll
+                for (int s = 0; s < 2; ++s)
+#pragma unroll
+                    for (int m = 0; m < E; ++m) { accd[s][m] += (double)accf[s][m]; accf[s][m] = 0.f; }
+                sumd += (double)sumf;
+                sumf = 0.f;
+            }
+        }
+#pragma unroll
+        for (int s = 0; s < 2; ++s)
+#pragma unroll
+            for (int m = 0; m < E; ++m) { accd[s][m] += (double)accf[s][m]; accf[s][m] = 0.f; }
+        sumd += (double)sumf;
+        sumf = 0.f;
+    }
+    double* pl = part + (size_t)ch * 2 * SL;
+    double* pr = pl + SL;
+    if (tid == 0) { pl[0] = (double)cnt_l; pr[0] = (double)cnt_r; }
+    if (tid < DP) pl[1 + tid] = sumd;
+    else if (tid < 2 * DP) pr[1 + tid - DP] = sumd;
+#pragma unroll
+    for (int m = 0; m < E; ++m) {
+        int e = tid + 256 * m;
+        if (e < T) { pl[1 + DP + e] = accd[0][m]; pr[1 + DP + e] = accd[1][m]; }
+    }
+}
+
+// Multinomial: warp per point; sub-label from two dot products with log theta_l / log theta_r,
+// count sums accumulated with shared-memory float atomics (exact for integer counts while a
+// chunk's per-category sum stays below 2^24).
+__global__ void __launch_bounds__(256) k_mult_sub_stats(
+    const float* __restrict__ x, int Dp, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const float* __restrict__ logtheta, const float* __restrict__ lrw, int draw,
+    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part, int SL)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* tl = reinterpret_cast<float*>(smem);   // Dp
+    float* tr = tl + Dp;                          // Dp
+    float* accl = tr + Dp;                        // Dp
+    float* accr = accl + Dp;                      // Dp
+    __shared__ int cnt[2];
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    for (int e = tid; e < Dp; e += 256) {
+        tl[e] = logtheta[(size_t)(3 * k + 1) * Dp + e];
+        tr[e] = logtheta[(size_t)(3 * k + 2) * Dp + e];
+        accl[e] = 0.f;
+        accr[e] = 0.f;
+    }
+    if (tid < 2) cnt[tid] = 0;
+    __syncthreads();
+    const float wl = lrw[2 * k], wr = lrw[2 * k + 1];
+    for (int pp = w; pp < len; pp += 8) {
+        const int64_t pt = perm[start + pp];
+        const float* xp = x + (size_t)pt * Dp;
+        int sv = 0;
+        if (draw) {
+            float dl = 0.f, dr = 0.f;
+            for (int d = lane; d < Dp; d += 32) {
+                float v = xp[d];
+                dl = fmaf(v, tl[d], dl);
+                dr = fmaf(v, tr[d], dr);
+            }
+#pragma unroll
+            for (int o = 16; o; o >>= 1) {
+                dl += __shfl_xor_sync(0xffffffffu, dl, o);
+                dr += __shfl_xor_sync(0xffffffffu, dr, o);
+            }
+            if (lane == 0) {
+                float rl = dl + wl, rr = dr + wr;
+                if (r_out) { r_out[2 * pt] = dl; r_out[2 * pt + 1] = dr; }
+                float mx = fmaxf(rl, rr);
+                float el = __expf(rl - mx), er = __expf(rr - mx);
+                float s = el + er;
+                float u1, u2;
+                draw_uniform2(rng, pt, u1, u2);
+                sv = alias_draw2(el / s, er / s, u1, u2);
+                sub[pt] = sv;
+            }
+            sv = __shfl_sync(0xffffffffu, lane == 0 ? sv : 0, 0);
+        } else {
+            sv = sub[pt];
+        }
+        if (sv == 1 || sv == 2) {
+            float* acc = sv == 1 ? accl : accr;
+            for (int d = lane; d < Dp; d += 32) atomicAdd(&acc[d], xp[d]);
+            if (lane == 0) atomicAdd(&cnt[sv - 1], 1);
+        }
+    }
+    __syncthreads();
+    double* pl = part + (size_t)ch * 2 * SL;
+    double* pr = pl + SL;
+    if (tid == 0) { pl[0] = cnt[0]; pr[0] = cnt[1]; }
+    for (int e = tid; e < Dp; e += 256) { pl[1 + e] = accl[e]; pr[1 + e] = accr[e]; }
+}
+
+template <int DP>
+static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout)
+{
+    constexpr int TP = DP >= 128 ? 128 : 256;
+    size_t sm = sizeof(float) * (2 * DP * DP + 3 * DP + TP * (DP + 1)) + sizeof(int32_t) * TP +
+                sizeof(uint16_t) * tri(DP);
+    auto kern = k_gauss_sub_stats<DP, TP>;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c,
+                                                c->d_lrw, c->d_mu, draw, r, c->d_sub, d_rout, c->d_part);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw)
+{
+    if (c->perm_K != K) DPMM_TRY(build_permutation(c, K));
+    RngArgs r = rng_args(c, d_u);
+    if (c->prior == DPMM_PRIOR_GAUSSIAN) {
+        switch (c->Dp) {
+            case 4: DPMM_TRY(launch_gauss_sub_stats_t<4>(c, draw, r, d_rout)); break;
+            case 8: DPMM_TRY(launch_gauss_sub_stats_t<8>(c, draw, r, d_rout)); break;
+            case 16: DPMM_TRY(launch_gauss_sub_stats_t<16>(c, draw, r, d_rout)); break;
+            case 32: DPMM_TRY(launch_gauss_sub_stats_t<32>(c, draw, r, d_rout)); break;
+            case 64: DPMM_TRY(launch_gauss_sub_stats_t<64>(c, draw, r, d_rout)); break;
+            case 128: DPMM_TRY(launch_gauss_sub_stats_t<128>(c, draw, r, d_rout)); break;
+            default: return fail(DPMM_ERR_INVALID_ARG, "unsupported padded dimension");
+        }
+    } else {
+        size_t sm = sizeof(float) * 4 * c->Dp;
+        if (sm > 48 * 1024)
+            DPMM_CUDA_TRY(cudaFuncSetAttribute(k_mult_sub_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_mult_sub_stats<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->Dp, c->d_perm, c->d_chunk, c->d_nchunks,
+                                                                 c->d_mu, c->d_lrw, draw ? 1 : 0, r, c->d_sub, d_rout,
+                                                                 c->d_part, 1 + c->Dp);
+        DPMM_LAUNCHED();
+    }
+    return launch_stats_finalize(c, K);
+}
+
+// One block per cluster: chunk partials summed in chunk order (FP64), shifted back to the
+// original coordinates, written as count / sum / full S for slots 3k (cluster = l + r),
+// 3k+1 (l), 3k+2 (r).
+__global__ void k_stats_finalize(const double* __restrict__ part, const int32_t* __restrict__ chunk,
+                                 const int32_t* __restrict__ nchunks, const float* __restrict__ muv,
+                                 const double* __restrict__ gshift, int D, int Dp, int gauss, int SL, int out_len,
+                                 double* __restrict__ stats)
+{
+    const int k = blockIdx.x;
+    const int nc = *nchunks;
+    // first chunk of this cluster (chunks are ordered by cluster)
+    int lo = 0, hi = nc;
+    while (lo < hi) {
+        int mid = (lo + hi) / 2;
+        if (chunk[3 * mid] < k) lo = mid + 1; else hi = mid;
+    }
+    const int c0 = lo;
+    int c1 = c0;
+    while (c1 < nc && chunk[3 * c1] == k) ++c1;
+    const int T = gauss ? Dp * (Dp + 1) / 2 : 0;
+    extern __shared__ double shd[];
+    double* n2 = shd;                 // [2]
+    double* sm2 = shd + 2;            // [2][D]
+    double* t = sm2 + 2 * D;          // [D] total shift (gauss)
+    for (int s = 0; s < 2; ++s) {
+        for (int e = threadIdx.x; e < 1 + D; e += blockDim.x) {
+            double acc = 0.0;
+            for (int q = c0; q < c1; ++q) acc += part[((size_t)q * 2 + s) * SL + e];
+            if (e == 0) n2[s] = acc; else sm2[s * D + e - 1] = acc;
+        }
+    }
+    if (gauss)
+        for (int e = threadIdx.x; e < D; e += blockDim.x) t[e] = (double)muv[(size_t)3 * k * Dp + e] + gshift[e];
+    __syncthreads();
+    double* out_c = stats + (size_t)(3 * k) * out_len;
+    double* out_l = out_c + out_len;
+    double* out_r = out_l + out_len;
+    if (threadIdx.x == 0) {
+        out_l[0] = n2[0];
+        out_r[0] = n2[1];
+        out_c[0] = n2[0] + n2[1];
+    }
+    for (int e = threadIdx.x; e < D; e += blockDim.x) {
+        double sl = sm2[e], sr = sm2[D + e];
+        if (gauss) { sl += n2[0] * t[e]; sr += n2[1] * t[e]; }
+        out_l[1 + e] = sl;
+        out_r[1 + e] = sr;
+        out_c[1 + e] = sl + sr;
+    }
+    if (!gauss) return;
+    // S = Sc + t Sc_sum^T + Sc_sum t^T + n t t^T, with Sc_sum = sum (x - t)
+    for (int e = threadIdx.x; e < T; e += blockDim.x) {
+        int i = 0, rem = e;
+        while (rem >= Dp - i) { rem -= Dp - i; ++i; }
+        int j = i + rem;
+        if (i >= D || j >= D) continue;
+        double v[2];
+        for (int s = 0; s < 2; ++s) {
+            double acc = 0.0;
+            for (int q = c0; q < c1; ++q) acc += part[((size_t)q * 2 + s) * SL + 1 + Dp + e];
+            double si = sm2[s * D + i], sj = sm2[s * D + j];
+            v[s] = acc + t[i] * sj + si * t[j] + n2[s] * t[i] * t[j];
+        }
+        size_t ij = 1 + D + (size_t)j * D + i, ji = 1 + D + (size_t)i * D + j;
+        out_l[ij] = v[0]; out_l[ji] = v[0];
+        out_r[ij] = v[1]; out_r[ji] = v[1];
+        out_c[ij] = v[0] + v[1]; out_c[ji] = v[0] + v[1];
+    }
+}
+
+dpmm_status launch_stats_finalize(dpmm_ctx* c, int K)
+{
+    const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    const int SL = gauss ? 1 + c->Dp + tri(c->Dp) : 1 + c->Dp;
+    size_t sm = sizeof(double) * (2 + 3 * (size_t)c->D);
+    if (sm > 48 * 1024)
+        DPMM_CUDA_TRY(cudaFuncSetAttribute(k_stats_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_stats_finalize<<<K, 256, sm, c->stream>>>(c->d_part, c->d_chunk, c->d_nchunks, c->d_mu, c->d_gshift, c->D,
+                                                c->Dp, gauss, SL, c->stat_len, c->d_stats);
+    DPMM_LAUNCHED();
+    c->stats_K = K;
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- relabels
+// mode 0 split:  table[l] = new 1-based label (0: not split); sub==2 moves; fresh sub-label
+// mode 1 merge:  table[l] = 1: becomes sub 1;  table[l] = -m (m = 1-based target): sub 2, label m
+// mode 2 reset:  table[l] != 0: fresh sub-label
+// mode 3 remap:  label = table[label]
+__global__ void k_relabel(int mode, int64_t N, int tlen, const int32_t* __restrict__ table, RngArgs rng,
+                          const uint32_t* __restrict__ bits, int32_t* __restrict__ labels, int32_t* __restrict__ sub)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    int lab = labels[i];
+    if (lab < 0 || lab >= tlen) return;
+    int t = table[lab];
+    switch (mode) {
+        case 0:
+            if (t != 0) {
+                if (sub[i] == 2) labels[i] = t;
+                sub[i] = (int)(draw_bits(rng, bits, i) % 2u + 1u);   // cudaKernel.cu:202-212
+            }
+            break;
+        case 1:
+            if (t == 1) sub[i] = 1;                                  // cudaKernel.cu:223-237
+            else if (t < 0) { sub[i] = 2; labels[i] = -t; }
+            break;
+        case 2:
+            if (t != 0) sub[i] = (int)(draw_bits(rng, bits, i) % 2u + 1u);   // cudaKernel.cu:248-254
+            break;
+        default:
+            labels[i] = t;                                           // cudaKernel.cu:172-178
+    }
+}
+
+dpmm_status launch_relabel(dpmm_ctx* c, int mode, int K, const int32_t* h_table, int tlen, const uint32_t* d_bits)
+{
+    (void)K;
+    if (tlen > c->k_max + 2) return fail(DPMM_ERR_INVALID_ARG, "relabel table larger than capacity");
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_remap, h_table, sizeof(int32_t) * tlen, cudaMemcpyHostToDevice, c->stream));
+    RngArgs r = rng_args(c, nullptr);
+    k_relabel<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(mode, c->N, tlen, c->d_remap, r, d_bits, c->d_labels,
+                                                             c->d_sub);
+    DPMM_LAUNCHED();
+    c->perm_K = -1;
+    return DPMM_OK;
+}
+
+__global__ void k_sub_count(const int32_t* __restrict__ sub, int64_t N, int32_t* __restrict__ out)
+{
+    int a = 0, b = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        int s = sub[i];
+        a += s == 1;
+        b += s == 2;
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(&out[0], a);
+        atomicAdd(&out[1], b);
+    }
+}
+
+dpmm_status launch_sub_count(dpmm_ctx* c, int32_t* h_l, int32_t* h_r)
+{
+    DPMM_CUDA_TRY(cudaMemsetAsync(c->d_aux, 0, 2 * sizeof(int32_t), c->stream));
+    k_sub_count<<<148 * 4, 256, 0, c->stream>>>(c->d_sub, c->N, c->d_aux);
+    DPMM_LAUNCHED();
+    int32_t h[2];
+    DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_aux, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    *h_l = h[0];
+    *h_r = h[1];
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- FP64 test seams
+// cudaKernel_gaussian::log_likelihood_labels for one cluster in FP64 (parameters in d_dbl_scratch:
+// mu[D], inv_sigma[D*D] col-major, scalar, log weight)
+__global__ void k_loglik_gauss_one(const float* __restrict__ x, int64_t N, int D, int Dp, const double* __restrict__ gshift,
+                                   const double* __restrict__ prm, double* __restrict__ r)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    const double* mu = prm;
+    const double* is = prm + D;
+    const double scalar = prm[D + D * D], logw = prm[D + D * D + 1];
+    double z[kMaxGaussDim];
+    for (int j = 0; j < D; ++j) z[j] = ((double)x[p * Dp + j] + gshift[j]) - mu[j];
+    double sum = 0;
+    for (int i = 0; i < D; ++i) {
+        double cc = 0;
+        for (int j = 0; j < D; ++j) cc += is[(size_t)j * D + i] * z[j];
+        sum += z[i] * cc;
+    }
+    r[p] = scalar - sum / 2 + logw;
+}
+
+dpmm_status launch_loglik_gauss_one(dpmm_ctx* c, double* d_r)
+{
+    k_loglik_gauss_one<<<blocks_for(c->N, 128), 128, 0, c->stream>>>(c->d_x, c->N, c->D, c->Dp, c->d_gshift,
+                                                                     c->d_dbl_scratch, d_r);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+__global__ void k_loglik_mult_one(const float* __restrict__ x, int64_t N, int D, int Dp, const double* __restrict__ lt,
+                                  double* __restrict__ r)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double sum = 0;
+    for (int i = 0; i < D; ++i) sum += lt[i] * (double)x[p * Dp + i];
+    r[p] = sum;
+}
+
+dpmm_status launch_loglik_mult_one(dpmm_ctx* c, double* d_r)
+{
+    k_loglik_mult_one<<<blocks_for(c->N, 128), 128, 0, c->stream>>>(c->d_x, c->N, c->D, c->Dp, c->d_dbl_scratch, d_r);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+constexpr int kSeamMaxK = 64;
+
+// cudaKernel::sample_log_cat_array on a caller matrix (FP64 softmax + alias, as the reference)
+__global__ void k_sample_log_cat(const double* __restrict__ r, int64_t N, int K, RngArgs rng, int32_t* __restrict__ labels)
+{
+    int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (p >= N) return;
+    double y[kSeamMaxK + 2];
+    int32_t a[kSeamMaxK + 2], b[kSeamMaxK + 2];
+    double mx = 0;
+    bool first = true;
+    for (int k = 0; k < K; ++k) {
+        double v = r[(size_t)k * N + p];
+        if (first || v > mx) { first = false; mx = v; }
+    }
+    double sum = 0;
+    for (int k = 0; k < K; ++k) { y[k + 1] = exp(r[(size_t)k * N + p] - mx); sum += y[k + 1]; }
+    for (int k = 0; k < K; ++k) y[k + 1] = (y[k + 1] / sum) * K;
+    float u1, u2;
+    draw_uniform2(rng, p, u1, u2);
+    AliasAcc<double, int32_t> acc{y, a, b, 1};
+    labels[p] = alias_draw<double, int32_t>(K, acc, u1, u2);
+}
+
+dpmm_status launch_sample_log_cat(dpmm_ctx* c, int K, const double* d_r, const float* d_u)
+{
+    if (K > kSeamMaxK) return fail(DPMM_ERR_INVALID_ARG, "sample_log_cat_array seam supports K <= 64");
+    RngArgs r = rng_args(c, d_u);
+    k_sample_log_cat<<<blocks_for(c->N, 128), 128, 0, c->stream>>>(d_r, c->N, K, r, c->d_labels);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+// cudaKernel::sample_log_cat_array_sub_cluster: m points given by indices, log-likelihoods m x 2
+__global__ void k_sample_log_cat_sub(const double* __restrict__ r, int m, const int32_t* __restrict__ idx,
+                                     const double* __restrict__ lrw, RngArgs rng, int64_t N, int32_t* __restrict__ sub)
+{
+    int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= m) return;
+    int64_t pt = idx[q];
+    if (pt < 0 || pt >= N) return;
+    double a = r[q] + log(lrw[0]);
+    double b = r[q + m] + log(lrw[1]);
+    double mx = fmax(a, b);
+    a = exp(a - mx);
+    b = exp(b - mx);
+    double s = a + b;
+    double y[4];
+    int32_t aa[4], bb[4];
+    y[1] = (a / s) * 2;
+    y[2] = (b / s) * 2;
+    float u1, u2;
+    draw_uniform2(rng, pt, u1, u2);
+    AliasAcc<double, int32_t> acc{y, aa, bb, 1};
+    sub[pt] = alias_draw<double, int32_t>(2, acc, u1, u2);
+}
+
+dpmm_status launch_sample_log_cat_sub(dpmm_ctx* c, int m, const double* d_r, const int32_t* d_idx, const double* d_lrw,
+                                      const float* d_u)
+{
+    RngArgs r = rng_args(c, d_u);
+    k_sample_log_cat_sub<<<blocks_for(m, 128), 128, 0, c->stream>>>(d_r, m, d_idx, d_lrw, r, c->N, c->d_sub);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+}  // namespace dpmm

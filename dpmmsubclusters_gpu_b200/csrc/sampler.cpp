@@ -1,0 +1,1049 @@
+// sampler.cpp -- host driver of the Chang & Fisher sub-cluster split/merge sampler running
+// on the device back-end of dpmm_capi.  It keeps the reference's iteration semantics:
+//   dp_parallel_sampling_class::dp_parallel / init_model / init_first_clusters / run_model
+//                                                   (dp_parallel_sampling.cpp:19-206)
+//   local_clusters_actions::group_step and the steps it calls (local_clusters_actions.cpp:14-490)
+//   shared_actions::sample_cluster_params / create_splittable_from_params /
+//                   merge_clusters_to_splittable / should_merge (shared_actions.cpp:9-111)
+//   niw / multinomial_prior posterior, lml, sampling (priors/niw.cpp, priors/multinomial_prior.cpp)
+//   global_params JSON keys and defaults (global_params.h:37-78, global_params.cpp:8-106)
+// What moved to the device: label / sub-label draws, sufficient statistics, the split ratios of
+// all clusters (one launch) and the merge ratios of all pairs (one launch).  Host FP64 keeps the
+// per-cluster bookkeeping, parameter draws and the sequential accept/reject decisions.
+#include <omp.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <ctime>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <numeric>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "dpmm_internal.h"
+#include "io.h"
+#include "linalg.h"
+
+namespace dpmm {
+namespace host {
+
+struct Hyper {               // niw_hyperparams {k, m, v, psi} / multinomial_hyper {alpha}
+    double k = 0, v = 0;
+    std::vector<double> m, psi;
+    std::vector<double> chol;    // lower Cholesky factor of psi (NIW)
+    double logdet = 0;           // log det psi (NIW)
+    std::vector<double> alpha;
+};
+
+struct Stats {               // niw_sufficient_statistics / multinomial_sufficient_statistics
+    int64_t N = 0;
+    std::vector<double> sum, S;
+};
+
+struct Dist {                // mv_gaussian (precision factor form) / multinomial_dist
+    std::vector<double> mu, W;   // inv_sigma = W W^T
+    double logdet_sigma = 0;
+    std::vector<double> log_theta;
+};
+
+struct ClusterParams {       // cluster_parameters (ds.h:39-118)
+    Hyper prior, post;
+    Dist dist;
+    Stats stats;
+};
+
+struct Splittable {          // splittable_cluster_params (ds.h:122-214) + local_cluster counts
+    ClusterParams c, l, r;
+    double lrw[2] = {0.5, 0.5};
+    bool splittable = false;
+    std::vector<std::pair<bool, double>> hist;
+    int64_t points_count = 0;
+};
+
+struct Config {
+    int prior = DPMM_PRIOR_GAUSSIAN;
+    int iterations = 100, initial_clusters = 1, burnout = 15;
+    int argmax_sample_stop = 5, split_stop = 5;
+    double alpha = 10.0, max_clusters = 1e300, outlier_mod = 0.0;
+    uint64_t seed = 0;
+    bool verbose = false;
+    Hyper hyper, outlier_hyper;
+    std::vector<int32_t> gt;
+    int loglik_mode = DPMM_LL_AUTO, rng_kind = DPMM_RNG_PHILOX, k_max = 0, device = 0;
+};
+
+class Sampler {
+public:
+    Sampler(const Config& cfg, dpmm_ctx* ctx, int64_t N, int D)
+        : cfg_(cfg), ctx_(ctx), N_(N), D_(D), gen_((unsigned long)cfg.seed)
+    {
+    }
+
+    // init_model + init_first_clusters, then iterations first..first+n-1 of run_model
+    dpmm_status init() { return init_first_clusters(); }
+    dpmm_status step(int n, dpmm_model_info* mi);
+    dpmm_status finish(dpmm_model_info* mi);
+    int num_clusters() const { return (int)clusters_.size(); }
+    int iteration() const { return iter_; }
+
+private:
+    // ----------------------------------------------------------------- prior maths
+    void finish_hyper(Hyper& h) const
+    {
+        if (cfg_.prior != DPMM_PRIOR_GAUSSIAN) return;
+        if (la::cholesky(h.psi.data(), D_, h.chol)) h.logdet = la::logdet_from_chol(h.chol, D_);
+        else h.logdet = NAN;
+    }
+
+    Hyper posterior(const Hyper& p, const Stats& s) const   // niw.cpp:23-49, multinomial_prior.cpp:12-22
+    {
+        if (s.N == 0) return p;
+        Hyper h;
+        if (cfg_.prior == DPMM_PRIOR_MULTINOMIAL) {
+            h.alpha.resize(D_);
+            for (int d = 0; d < D_; ++d) h.alpha[d] = p.alpha[d] + s.sum[d];
+            return h;
+        }
+        const int D = D_;
+        h.k = p.k + (double)s.N;
+        h.v = p.v + (double)s.N;
+        h.m.resize(D);
+        for (int i = 0; i < D; ++i) h.m[i] = (p.m[i] * p.k + s.sum[i]) / h.k;
+        h.psi.resize((size_t)D * D);
+        for (int j = 0; j < D; ++j)
+            for (int i = 0; i <= j; ++i) {      // upper triangle, mirrored (selfadjointView<Upper>)
+                size_t ij = (size_t)j * D + i;
+                double tm = p.v * p.psi[ij] + p.k * p.m[i] * p.m[j];
+                double v = (tm - h.k * h.m[i] * h.m[j] + s.S[ij]) / h.v;
+                h.psi[ij] = v;
+                h.psi[(size_t)i * D + j] = v;
+            }
+        finish_hyper(h);
+        return h;
+    }
+
+    static double lmvgamma(double x, int D)    // utils.cpp:94-102
+    {
+        double r = D * (D - 1) / 4.0 * std::log(M_PI);
+        for (int d = 1; d <= D; ++d) r += std::lgamma(x + (1 - d) / 2.0);
+        return r;
+    }
+
+    double lml(const Hyper& p, const Hyper& q, const Stats& s) const   // niw.cpp:122-138 / multinomial_prior.cpp:56-67
+    {
+        if (cfg_.prior == DPMM_PRIOR_MULTINOMIAL) {
+            double s0 = 0, sp = 0, v = 0;
+            for (int d = 0; d < D_; ++d) {
+                s0 += p.alpha[d];
+                sp += q.alpha[d];
+                v += std::lgamma(q.alpha[d]) - std::lgamma(p.alpha[d]);
+            }
+            return std::lgamma(s0) - std::lgamma(sp) + v;
+        }
+        const int D = D_;
+        return -(double)s.N * D * 0.5 * std::log(M_PI) + lmvgamma(q.v / 2.0, D) - lmvgamma(p.v / 2.0, D) +
+               (p.v / 2.0) * (D * std::log(p.v) + p.logdet) - (q.v / 2.0) * (D * std::log(q.v) + q.logdet) +
+               (D / 2.0) * std::log(p.k / q.k);
+    }
+
+    Stats aggregate(const Stats& a, const Stats& b) const   // niw.cpp:140-148
+    {
+        Stats o;
+        o.N = a.N + b.N;
+        o.sum.resize(a.sum.size());
+        for (size_t i = 0; i < a.sum.size(); ++i) o.sum[i] = a.sum[i] + b.sum[i];
+        o.S.resize(a.S.size());
+        for (size_t i = 0; i < a.S.size(); ++i) o.S[i] = a.S[i] + b.S[i];
+        return o;
+    }
+
+    Stats empty_stats() const
+    {
+        Stats s;
+        s.sum.assign(D_, 0.0);
+        if (cfg_.prior == DPMM_PRIOR_GAUSSIAN) s.S.assign((size_t)D_ * D_, 0.0);
+        return s;
+    }
+
+    // niw::sample_distribution (niw.cpp:82-107) in factor form: with v psi = L L^T and A the
+    // Bartlett factor (A_ii = sqrt(chi2(v - i)), A_ij ~ N(0,1) below the diagonal, the draw of
+    // stats::rinvwish2), the precision is W W^T with W = L^-T A ~ Wishart(v, (v psi)^-1); then
+    // Sigma = (L A^-T)(L A^-T)^T, log det Sigma = 2 sum log L_ii - 2 sum log A_ii, and
+    // mu = m + L A^-T z / sqrt(k), z ~ N(0, I).  multinomial_prior::sample_distribution
+    // (multinomial_prior.cpp:24-49): log of a Dirichlet(alpha) draw.
+    Dist sample(const Hyper& h, std::mt19937_64& g) const
+    {
+        Dist d;
+        if (cfg_.prior == DPMM_PRIOR_MULTINOMIAL) {
+            std::vector<double> x(D_);
+            double s = 0;
+            for (int i = 0; i < D_; ++i) {
+                std::gamma_distribution<double> ga(h.alpha[i], 1.0);
+                x[i] = ga(g);
+                s += x[i];
+            }
+            d.log_theta.resize(D_);
+            for (int i = 0; i < D_; ++i) d.log_theta[i] = std::log(x[i] / s);
+            return d;
+        }
+        const int D = D_;
+        std::vector<double> L((size_t)D * D);
+        const double sv = std::sqrt(h.v);
+        for (size_t e = 0; e < L.size(); ++e) L[e] = h.chol[e] * sv;
+        std::normal_distribution<double> nd(0.0, 1.0);
+        std::vector<double> A((size_t)D * D, 0.0);
+        for (int i = 1; i < D; ++i)
+            for (int j = 0; j < i; ++j) A[(size_t)j * D + i] = nd(g);
+        for (int i = 0; i < D; ++i) {
+            std::chi_squared_distribution<double> cs(h.v - i);
+            A[(size_t)i * D + i] = std::sqrt(cs(g));
+        }
+        // W = L^-T A: solve L^T W = A column by column (back substitution; A is lower-triangular)
+        d.W.assign((size_t)D * D, 0.0);
+        for (int c = 0; c < D; ++c) {
+            double* w = &d.W[(size_t)c * D];
+            for (int i = D - 1; i >= 0; --i) {
+                double s = i >= c ? A[(size_t)c * D + i] : 0.0;
+                for (int q = i + 1; q < D; ++q) s -= L[(size_t)i * D + q] * w[q];
+                w[i] = s / L[(size_t)i * D + i];
+            }
+        }
+        double ldl = 0, lda = 0;
+        for (int i = 0; i < D; ++i) {
+            ldl += std::log(L[(size_t)i * D + i]);
+            lda += std::log(A[(size_t)i * D + i]);
+        }
+        d.logdet_sigma = 2 * ldl - 2 * lda;
+        // mu = m + L y / sqrt(k) with A^T y = z
+        std::vector<double> z(D), y(D);
+        for (int i = 0; i < D; ++i) z[i] = nd(g);
+        for (int i = D - 1; i >= 0; --i) {
+            double s = z[i];
+            for (int q = i + 1; q < D; ++q) s -= A[(size_t)i * D + q] * y[q];
+            y[i] = s / A[(size_t)i * D + i];
+        }
+        d.mu.resize(D);
+        const double isk = 1.0 / std::sqrt(h.k);
+        for (int i = 0; i < D; ++i) {
+            double s = 0;
+            for (int q = 0; q <= i; ++q) s += L[(size_t)q * D + i] * y[q];
+            d.mu[i] = h.m[i] + s * isk;
+        }
+        return d;
+    }
+
+    // per-draw generator: seeded from (seed, draw counter) so draws can run in parallel and
+    // stay reproducible for a given seed
+    std::mt19937_64 draw_gen(uint64_t id) const
+    {
+        std::seed_seq sq{(uint32_t)cfg_.seed, (uint32_t)(cfg_.seed >> 32), (uint32_t)id, (uint32_t)(id >> 32)};
+        return std::mt19937_64(sq);
+    }
+
+    std::vector<double> dirichlet(const std::vector<double>& a)   // distributions_util/dirichlet.h:39-48
+    {
+        std::vector<double> x(a.size());
+        double s = 0;
+        for (size_t i = 0; i < a.size(); ++i) {
+            std::gamma_distribution<double> g(a[i], 1.0);
+            x[i] = g(gen_);
+            s += x[i];
+        }
+        for (double& v : x) v /= s;
+        return x;
+    }
+
+    double uniform()
+    {
+        std::uniform_real_distribution<double> u(0, 1);
+        return u(gen_);
+    }
+
+    std::vector<std::pair<bool, double>> fresh_hist() const
+    {
+        return std::vector<std::pair<bool, double>>(cfg_.burnout + 5, std::make_pair(false, 0.0));
+    }
+
+    // ----------------------------------------------------------------- device glue
+    dpmm_status upload_params(const std::vector<double>& weights);
+    dpmm_status update_suff_stats_posterior(const std::vector<int32_t>& indices);
+    void sample_cluster_params_all();
+    void sample_clusters();
+    dpmm_status reset_bad_clusters();
+    dpmm_status check_and_split(bool final_, std::vector<int32_t>& all_indices);
+    dpmm_status check_and_merge(bool final_);
+    dpmm_status remove_empty_clusters();
+    dpmm_status group_step(bool no_more_splits, bool final_);
+    dpmm_status init_first_clusters();
+    double calculate_posterior() const;
+    double nmi(const std::vector<int32_t>& labels) const;
+    Config cfg_;
+    dpmm_ctx* ctx_;
+    int64_t N_;
+    int D_;
+    int iter_ = 0;
+    std::mt19937 gen_;
+    uint64_t draw_ctr_ = 0;
+    std::vector<Splittable> clusters_;
+    std::vector<double> weights_;
+
+};
+
+}  // namespace host
+}  // namespace dpmm
+
+struct dpmm_model_info {
+    int64_t n = 0;
+    std::vector<int32_t> labels;
+    std::vector<double> weights, iter_count, likelihood_history, nmi_history;
+    std::vector<int32_t> cluster_count_history;
+};
+
+namespace dpmm {
+namespace host {
+
+// thin_cluster_params broadcast + per-cluster parameter copies (local_clusters_actions.cpp:373-382)
+dpmm_status Sampler::upload_params(const std::vector<double>& weights)
+{
+    const int K = (int)clusters_.size();
+    const int D = D_;
+    std::vector<double> w(K, 1.0), lrw(2 * (size_t)K);
+    for (int k = 0; k < K; ++k) {
+        w[k] = k < (int)weights.size() ? weights[k] : 0.0;
+        lrw[2 * k] = clusters_[k].lrw[0];
+        lrw[2 * k + 1] = clusters_[k].lrw[1];
+    }
+    if (cfg_.prior == DPMM_PRIOR_MULTINOMIAL) {
+        std::vector<double> lt((size_t)K * D), lt_lr((size_t)2 * K * D);
+        for (int k = 0; k < K; ++k) {
+            std::memcpy(&lt[(size_t)k * D], clusters_[k].c.dist.log_theta.data(), sizeof(double) * D);
+            std::memcpy(&lt_lr[(size_t)(2 * k) * D], clusters_[k].l.dist.log_theta.data(), sizeof(double) * D);
+            std::memcpy(&lt_lr[(size_t)(2 * k + 1) * D], clusters_[k].r.dist.log_theta.data(), sizeof(double) * D);
+        }
+        return dpmm_set_multinomial_params(ctx_, K, lt.data(), w.data(), lt_lr.data(), lrw.data());
+    }
+    std::vector<double> mu((size_t)K * D), W((size_t)K * D * D), ld(K), mu_lr((size_t)2 * K * D),
+        W_lr((size_t)2 * K * D * D), ld_lr(2 * (size_t)K);
+    for (int k = 0; k < K; ++k) {
+        const Dist* ds[3] = {&clusters_[k].c.dist, &clusters_[k].l.dist, &clusters_[k].r.dist};
+        std::memcpy(&mu[(size_t)k * D], ds[0]->mu.data(), sizeof(double) * D);
+        std::memcpy(&W[(size_t)k * D * D], ds[0]->W.data(), sizeof(double) * D * D);
+        ld[k] = ds[0]->logdet_sigma;
+        for (int s = 0; s < 2; ++s) {
+            std::memcpy(&mu_lr[(size_t)(2 * k + s) * D], ds[1 + s]->mu.data(), sizeof(double) * D);
+            std::memcpy(&W_lr[(size_t)(2 * k + s) * D * D], ds[1 + s]->W.data(), sizeof(double) * D * D);
+            ld_lr[2 * k + s] = ds[1 + s]->logdet_sigma;
+        }
+    }
+    return dpmm_set_gaussian_factors(ctx_, K, mu.data(), W.data(), ld.data(), w.data(), mu_lr.data(), W_lr.data(),
+                                     ld_lr.data(), lrw.data());
+}
+
+// local_clusters_actions::update_suff_stats_posterior (local_clusters_actions.cpp:103-168)
+dpmm_status Sampler::update_suff_stats_posterior(const std::vector<int32_t>& indices)
+{
+    const int n = (int)indices.size();
+    if (n == 0) return DPMM_OK;
+    const int D = D_;
+    const bool gauss = cfg_.prior == DPMM_PRIOR_GAUSSIAN;
+    std::vector<int64_t> cnt(3 * (size_t)n);
+    std::vector<double> sum(3 * (size_t)n * D), S(gauss ? 3 * (size_t)n * D * D : 0);
+    DPMM_TRY(dpmm_create_sufficient_statistics(ctx_, n, indices.data(), cnt.data(), sum.data(),
+                                               gauss ? S.data() : nullptr));
+#pragma omp parallel for schedule(dynamic)
+    for (int q = 0; q < n; ++q) {
+        Splittable& sc = clusters_[indices[q]];
+        ClusterParams* cp[3] = {&sc.c, &sc.l, &sc.r};
+        for (int s = 0; s < 3; ++s) {
+            Stats st;
+            st.N = cnt[3 * (size_t)q + s];
+            st.sum.assign(&sum[(3 * (size_t)q + s) * D], &sum[(3 * (size_t)q + s) * D] + D);
+            if (gauss) st.S.assign(&S[(3 * (size_t)q + s) * D * D], &S[(3 * (size_t)q + s) * D * D] + (size_t)D * D);
+            cp[s]->stats = std::move(st);
+            cp[s]->post = posterior(cp[s]->prior, cp[s]->stats);
+        }
+        sc.points_count = sc.c.stats.N;
+    }
+    return DPMM_OK;
+}
+
+// shared_actions::sample_cluster_params (shared_actions.cpp:9-55) for every cluster, with the
+// three distribution draws of all clusters done in parallel
+void Sampler::sample_cluster_params_all()
+{
+    const int K = (int)clusters_.size();
+    std::vector<int> todo;
+    for (int i = 0; i < K; ++i)
+        if (!(cfg_.outlier_mod > 0 && i == 1)) todo.push_back(i);   // local_clusters_actions.cpp:348-351
+    const uint64_t base = draw_ctr_;
+    draw_ctr_ += 3 * (uint64_t)K;
+    std::vector<double> lml_lr(K, 0.0);
+#pragma omp parallel for schedule(dynamic)
+    for (int t = 0; t < (int)todo.size(); ++t) {
+        const int i = todo[t];
+        Splittable& sc = clusters_[i];
+        ClusterParams* cp[3] = {&sc.c, &sc.l, &sc.r};
+        for (int s = 0; s < 3; ++s) {
+            std::mt19937_64 g = draw_gen(base + 3 * (uint64_t)i + s);
+            cp[s]->dist = sample(cp[s]->post, g);
+        }
+        lml_lr[i] = lml(sc.l.prior, sc.l.post, sc.l.stats) + lml(sc.r.prior, sc.r.post, sc.r.stats);
+    }
+    const int B = cfg_.burnout;
+    for (int i : todo) {
+        Splittable& sc = clusters_[i];
+        std::vector<double> pc = {(double)sc.l.stats.N + cfg_.alpha / 2, (double)sc.r.stats.N + cfg_.alpha / 2};
+        std::vector<double> w = dirichlet(pc);
+        sc.lrw[0] = w[0];
+        sc.lrw[1] = w[1];
+        for (int q = 0; q < B - 1; ++q) sc.hist[q] = sc.hist[q + 1];
+        sc.hist[B - 1] = std::make_pair(true, lml_lr[i]);
+        double now = 0.0;
+        bool ready = true;
+        for (int q = 0; q < B; ++q) {
+            if (sc.hist[q].first) now += sc.hist[q].second * (1 / (B - 0.1));
+            else ready = false;
+        }
+        if (ready && now - sc.hist[B - 1].second < 1e-2) sc.splittable = true;
+        sc.points_count = sc.c.stats.N;
+    }
+}
+
+// local_clusters_actions::sample_clusters (local_clusters_actions.cpp:341-371)
+void Sampler::sample_clusters()
+{
+    sample_cluster_params_all();
+    std::vector<double> pc;
+    for (size_t i = 0; i < clusters_.size(); ++i) {
+        if (cfg_.outlier_mod > 0 && i == 1) continue;
+        pc.push_back((double)clusters_[i].points_count);
+    }
+    pc.push_back(cfg_.alpha);
+    std::vector<double> d;
+    if (pc.size() == 2 && pc[0] == 0.0) d = {0.0, 1.0};   // local_clusters_actions.cpp:323-339
+    else d = dirichlet(pc);
+    weights_.clear();
+    for (size_t i = 0; i + 1 < d.size(); ++i) weights_.push_back(d[i] * (1 - cfg_.outlier_mod));
+    if (cfg_.outlier_mod > 0) weights_.insert(weights_.begin(), cfg_.outlier_mod);
+}
+
+// local_clusters_actions::reset_bad_clusters (local_clusters_actions.cpp:429-447)
+dpmm_status Sampler::reset_bad_clusters()
+{
+    std::vector<int32_t> bad;
+    for (size_t i = 0; i < clusters_.size(); ++i) {
+        Splittable& sc = clusters_[i];
+        if (sc.l.stats.N == 0 || sc.r.stats.N == 0) {
+            bad.push_back((int32_t)i);
+            sc.hist = fresh_hist();
+            sc.splittable = false;
+        }
+    }
+    if (bad.empty()) return DPMM_OK;
+    DPMM_TRY(dpmm_reset_bad_clusters(ctx_, (int)bad.size(), bad.data(), nullptr));
+    return update_suff_stats_posterior(bad);
+}
+
+// local_clusters_actions::check_and_split + should_split_local + split_cluster_local
+// (local_clusters_actions.cpp:183-194, 215-285), split ratios from one device launch
+dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indices)
+{
+    const int K = (int)clusters_.size();
+    all_indices.clear();
+    std::vector<int> split(K, 0);
+    bool any_candidate = false;
+    for (int i = 0; i < K; ++i)
+        if (clusters_[i].splittable && clusters_[i].c.stats.N > 1 && !(cfg_.outlier_mod > 0 && i == 1))
+            any_candidate = true;
+    if (!any_candidate || final_) return DPMM_OK;
+    std::vector<double> hr(K);
+    DPMM_TRY(dpmm_split_hastings(ctx_, K, cfg_.alpha, nullptr, hr.data()));
+    for (int i = 0; i < K; ++i) {
+        if (cfg_.outlier_mod > 0 && i == 1) continue;
+        Splittable& sc = clusters_[i];
+        if (!(sc.splittable && sc.c.stats.N > 1)) continue;
+        if (sc.l.stats.N == 0 || sc.r.stats.N == 0) continue;
+        double log_hr = hr[i];
+        if (cfg_.outlier_mod > 0 && i == 0) {
+            // the outlier cluster has its own prior: evaluate its ratio on the host
+            Hyper p = posterior(sc.c.prior, sc.c.stats), pl = posterior(sc.c.prior, sc.l.stats),
+                  pr = posterior(sc.c.prior, sc.r.stats);
+            log_hr = std::log(cfg_.alpha) + std::lgamma((double)sc.l.stats.N) + lml(sc.l.prior, pl, sc.l.stats) +
+                     std::lgamma((double)sc.r.stats.N) + lml(sc.r.prior, pr, sc.r.stats) -
+                     (std::lgamma((double)sc.c.stats.N) + lml(sc.c.prior, p, sc.c.stats));
+        }
+        const double u = uniform();
+        if (log_hr > std::log(u)) split[i] = 1;
+    }
+    int n_split = std::accumulate(split.begin(), split.end(), 0);
+    // capacity guard: the device tables hold k_max clusters
+    while (n_split > 0 && K + n_split > ctx_->k_max) {
+        for (int i = K - 1; i >= 0; --i)
+            if (split[i]) { split[i] = 0; --n_split; break; }
+    }
+    if (n_split == 0) return DPMM_OK;
+    std::vector<int32_t> idx, nidx;
+    int new_index = K;
+    clusters_.resize(K + n_split);
+    for (int i = 0; i < K; ++i) {
+        if (!split[i]) continue;
+        idx.push_back(i);
+        nidx.push_back(new_index);
+        // split_cluster_local: the new cluster takes r, cluster i keeps l
+        Splittable& sc = clusters_[i];
+        Splittable ns = sc;
+        auto make = [&](const ClusterParams& p, Splittable& out) {   // create_splittable_from_params
+            out.l = p;
+            out.r = p;
+            std::mt19937_64 g1 = draw_gen(draw_ctr_++), g2 = draw_gen(draw_ctr_++);
+            out.l.dist = sample(p.post, g1);
+            out.r.dist = sample(p.post, g2);
+            std::vector<double> w = dirichlet({cfg_.alpha / 2, cfg_.alpha / 2});
+            out.lrw[0] = w[0];
+            out.lrw[1] = w[1];
+            out.c = p;
+            out.hist = fresh_hist();
+            out.splittable = false;
+        };
+        ClusterParams r = sc.r, l = sc.l;
+        make(r, ns);
+        make(l, sc);
+        ns.points_count = ns.c.stats.N;
+        sc.points_count = sc.c.stats.N;
+        clusters_[new_index] = std::move(ns);
+        ++new_index;
+    }
+    all_indices = idx;
+    all_indices.insert(all_indices.end(), nidx.begin(), nidx.end());
+    return dpmm_split_clusters(ctx_, (int)idx.size(), idx.data(), nidx.data(), nullptr);
+}
+
+// local_clusters_actions::check_and_merge + shared_actions::should_merge + merge_clusters
+// (local_clusters_actions.cpp:204-213, 287-321; shared_actions.cpp:72-111); all pair ratios
+// from one device launch, accepted greedily in (i, j) order
+dpmm_status Sampler::check_and_merge(bool final_)
+{
+    const int K = (int)clusters_.size();
+    int n_split = 0;
+    for (auto& c : clusters_) n_split += c.splittable && c.c.stats.N > 0;
+    if (n_split < 2) return DPMM_OK;
+    std::vector<double> hr((size_t)K * K);
+    DPMM_TRY(dpmm_merge_hastings(ctx_, K, cfg_.alpha, hr.data()));
+    std::vector<int32_t> idx, nidx;
+    for (int i = 0; i < K; ++i) {
+        if (cfg_.outlier_mod > 0 && i == 0) continue;
+        for (int j = i + 1; j < K; ++j) {
+            Splittable& a = clusters_[i];
+            Splittable& b = clusters_[j];
+            if (!(a.splittable && b.splittable && a.c.stats.N > 0 && b.c.stats.N > 0)) continue;
+            const double log_hr = hr[(size_t)i * K + j];
+            const double u = uniform();
+            if (!((log_hr > std::log(u)) || (final_ && log_hr > std::log(0.1)))) continue;
+            // merge_clusters_to_splittable(a, b.c) then local bookkeeping
+            a.c.stats = aggregate(a.c.stats, b.c.stats);
+            a.c.post = posterior(a.c.prior, a.c.stats);
+            std::vector<double> w = dirichlet({(double)a.c.stats.N + cfg_.alpha / 2, (double)b.c.stats.N + cfg_.alpha / 2});
+            a.lrw[0] = w[0];
+            a.lrw[1] = w[1];
+            a.l = a.c;
+            a.r = b.c;
+            a.splittable = false;
+            a.hist = fresh_hist();
+            a.points_count += b.points_count;
+            b.points_count = 0;
+            b.c.stats.N = 0;
+            b.splittable = false;
+            idx.push_back(i);
+            nidx.push_back(j);
+        }
+    }
+    if (idx.empty()) return DPMM_OK;
+    return dpmm_merge_clusters(ctx_, (int)idx.size(), idx.data(), nidx.data());
+}
+
+// local_clusters_actions::remove_empty_clusters (local_clusters_actions.cpp:384-419)
+dpmm_status Sampler::remove_empty_clusters()
+{
+    std::vector<Splittable> keep;
+    std::vector<int32_t> limits;
+    int removed = 0;
+    const size_t K = clusters_.size();
+    for (size_t i = 0; i < K; ++i) {
+        const int64_t pc = clusters_[i].points_count;
+        if (pc == 0) {
+            limits.push_back((int32_t)(i - removed + 1));
+            ++removed;
+        }
+        if (pc > 0 || (cfg_.outlier_mod > 0 && i == 0) || (cfg_.outlier_mod > 0 && i == 1 && K == 2))
+            keep.push_back(std::move(clusters_[i]));
+    }
+    clusters_ = std::move(keep);
+    if (limits.empty()) return DPMM_OK;
+    return dpmm_remove_empty_clusters(ctx_, (int)limits.size(), limits.data());
+}
+
+// local_clusters_actions::group_step (local_clusters_actions.cpp:460-490)
+dpmm_status Sampler::group_step(bool no_more_splits, bool final_)
+{
+    sample_clusters();
+    DPMM_TRY(upload_params(weights_));
+    const int K = (int)clusters_.size();
+    DPMM_TRY(dpmm_create_clusters_labels(ctx_, K, final_ ? 1 : 0, nullptr, nullptr));
+    DPMM_TRY(dpmm_create_subclusters_labels(ctx_, K, nullptr, nullptr));
+    std::vector<int32_t> all(K);
+    std::iota(all.begin(), all.end(), 0);
+    DPMM_TRY(update_suff_stats_posterior(all));
+    DPMM_TRY(reset_bad_clusters());
+    if (!no_more_splits) {
+        std::vector<int32_t> idx;
+        DPMM_TRY(check_and_split(final_, idx));
+        DPMM_TRY(update_suff_stats_posterior(idx));
+        DPMM_TRY(check_and_merge(final_));
+    }
+    return remove_empty_clusters();
+}
+
+// dp_parallel_sampling_class::init_model + init_first_clusters (dp_parallel_sampling.cpp:48-87)
+dpmm_status Sampler::init_first_clusters()
+{
+    DPMM_TRY(dpmm_sample_labels(ctx_, cfg_.initial_clusters, cfg_.outlier_mod, nullptr));
+    DPMM_TRY(dpmm_sample_sub_labels(ctx_, nullptr));
+    clusters_.clear();
+    if (cfg_.outlier_mod > 0) {   // create_outlier_local_cluster (local_clusters_actions.cpp:48-79)
+        Splittable sc;
+        sc.c.prior = cfg_.outlier_hyper;
+        sc.c.stats = empty_stats();
+        DPMM_TRY(all_points_stats(ctx_, &sc.c.stats.N, sc.c.stats.sum.data(),
+                                  cfg_.prior == DPMM_PRIOR_GAUSSIAN ? sc.c.stats.S.data() : nullptr));
+        sc.c.post = posterior(cfg_.outlier_hyper, sc.c.stats);
+        std::mt19937_64 g = draw_gen(draw_ctr_++);
+        sc.c.dist = sample(sc.c.post, g);
+        sc.l = sc.c;
+        sc.r = sc.c;
+        sc.hist = fresh_hist();
+        int32_t l = 0, r = 0;
+        DPMM_TRY(dpmm_get_sub_labels_count(ctx_, &l, &r));
+        sc.l.stats.N = l;
+        sc.r.stats.N = r;
+        sc.points_count = sc.c.stats.N;
+        clusters_.push_back(std::move(sc));
+    }
+    for (int i = 0; i < cfg_.initial_clusters; ++i) {   // create_first_local_cluster (:14-46)
+        Splittable sc;
+        sc.c.prior = cfg_.hyper;
+        sc.c.stats = empty_stats();
+        std::mt19937_64 g = draw_gen(draw_ctr_++);
+        sc.c.dist = sample(cfg_.hyper, g);
+        sc.c.post = cfg_.hyper;
+        sc.c.stats.N = N_;
+        sc.l = sc.c;
+        sc.r = sc.c;
+        sc.hist = fresh_hist();
+        sc.l.stats.N = 0;
+        sc.r.stats.N = 0;
+        int32_t l = 0, r = 0;
+        DPMM_TRY(dpmm_get_sub_labels_count(ctx_, &l, &r));
+        sc.l.stats.N = l;
+        sc.r.stats.N = r;
+        sc.points_count = sc.c.stats.N;
+        clusters_.push_back(std::move(sc));
+        DPMM_TRY(dpmm_sample_sub_labels(ctx_, nullptr));   // split_first_cluster_worker
+    }
+    std::vector<int32_t> all(clusters_.size());
+    std::iota(all.begin(), all.end(), 0);
+    DPMM_TRY(update_suff_stats_posterior(all));
+    sample_clusters();
+    return DPMM_OK;
+}
+
+// dp_parallel_sampling_class::calculate_posterior (dp_parallel_sampling.cpp:218-236)
+double Sampler::calculate_posterior() const
+{
+    double lp = std::lgamma(cfg_.alpha) - std::lgamma((double)N_ + cfg_.alpha);
+    for (const Splittable& sc : clusters_) {
+        if (sc.c.stats.N == 0) continue;
+        lp += lml(sc.c.prior, sc.c.post, sc.c.stats);
+        lp += std::log(cfg_.alpha) + std::lgamma((double)sc.c.stats.N);
+    }
+    return lp;
+}
+
+// NMI = 2 I(X;Y) / (H(X) + H(Y)) (dp_parallel_sampling.cpp:171-179)
+double Sampler::nmi(const std::vector<int32_t>& labels) const
+{
+    const size_t n = std::min(labels.size(), cfg_.gt.size());
+    if (n == 0) return NAN;
+    std::map<int32_t, int> ia, ib;
+    for (size_t i = 0; i < n; ++i) {
+        ia.emplace(cfg_.gt[i], (int)ia.size());
+        ib.emplace(labels[i], (int)ib.size());
+    }
+    std::vector<double> ca(ia.size(), 0), cb(ib.size(), 0), joint(ia.size() * ib.size(), 0);
+    for (size_t i = 0; i < n; ++i) {
+        int a = ia[cfg_.gt[i]], b = ib[labels[i]];
+        ca[a] += 1;
+        cb[b] += 1;
+        joint[(size_t)a * ib.size() + b] += 1;
+    }
+    double ha = 0, hb = 0, mi = 0;
+    for (double v : ca) if (v > 0) ha -= v / n * std::log(v / n);
+    for (double v : cb) if (v > 0) hb -= v / n * std::log(v / n);
+    for (size_t a = 0; a < ca.size(); ++a)
+        for (size_t b = 0; b < cb.size(); ++b) {
+            double v = joint[a * cb.size() + b];
+            if (v > 0) mi += v / n * std::log(v * n / (ca[a] * cb[b]));
+        }
+    return (ha + hb) > 0 ? 2 * mi / (ha + hb) : 1.0;
+}
+
+// dp_parallel_sampling_class::run_model (dp_parallel_sampling.cpp:132-206), n iterations at a time
+dpmm_status Sampler::step(int n, dpmm_model_info* mi)
+{
+    mi->n = N_;
+    for (int q = 0; q < n && iter_ < cfg_.iterations; ++q) {
+        const int i = ++iter_;
+        const bool final_ = i >= cfg_.iterations - cfg_.argmax_sample_stop;
+        const bool no_more_splits =
+            i >= cfg_.iterations - cfg_.split_stop || (double)clusters_.size() >= cfg_.max_clusters;
+        auto t0 = std::chrono::steady_clock::now();
+        DPMM_TRY(group_step(no_more_splits, final_));
+        auto t1 = std::chrono::steady_clock::now();
+        mi->iter_count.push_back(std::chrono::duration<double>(t1 - t0).count());
+        mi->cluster_count_history.push_back((int32_t)clusters_.size());
+        if (cfg_.verbose) {
+            mi->likelihood_history.push_back(calculate_posterior());
+            if (!cfg_.gt.empty()) {
+                std::vector<int32_t> lab(N_);
+                DPMM_TRY(dpmm_get_labels(ctx_, lab.data()));
+                mi->nmi_history.push_back(nmi(lab));
+            }
+            std::printf("Iteration: %d || Clusters count: %d || Log posterior: %f || NMI score: %f || Iter Time: %f\n", i,
+                        (int)clusters_.size(), mi->likelihood_history.back(),
+                        mi->nmi_history.empty() ? -1.0 : mi->nmi_history.back(), mi->iter_count.back());
+        } else {
+            mi->likelihood_history.push_back(1);
+        }
+    }
+    return DPMM_OK;
+}
+
+dpmm_status Sampler::finish(dpmm_model_info* mi)
+{
+    mi->n = N_;
+    mi->labels.resize(N_);
+    DPMM_TRY(dpmm_get_labels(ctx_, mi->labels.data()));
+    mi->weights = weights_;
+    return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- config helpers
+static Hyper default_hyper(int prior, int D)   // niw.cpp:195-198 / multinomial_prior.cpp:98-101
+{
+    Hyper h;
+    if (prior == DPMM_PRIOR_GAUSSIAN) {
+        h.k = 1.0;
+        h.v = 5;
+        h.m.assign(D, 0.0);
+        h.psi.assign((size_t)D * D, 0.0);
+        for (int i = 0; i < D; ++i) h.psi[(size_t)i * D + i] = 1.0;
+    } else {
+        h.alpha.assign(D, 0.0);
+    }
+    return h;
+}
+
+static uint64_t resolve_seed(uint64_t s)   // global_params::init_random (global_params.cpp:97-106)
+{
+    if (s != 0) return s;
+    std::srand((unsigned)std::time(nullptr));
+    return (uint64_t)std::rand();
+}
+
+struct SamplerHandle {
+    Config cfg;
+    dpmm_ctx* ctx = nullptr;
+    std::unique_ptr<Sampler> sampler;
+    dpmm_model_info mi;
+    ~SamplerHandle()
+    {
+        sampler.reset();
+        if (ctx) dpmm_destroy(ctx);
+    }
+};
+
+// dp_parallel_sampling_class(N, x, seed, prior) + global_params::init + init_model + init_first_clusters
+dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* points, bool f32,
+                         std::unique_ptr<SamplerHandle>& out)
+{
+    auto h = std::make_unique<SamplerHandle>();
+    Config& cfg = h->cfg;
+    cfg = cfg_in;
+    cfg.seed = resolve_seed(cfg.seed);
+    auto finish = [&](Hyper& hp) -> dpmm_status {
+        if (cfg.prior == DPMM_PRIOR_GAUSSIAN) {
+            if ((int)hp.m.size() != D || (int)hp.psi.size() != D * D)
+                return fail(DPMM_ERR_INVALID_ARG, "NIW hyper-parameters do not match the data dimension");
+            if (!la::cholesky(hp.psi.data(), D, hp.chol)) return fail(DPMM_ERR_NOT_PD, "prior psi is not positive definite");
+            hp.logdet = la::logdet_from_chol(hp.chol, D);
+        } else if ((int)hp.alpha.size() != D) {
+            return fail(DPMM_ERR_INVALID_ARG, "multinomial alpha does not match the data dimension");
+        }
+        return DPMM_OK;
+    };
+    DPMM_TRY(finish(cfg.hyper));
+    DPMM_TRY(finish(cfg.outlier_hyper));
+    if (cfg.burnout < 1) return fail(DPMM_ERR_INVALID_ARG, "burnout must be >= 1");
+    if (cfg.initial_clusters < 1) return fail(DPMM_ERR_INVALID_ARG, "initial_clusters must be >= 1");
+    if (!(cfg.alpha > 0)) return fail(DPMM_ERR_INVALID_ARG, "alpha must be positive");
+    dpmm_desc desc{};
+    desc.n_points = N;
+    desc.dim = D;
+    desc.prior_type = cfg.prior;
+    desc.k_max = cfg.k_max > 0 ? cfg.k_max : 256;
+    desc.rng_kind = cfg.rng_kind;
+    desc.seed = cfg.seed;
+    desc.loglik_mode = cfg.loglik_mode;
+    desc.device = cfg.device;
+    if (desc.k_max < cfg.initial_clusters + 2) desc.k_max = cfg.initial_clusters + 2;
+    DPMM_TRY(dpmm_create(&desc, &h->ctx));
+    if (f32) DPMM_TRY(dpmm_upload_points_f32(h->ctx, static_cast<const float*>(points)));
+    else DPMM_TRY(dpmm_upload_points(h->ctx, static_cast<const double*>(points)));
+    if (cfg.prior == DPMM_PRIOR_GAUSSIAN)
+        DPMM_TRY(dpmm_set_prior_niw(h->ctx, cfg.hyper.k, cfg.hyper.m.data(), cfg.hyper.v, cfg.hyper.psi.data()));
+    else
+        DPMM_TRY(dpmm_set_prior_multinomial(h->ctx, cfg.hyper.alpha.data()));
+    h->sampler = std::make_unique<Sampler>(cfg, h->ctx, N, D);
+    DPMM_TRY(h->sampler->init());
+    out = std::move(h);
+    return DPMM_OK;
+}
+
+dpmm_status run_sampler(const Config& cfg, int64_t N, int D, const void* points, bool f32, dpmm_model_info** out)
+{
+    std::unique_ptr<SamplerHandle> h;
+    DPMM_TRY(make_sampler(cfg, N, D, points, f32, h));
+    DPMM_TRY(h->sampler->step(h->cfg.iterations, &h->mi));
+    DPMM_TRY(h->sampler->finish(&h->mi));
+    *out = new dpmm_model_info(std::move(h->mi));
+    return DPMM_OK;
+}
+
+static Hyper hyper_from_run(int prior, int D, double k, double v, const double* m, const double* psi, const double* alpha)
+{
+    Hyper h = default_hyper(prior, D);
+    if (prior == DPMM_PRIOR_GAUSSIAN && m && psi) {
+        h.k = k;
+        h.v = v;
+        h.m.assign(m, m + D);
+        h.psi.assign(psi, psi + (size_t)D * D);
+    } else if (prior == DPMM_PRIOR_MULTINOMIAL && alpha) {
+        h.alpha.assign(alpha, alpha + D);
+    }
+    return h;
+}
+
+// niw::create_hyperparams / multinomial_prior::create_hyperparams (niw.cpp:155-193,
+// multinomial_prior.cpp:80-96)
+static Hyper hyper_from_json(int prior, int D, const io::Json& j)
+{
+    Hyper h = default_hyper(prior, D);
+    if (prior == DPMM_PRIOR_GAUSSIAN) {
+        h.k = j["k"].as_double(0.0);
+        h.v = j["v"].as_double(0.0);
+        const io::Json& m = j["m"];
+        if (m.size() > 0) {
+            h.m.resize(m.size());
+            for (size_t i = 0; i < m.size(); ++i) h.m[i] = m[i].as_double(0.0);
+        }
+        const io::Json& psi = j["psi"];
+        if (psi.size() > 0 && psi[0].size() > 0) {
+            const size_t rows = psi.size(), cols = psi[0].size();
+            h.psi.assign(rows * cols, 0.0);
+            for (size_t r = 0; r < rows; ++r)
+                for (size_t c = 0; c < cols; ++c) h.psi[c * rows + r] = psi[r][c].as_double(0.0);
+        }
+    } else {
+        const io::Json& a = j["alpha"];
+        if (a.size() > 0) {
+            h.alpha.resize(a.size());
+            for (size_t i = 0; i < a.size(); ++i) h.alpha[i] = a[i].as_double(0.0);
+        }
+    }
+    return h;
+}
+
+}  // namespace host
+}  // namespace dpmm
+
+using namespace dpmm;
+
+static host::Config config_from_run(const dpmm_run_desc* run, int64_t n, int32_t d)
+{
+    host::Config cfg;
+    cfg.prior = run->prior_type;
+    cfg.iterations = run->iterations > 0 ? run->iterations : 100;
+    cfg.initial_clusters = run->initial_clusters > 0 ? run->initial_clusters : 1;
+    cfg.burnout = run->burnout > 0 ? run->burnout : 15;
+    cfg.alpha = run->alpha;
+    cfg.max_clusters = run->max_clusters > 0 ? run->max_clusters : 1e300;
+    cfg.outlier_mod = run->outlier_weight;
+    cfg.seed = run->seed;
+    cfg.verbose = run->verbose != 0;
+    cfg.loglik_mode = run->loglik_mode;
+    cfg.rng_kind = run->rng_kind;
+    cfg.k_max = run->k_max;
+    cfg.device = run->device;
+    cfg.hyper = host::hyper_from_run(cfg.prior, d, run->niw_k, run->niw_v, run->niw_m, run->niw_psi, run->mult_alpha);
+    cfg.outlier_hyper = host::hyper_from_run(cfg.prior, d, run->out_niw_k, run->out_niw_v, run->out_niw_m,
+                                             run->out_niw_psi, run->out_mult_alpha);
+    if (run->gt) cfg.gt.assign(run->gt, run->gt + n);
+    return cfg;
+}
+
+extern "C" dpmm_status dpmm_dp_parallel(const dpmm_run_desc* run, int64_t n, int32_t d, const double* points,
+                                        dpmm_model_info** out)
+{
+    if (!run || !points || !out || n <= 0 || d <= 0) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    *out = nullptr;
+    return host::run_sampler(config_from_run(run, n, d), n, d, points, false, out);
+}
+
+struct dpmm_sampler {
+    std::unique_ptr<host::SamplerHandle> h;
+};
+
+extern "C" dpmm_status dpmm_sampler_create(const dpmm_run_desc* run, int64_t n, int32_t d, const void* points,
+                                           int32_t points_f32, dpmm_sampler** out)
+{
+    if (!run || !points || !out || n <= 0 || d <= 0) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    *out = nullptr;
+    auto s = std::make_unique<dpmm_sampler>();
+    DPMM_TRY(host::make_sampler(config_from_run(run, n, d), n, d, points, points_f32 != 0, s->h));
+    *out = s.release();
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sampler_step(dpmm_sampler* s, int32_t n_iters)
+{
+    if (!s || n_iters < 0) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    return s->h->sampler->step(n_iters, &s->h->mi);
+}
+
+extern "C" dpmm_status dpmm_sampler_num_clusters(const dpmm_sampler* s, int32_t* k)
+{
+    if (!s || !k) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    *k = s->h->sampler->num_clusters();
+    return DPMM_OK;
+}
+
+extern "C" void* dpmm_sampler_stream(const dpmm_sampler* s) { return s ? (void*)s->h->ctx->stream : nullptr; }
+
+extern "C" dpmm_ctx* dpmm_sampler_context(const dpmm_sampler* s) { return s ? s->h->ctx : nullptr; }
+
+extern "C" dpmm_status dpmm_sampler_model_info(dpmm_sampler* s, dpmm_model_info** out)
+{
+    if (!s || !out) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    DPMM_TRY(s->h->sampler->finish(&s->h->mi));
+    *out = new dpmm_model_info(s->h->mi);
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sampler_destroy(dpmm_sampler* s)
+{
+    delete s;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_dp_parallel_from_file(const char* npy_path, const char* params_path, int32_t prior_type,
+                                                  const dpmm_run_desc* ov, dpmm_model_info** out)
+{
+    if (!npy_path || !params_path || !out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    std::vector<double> pts;
+    int64_t rows = 0, cols = 0;
+    std::string err;
+    if (!io::read_npy(npy_path, pts, rows, cols, err)) return fail(DPMM_ERR_IO, err);
+    std::string text;
+    if (!io::read_file(params_path, text)) return fail(DPMM_ERR_IO, std::string("cannot read ") + params_path);
+    io::Json root;
+    if (!io::parse_json(text, root, err)) return fail(DPMM_ERR_IO, "params JSON: " + err);
+    const int D = (int)cols;
+    host::Config cfg;   // global_params.h:37-78 defaults, then global_params.cpp:25-65 keys
+    cfg.prior = prior_type;
+    cfg.burnout = 20;
+    cfg.outlier_mod = 0.05;
+    cfg.alpha = root["alpha"].as_double(10.0);
+    cfg.hyper = root["hyper_params"].is_null() ? host::default_hyper(prior_type, D)
+                                               : host::hyper_from_json(prior_type, D, root["hyper_params"]);
+    cfg.iterations = (int)root["iterations"].as_int(100);
+    cfg.initial_clusters = (int)root["initial_clusters"].as_int(1);
+    cfg.verbose = root["use_verbose"].as_bool(false);
+    cfg.burnout = (int)root["burnout_period"].as_int(20);
+    cfg.max_clusters = root["max_num_of_clusters"].as_double(1e300);
+    cfg.outlier_mod = root["outlier_mod"].as_double(0.05);
+    cfg.outlier_hyper = root["outlier_hyper_params"].is_null()
+                            ? host::default_hyper(prior_type, D)
+                            : host::hyper_from_json(prior_type, D, root["outlier_hyper_params"]);
+    cfg.seed = (uint64_t)root["randomSeed"].as_double(0);
+    const io::Json& gt = root["gt"];
+    for (size_t i = 0; i < gt.size(); ++i) cfg.gt.push_back((int32_t)gt[i].as_int(0));
+    // force_kernel (global_params.cpp:65): 1 -> SIMT FP32 contraction, 2 -> tensor cores
+    int fk = (int)root["force_kernel"].as_int(0);
+    cfg.loglik_mode = fk == 1 ? DPMM_LL_FP32 : fk == 2 ? DPMM_LL_TC_BF16X3 : DPMM_LL_AUTO;
+    if (ov) {
+        cfg.loglik_mode = ov->loglik_mode;
+        cfg.rng_kind = ov->rng_kind;
+        cfg.k_max = ov->k_max;
+        cfg.device = ov->device;
+        if (ov->seed) cfg.seed = ov->seed;
+    }
+    return host::run_sampler(cfg, rows, D, pts.data(), false, out);
+}
+
+extern "C" int64_t dpmm_model_info_n(const dpmm_model_info* mi) { return mi ? mi->n : 0; }
+extern "C" const int32_t* dpmm_model_info_labels(const dpmm_model_info* mi) { return mi ? mi->labels.data() : nullptr; }
+extern "C" int32_t dpmm_model_info_num_weights(const dpmm_model_info* mi) { return mi ? (int32_t)mi->weights.size() : 0; }
+extern "C" const double* dpmm_model_info_weights(const dpmm_model_info* mi) { return mi ? mi->weights.data() : nullptr; }
+extern "C" int32_t dpmm_model_info_iterations(const dpmm_model_info* mi) { return mi ? (int32_t)mi->iter_count.size() : 0; }
+extern "C" const double* dpmm_model_info_iter_count(const dpmm_model_info* mi) { return mi ? mi->iter_count.data() : nullptr; }
+extern "C" const double* dpmm_model_info_likelihood_history(const dpmm_model_info* mi)
+{
+    return mi ? mi->likelihood_history.data() : nullptr;
+}
+extern "C" const double* dpmm_model_info_nmi_history(const dpmm_model_info* mi)
+{
+    return (mi && !mi->nmi_history.empty()) ? mi->nmi_history.data() : nullptr;
+}
+extern "C" const int32_t* dpmm_model_info_cluster_count_history(const dpmm_model_info* mi)
+{
+    return mi ? mi->cluster_count_history.data() : nullptr;
+}
+
+extern "C" dpmm_status dpmm_model_info_write_json(const dpmm_model_info* mi, const char* path)
+{
+    if (!mi || !path) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    std::ofstream f(path);
+    if (!f) return fail(DPMM_ERR_IO, std::string("cannot write ") + path);
+    char buf[64];
+    f << "{\"labels\": [";
+    for (size_t i = 0; i < mi->labels.size(); ++i) f << (i ? ", " : "") << mi->labels[i];
+    f << "], \"weights\": [";
+    for (size_t i = 0; i < mi->weights.size(); ++i) {
+        std::snprintf(buf, sizeof(buf), "%.17g", mi->weights[i]);
+        f << (i ? ", " : "") << buf;
+    }
+    f << "], \"iter_count\": [";
+    for (size_t i = 0; i < mi->iter_count.size(); ++i) {
+        std::snprintf(buf, sizeof(buf), "%.9g", mi->iter_count[i]);
+        f << (i ? ", " : "") << buf;
+    }
+    f << "]}\n";
+    return f ? DPMM_OK : fail(DPMM_ERR_IO, "write failed");
+}
+
+extern "C" void dpmm_model_info_free(dpmm_model_info* mi) { delete mi; }

@@ -1,0 +1,322 @@
+/*
+ * dpmm_capi.h -- C ABI of the B200 (sm_100a) implementation of the per-iteration
+ * data-parallel path of the Chang & Fisher sub-cluster DPMM sampler.
+ *
+ * Two layers, both plain C (pointers, sizes, status codes; no C++ or torch types):
+ *
+ *  1. Device back-end (dpmm_ctx).  One entry point per method of the reference's
+ *     device back-end class `cudaKernel` (DPMMSubClusters/cudaKernel.cuh:31-138) and
+ *     its Gaussian / multinomial subclasses, so a C++ adapter deriving from
+ *     `cudaKernel` can forward every call here and `prior::get_cuda()`,
+ *     `local_clusters_actions::group_step` and `dp_parallel` stay unchanged.
+ *     Each declaration names the reference method it replaces (file:line).
+ *
+ *  2. Whole sampler (dpmm_model_info).  dpmm_dp_parallel / dpmm_dp_parallel_from_file
+ *     run the reference's iteration loop (dp_parallel_sampling.cpp:89-206) with this
+ *     back-end and return what `ModelInfo` holds (labels, weights, iter_count, ...).
+ *
+ * Conventions (same as the reference):
+ *   - points are point-major: the reference's Eigen D x N column-major matrix, i.e.
+ *     point n occupies points[n*D .. n*D+D-1];
+ *   - labels are 1-based int32; sub-labels are in {1, 2};
+ *   - square matrices (inv_sigma, psi, S) are D x D column-major (Eigen's default);
+ *   - uniforms are float in (0, 1], two per point per draw (u[2n], u[2n+1]), playing
+ *     the role of the two curand_uniform() calls of the reference's alias draw
+ *     (cudaKernel.cu:115-116).  A NULL uniforms pointer means "draw them on the device"
+ *     with the context's generator (Philox4x32-10, or cuRAND XORWOW in compat mode).
+ *
+ * Error convention: every function returns a dpmm_status; nothing calls exit().  The
+ * reference instead printf()s and exit(EXIT_FAILURE)s on any CUDA error
+ * (cudaKernel.cu:1492-1508).  dpmm_last_error() gives a message for the calling thread.
+ *
+ * Threading: a context is used by one host thread at a time; separate contexts may be
+ * driven from separate threads.  All device memory is allocated at dpmm_create (at
+ * capacity k_max); the phase calls do not allocate.
+ */
+#ifndef DPMM_CAPI_H
+#define DPMM_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DPMM_CAPI_VERSION 1
+
+typedef enum dpmm_status {
+    DPMM_OK = 0,
+    DPMM_ERR_INVALID_ARG = 1,
+    DPMM_ERR_OOM = 2,
+    DPMM_ERR_CUDA = 3,
+    DPMM_ERR_NOT_PD = 4,       /* a matrix that must be positive definite is not */
+    DPMM_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+    DPMM_ERR_NUMERIC = 6,      /* NaN / Inf in inputs or results */
+    DPMM_ERR_STATE = 7,        /* call out of order (e.g. no points uploaded) */
+    DPMM_ERR_IO = 8,           /* file could not be read / parsed */
+    DPMM_ERR_NO_DEVICE = 9
+} dpmm_status;
+
+/* prior_type (global_params.h:11-15) */
+typedef enum dpmm_prior_type { DPMM_PRIOR_GAUSSIAN = 0, DPMM_PRIOR_MULTINOMIAL = 1 } dpmm_prior_type;
+
+/* device random generator for draws whose uniforms the caller does not supply */
+typedef enum dpmm_rng_kind {
+    DPMM_RNG_PHILOX = 0,        /* counter-based Philox4x32-10: stateless, (seed, point, draw) */
+    DPMM_RNG_CURAND_XORWOW = 1  /* per-point curandStateXORWOW, curand_init(seed, point, 0):
+                                   the reference's stream and call order (cudaKernel.cu:19-25) */
+} dpmm_rng_kind;
+
+/* how the N x K log-likelihood contraction is computed */
+typedef enum dpmm_loglik_mode {
+    DPMM_LL_FP32 = 0,           /* SIMT FP32 ("plain FP32 form") */
+    DPMM_LL_TC_BF16X3 = 1,      /* tcgen05 tensor cores, split-BF16 (hi*hi + lo*hi + hi*lo), FP32 accumulate */
+    DPMM_LL_AUTO = 2            /* tensor cores where the shape allows, else FP32 */
+} dpmm_loglik_mode;
+
+typedef struct dpmm_desc {
+    int64_t n_points;     /* N */
+    int32_t dim;          /* D */
+    int32_t prior_type;   /* dpmm_prior_type */
+    int32_t k_max;        /* capacity for clusters (0 -> 256) */
+    int32_t rng_kind;     /* dpmm_rng_kind */
+    uint64_t seed;        /* device generator seed */
+    int32_t loglik_mode;  /* dpmm_loglik_mode */
+    int32_t device;       /* CUDA device ordinal */
+    int32_t verbose;
+    int32_t reserved[7];
+} dpmm_desc;
+
+typedef struct dpmm_ctx dpmm_ctx;
+
+const char* dpmm_status_string(dpmm_status s);
+/* message of the last failing call on this host thread ("" if none) */
+const char* dpmm_last_error(void);
+int dpmm_capi_version(void);
+
+/* ------------------------------------------------------------------ device back-end */
+
+/* cudaKernel::init (cudaKernel.cu:537-635).  Unlike the reference it does not call
+ * cudaDeviceReset, so several contexts (samplers) can share a device. */
+dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out);
+/* cudaKernel::release (cudaKernel.cu:691-720) */
+dpmm_status dpmm_destroy(dpmm_ctx* ctx);
+
+/* The H2D copy of the points inside cudaKernel::init (cudaKernel.cu:622-626).
+ * points: N*D values, point-major. */
+dpmm_status dpmm_upload_points(dpmm_ctx* ctx, const double* points);
+dpmm_status dpmm_upload_points_f32(dpmm_ctx* ctx, const float* points);
+
+/* cudaKernel::sample_labels (cudaKernel.cu:1103-1111): labels uniform in
+ * [1 + o, initial_clusters + o], o = (outlier_mod > 0). */
+dpmm_status dpmm_sample_labels(dpmm_ctx* ctx, int initial_clusters, double outlier_mod,
+                               const float* uniforms /* N or NULL */);
+/* cudaKernel::sample_sub_labels (cudaKernel.cu:1093-1101) */
+dpmm_status dpmm_sample_sub_labels(dpmm_ctx* ctx, const float* uniforms /* N or NULL */);
+
+/* cudaKernel::update_labels (cudaKernel.cu:1145-1148); the set_labels / set_sub_labels
+ * seams of the reference's test double (test/myCudaKernel.h). */
+dpmm_status dpmm_set_labels(dpmm_ctx* ctx, const int32_t* labels);
+dpmm_status dpmm_set_sub_labels(dpmm_ctx* ctx, const int32_t* sub_labels);
+/* cudaKernel::get_labels / get_sub_labels (cudaKernel.cu:1113-1143) */
+dpmm_status dpmm_get_labels(dpmm_ctx* ctx, int32_t* labels);
+dpmm_status dpmm_get_sub_labels(dpmm_ctx* ctx, int32_t* sub_labels);
+/* cudaKernel::get_sub_labels_count (cudaKernel.cu:1237-1257) */
+dpmm_status dpmm_get_sub_labels_count(dpmm_ctx* ctx, int32_t* l, int32_t* r);
+
+/* Cluster parameters for the next label / sub-label phase: the thin_cluster_params
+ * broadcast (local_clusters_actions.cpp:373-382, 449-458) plus the per-cluster H2D copies
+ * the reference makes inside cudaKernel_gaussian::log_likelihood_labels / _sub_labels
+ * (cudaKernel_gaussian.cu:43-113).
+ *   mu[K*D], inv_sigma[K*D*D] (col-major), logdet_sigma[K], weights[K]: cluster k;
+ *   mu_lr[2K*D], inv_sigma_lr[2K*D*D], logdet_sigma_lr[2K], lr_weights[2K]: sub-cluster
+ *   (k, s) at index 2k+s, s = 0 (l) / 1 (r).
+ * The precision matrices are factored on the host (FP64 Cholesky, inv_sigma = W W^T);
+ * a matrix that is not positive definite gives DPMM_ERR_NOT_PD. */
+dpmm_status dpmm_set_gaussian_params(dpmm_ctx* ctx, int K, const double* mu,
+                                     const double* inv_sigma, const double* logdet_sigma,
+                                     const double* weights, const double* mu_lr,
+                                     const double* inv_sigma_lr, const double* logdet_sigma_lr,
+                                     const double* lr_weights);
+/* Same, given precision square-root factors W (inv_sigma = W W^T, D x D col-major, any such
+ * factor), as the Bartlett draw of niw::sample_distribution (niw.cpp:61-107) produces directly;
+ * no host factorisation is done. */
+dpmm_status dpmm_set_gaussian_factors(dpmm_ctx* ctx, int K, const double* mu, const double* w,
+                                      const double* logdet_sigma, const double* weights,
+                                      const double* mu_lr, const double* w_lr,
+                                      const double* logdet_sigma_lr, const double* lr_weights);
+/* multinomial_dist{alpha = log theta} per cluster / sub-cluster (cudaKernel_multinomial.cu:37-76);
+ * weights are accepted but, as in the reference, do not enter the label log-likelihood. */
+dpmm_status dpmm_set_multinomial_params(dpmm_ctx* ctx, int K, const double* log_theta,
+                                        const double* weights, const double* log_theta_lr,
+                                        const double* lr_weights);
+
+/* cudaKernel::create_clusters_labels (cudaKernel.cu:1400-1490): N x K log-likelihood,
+ * softmax and Walker-alias draw per point (argmax when final != 0), fused in one kernel;
+ * the N x K matrix never reaches memory.
+ *   uniforms: 2N or NULL.  loglik_out (test seam, nullable): N x K point-major, each
+ *   value WITHOUT the cluster-independent constant -D*D*log(2*pi)/2 (Gaussian). */
+dpmm_status dpmm_create_clusters_labels(dpmm_ctx* ctx, int K, int final_, const float* uniforms,
+                                        float* loglik_out);
+/* cudaKernel::create_subclusters_labels (cudaKernel.cu:1299-1398): for every point its two
+ * sub-cluster log-likelihoods (+ log lr_weights), 2-way softmax and alias draw, using the
+ * labels of the last label phase.  Fused with the sufficient-statistic reduction of
+ * dpmm_create_sufficient_statistics (results kept on the device and returned by it).
+ *   loglik_out (nullable): N x 2 point-major, without the -D*D*log(2*pi)/2 constant. */
+dpmm_status dpmm_create_subclusters_labels(dpmm_ctx* ctx, int K, const float* uniforms,
+                                           float* loglik_out);
+/* cudaKernel::create_sufficient_statistics (cudaKernel.cu:844-941): for each of the n
+ * listed clusters (0-based indices) the statistics of the cluster (slot 3i), its l (3i+1)
+ * and r (3i+2) sub-clusters: count, sum x (D) and, Gaussian only, the uncentred scatter
+ * S = sum x x^T (D x D).  Any output pointer may be NULL.  Computed from the current labels
+ * and sub-labels with a deterministic segmented reduction (FP32 within a chunk of points,
+ * shifted; FP64 across chunks). */
+dpmm_status dpmm_create_sufficient_statistics(dpmm_ctx* ctx, int n, const int32_t* indices,
+                                              int64_t* count, double* sum, double* S);
+
+/* cudaKernel::split_cluster_local_worker (cudaKernel.cu:1204-1214), applied for each pair in
+ * order: in cluster index[i], sub==2 points move to new_index[i]; every point of it gets a
+ * fresh random sub-label (curand()%2+1).  bits (nullable, N values) stands for curand(). */
+dpmm_status dpmm_split_clusters(dpmm_ctx* ctx, int n, const int32_t* index, const int32_t* new_index,
+                                const uint32_t* bits);
+/* cudaKernel::merge_clusters_worker (cudaKernel.cu:1215-1225), each pair in order */
+dpmm_status dpmm_merge_clusters(dpmm_ctx* ctx, int n, const int32_t* index, const int32_t* new_index);
+/* cudaKernel::reset_bad_clusters_worker (cudaKernel.cu:1226-1236), each index in order */
+dpmm_status dpmm_reset_bad_clusters(dpmm_ctx* ctx, int n, const int32_t* index, const uint32_t* bits);
+/* cudaKernel::remove_empty_clusters_worker (cudaKernel.cu:1194-1203) called once per limit,
+ * in order (labels > limit are decremented); applied as one relabel pass. */
+dpmm_status dpmm_remove_empty_clusters(dpmm_ctx* ctx, int n, const int32_t* limits);
+
+/* Test seams of the reference's test double (test/myCudaKernel.h):
+ * cudaKernel_gaussian::log_likelihood_labels (cudaKernel_gaussian.cu:82-113) for one cluster,
+ * r_out[N] in FP64 INCLUDING the -D*D*log(2*pi)/2 constant; */
+dpmm_status dpmm_log_likelihood_labels_gaussian(dpmm_ctx* ctx, const double* mu,
+                                                const double* inv_sigma, double logdet_sigma,
+                                                double weight, double* r_out);
+/* cudaKernel_multinomial::log_likelihood_labels (cudaKernel_multinomial.cu:60-76) */
+dpmm_status dpmm_log_likelihood_labels_multinomial(dpmm_ctx* ctx, const double* log_theta,
+                                                   double* r_out);
+/* cudaKernel::sample_log_cat_array (cudaKernel.cu:805-829): softmax + alias draw of labels
+ * from a caller-given N x K column-major log-likelihood matrix (FP64 arithmetic). */
+dpmm_status dpmm_sample_log_cat_array(dpmm_ctx* ctx, int K, const double* loglik,
+                                      const float* uniforms);
+/* cudaKernel::sample_log_cat_array_sub_cluster (cudaKernel.cu:775-803): m points with
+ * indices[m], loglik m x 2 column-major, lr_weights[2]; writes their sub-labels. */
+dpmm_status dpmm_sample_log_cat_array_sub_cluster(dpmm_ctx* ctx, int m, const double* loglik,
+                                                  const int32_t* indices, const double* lr_weights,
+                                                  const float* uniforms);
+
+/* ---- split / merge Hastings in one launch each (FP64 on the device) -------------------- */
+
+/* Prior hyper-parameters: niw_hyperparams{k, m, v, psi} (priors/niw_hyperparams.h:9-43) or
+ * multinomial_hyper{alpha} (priors/multinomial_hyper.h:9-29). */
+dpmm_status dpmm_set_prior_niw(dpmm_ctx* ctx, double k, const double* m, double v, const double* psi);
+dpmm_status dpmm_set_prior_multinomial(dpmm_ctx* ctx, const double* alpha);
+
+/* For the K clusters whose statistics the last dpmm_create_subclusters_labels /
+ * dpmm_create_sufficient_statistics left on the device: the posterior of the cluster and
+ * of its two sub-clusters (niw.cpp:23-49 / multinomial_prior.cpp:12-22), their log
+ * marginal likelihoods (niw.cpp:122-138 / multinomial_prior.cpp:56-67) into lml[3K]
+ * (slots 3k, 3k+1, 3k+2), and the split log Hastings ratio of each cluster
+ * (local_clusters_actions.cpp:222-233) into split_log_hr[K] (NaN where N_l or N_r is 0). */
+dpmm_status dpmm_split_hastings(dpmm_ctx* ctx, int K, double alpha, double* lml, double* split_log_hr);
+/* Merge log Hastings ratio (shared_actions.cpp:88-111) of every pair i < j of the K clusters
+ * in one launch: merge_log_hr[i*K + j] (row-major; entries with i >= j or an empty cluster
+ * are NaN).  Uses the cluster-level statistics on the device. */
+dpmm_status dpmm_merge_hastings(dpmm_ctx* ctx, int K, double alpha, double* merge_log_hr);
+
+/* Synchronise the context's stream; returns any pending device error. */
+dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
+
+/* Diagnostics (no counterpart in the reference, which prints per-iteration wall times only):
+ * kernels this library has launched in this process; bytes it copied host->device and
+ * device->host; device time per phase of a context (ms[8], calls[8]: labels, sub-labels +
+ * statistics, statistics only, split ratios, merge ratios, relabels, parameters, -) accumulated
+ * while timing is on.  enable = 1 / 0 switches timing on / off and clears the counters, -1 only
+ * reads them.  Timing adds one event synchronisation per phase. */
+uint64_t dpmm_kernel_launch_count(void);
+void dpmm_transfer_bytes(uint64_t* h2d, uint64_t* d2h);
+dpmm_status dpmm_phase_times(dpmm_ctx* ctx, int enable, double* ms, int64_t* calls);
+
+/* ------------------------------------------------------------------ whole sampler */
+
+/* Arguments of dp_parallel_sampling_class::dp_parallel (dp_parallel_sampling.h:17-29) and the
+ * --params_path JSON keys (global_params.cpp:25-65). */
+typedef struct dpmm_run_desc {
+    int32_t prior_type;          /* dpmm_prior_type */
+    int32_t iterations;          /* iters (default 100) */
+    int32_t initial_clusters;    /* init_clusters (default 1) */
+    int32_t burnout;             /* burnout_period (default 15 via dp_parallel, 20 via JSON) */
+    double alpha;                /* concentration */
+    double max_clusters;         /* max_num_of_clusters (<= 0 -> unlimited) */
+    double outlier_weight;       /* outlier_mod */
+    uint64_t seed;               /* randomSeed (0 -> time based, as the reference) */
+    int32_t verbose;             /* use_verbose: log posterior (+ NMI with gt) per iteration */
+    int32_t loglik_mode;         /* dpmm_loglik_mode */
+    int32_t rng_kind;            /* dpmm_rng_kind */
+    int32_t k_max;               /* cluster capacity (0 -> 256) */
+    /* hyper_params: NIW (k, m[D], v, psi[D*D]) or multinomial alpha[D]; NULL -> defaults */
+    double niw_k, niw_v;
+    const double* niw_m;
+    const double* niw_psi;
+    const double* mult_alpha;
+    /* outlier_hyper_params (same layout); NULL -> defaults */
+    double out_niw_k, out_niw_v;
+    const double* out_niw_m;
+    const double* out_niw_psi;
+    const double* out_mult_alpha;
+    const int32_t* gt;           /* ground-truth labels for NMI (nullable) */
+    int32_t device;
+    int32_t reserved[7];
+} dpmm_run_desc;
+
+typedef struct dpmm_model_info dpmm_model_info;
+
+/* Step-wise form of the same run: dpmm_sampler_create does what the constructor, init_model and
+ * init_first_clusters do (dp_parallel_sampling.cpp:19-23, 48-87); each dpmm_sampler_step runs
+ * n iterations of run_model's loop (dp_parallel_sampling.cpp:139-200), counting iterations from
+ * 1 to run->iterations exactly as the reference does (argmax labels and no more split / merge
+ * moves in the last 5).  points: N*D point-major, in host or device memory (any address the
+ * CUDA runtime can copy from); points_f32 selects float instead of double. */
+typedef struct dpmm_sampler dpmm_sampler;
+dpmm_status dpmm_sampler_create(const dpmm_run_desc* run, int64_t n, int32_t d, const void* points,
+                                int32_t points_f32, dpmm_sampler** out);
+dpmm_status dpmm_sampler_step(dpmm_sampler* s, int32_t n_iters);
+dpmm_status dpmm_sampler_num_clusters(const dpmm_sampler* s, int32_t* k);
+/* stream of the sampler's device work (cudaStream_t), for timing with events */
+void* dpmm_sampler_stream(const dpmm_sampler* s);
+/* the device back-end context the sampler drives (for dpmm_phase_times) */
+dpmm_ctx* dpmm_sampler_context(const dpmm_sampler* s);
+/* ModelInfo of the iterations run so far (labels copied from the device) */
+dpmm_status dpmm_sampler_model_info(dpmm_sampler* s, dpmm_model_info** out);
+dpmm_status dpmm_sampler_destroy(dpmm_sampler* s);
+
+/* dp_parallel_sampling_class(N, x, seed, prior) + dp_parallel(...) (dp_parallel_sampling.cpp:19-23,
+ * 89-117).  points: N*D point-major. */
+dpmm_status dpmm_dp_parallel(const dpmm_run_desc* run, int64_t n, int32_t d, const double* points,
+                             dpmm_model_info** out);
+/* dp_parallel_sampling_class(npy, json, prior) + dp_parallel_from_file() (dp_parallel_sampling.cpp:25-31,
+ * 119-122): reads an N x D .npy (float64 / float32 / int32 / int64 / uint8 / uint16 / bf16 counts
+ * read exactly) and the params JSON (accepts // comments). */
+dpmm_status dpmm_dp_parallel_from_file(const char* npy_path, const char* params_path, int32_t prior_type,
+                                       const dpmm_run_desc* overrides /* nullable */,
+                                       dpmm_model_info** out);
+/* ModelInfo accessors (modelInfo.h:45-56).  Arrays stay valid until dpmm_model_info_free. */
+int64_t dpmm_model_info_n(const dpmm_model_info* mi);
+const int32_t* dpmm_model_info_labels(const dpmm_model_info* mi);
+int32_t dpmm_model_info_num_weights(const dpmm_model_info* mi);
+const double* dpmm_model_info_weights(const dpmm_model_info* mi);
+int32_t dpmm_model_info_iterations(const dpmm_model_info* mi);
+const double* dpmm_model_info_iter_count(const dpmm_model_info* mi);
+const double* dpmm_model_info_likelihood_history(const dpmm_model_info* mi);
+const double* dpmm_model_info_nmi_history(const dpmm_model_info* mi);  /* NULL without gt */
+const int32_t* dpmm_model_info_cluster_count_history(const dpmm_model_info* mi);
+/* write {"labels": [...], "weights": [...], "iter_count": [...]} as main.cpp:72-87 does */
+dpmm_status dpmm_model_info_write_json(const dpmm_model_info* mi, const char* path);
+void dpmm_model_info_free(dpmm_model_info* mi);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DPMM_CAPI_H */
