@@ -147,7 +147,7 @@ static void free_ctx(dpmm_ctx* c)
     void* bufs[] = {c->d_x, c->d_gshift, c->d_labels, c->d_sub, c->d_curand, c->d_Wt, c->d_b, c->d_c, c->d_lrw,
                     c->d_mu, c->d_perm, c->d_blk_hist, c->d_seg, c->d_chunk, c->d_nchunks, c->d_part, c->d_stats,
                     c->d_u, c->d_bits, c->d_remap, c->d_aux, c->d_r64, c->d_dbl_scratch, c->d_prior, c->d_lml,
-                    c->d_split_hr, c->d_merge_hr, c->d_post_logdet};
+                    c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -221,6 +221,7 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     if (gauss) {
         chk(dev_alloc(&c->d_Wt, (size_t)3 * KM * Dp * Dp));
         chk(dev_alloc(&c->d_b, (size_t)3 * KM * Dp));
+        if (Dp == 32 || Dp == 64) chk(dev_alloc(&c->d_Btc, (size_t)(KM + 1) / 2 * 32768));
     }
     chk(dev_alloc(&c->d_c, (size_t)3 * KM));
     chk(dev_alloc(&c->d_lrw, (size_t)2 * KM));
@@ -232,6 +233,8 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     chk(dev_alloc(&c->d_part, (size_t)c->max_chunks * 2 * SL));
     chk(dev_alloc(&c->d_stats, (size_t)3 * KM * c->stat_len));
     chk(dev_alloc(&c->d_remap, (size_t)KM + 2));
+    chk(dev_alloc(&c->d_mask, (size_t)KM));
+    c->stats_ok.assign(KM, 0);
     chk(dev_alloc(&c->d_aux, (size_t)KM + 16));
     chk(dev_alloc(&c->d_dbl_scratch, (size_t)std::max(2 + c->D + c->D * c->D, 4 * KM) + 64));
     chk(dev_alloc(&c->d_prior, (size_t)(gauss ? c->D + c->D * c->D : c->D)));
@@ -332,7 +335,7 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
     if (bad) return fail(DPMM_ERR_NUMERIC, "points contain NaN or Inf");
     c->points_ready = true;
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -356,7 +359,7 @@ extern "C" dpmm_status dpmm_sample_labels(dpmm_ctx* c, int initial_clusters, dou
     const float* du;
     DPMM_TRY(stage_uniforms(c, u, c->N, &du));
     DPMM_TRY(launch_labels_init(c, initial_clusters, outlier_mod, du));
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -366,7 +369,7 @@ extern "C" dpmm_status dpmm_sample_sub_labels(dpmm_ctx* c, const float* u)
     const float* du;
     DPMM_TRY(stage_uniforms(c, u, c->N, &du));
     DPMM_TRY(launch_sub_labels_init(c, du));
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -376,7 +379,7 @@ extern "C" dpmm_status dpmm_set_labels(dpmm_ctx* c, const int32_t* labels)
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_labels, labels, sizeof(int32_t) * c->N, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -385,7 +388,7 @@ extern "C" dpmm_status dpmm_set_sub_labels(dpmm_ctx* c, const int32_t* sub)
     if (!c || !sub) return fail(DPMM_ERR_INVALID_ARG, "null argument");
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_sub, sub, sizeof(int32_t) * c->N, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -483,6 +486,10 @@ static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, con
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, hmu, sizeof(float) * 3 * K * (size_t)Dp, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hlrw.data(), sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
     g_h2d_bytes += sizeof(float) * 3 * (size_t)K * ((size_t)Dp * Dp + 2 * Dp + 1) + sizeof(float) * 2 * K;
+    {
+        PhaseTimer pt(c, PH_PARAMS);
+        DPMM_TRY(pack_tc_params(c, K));
+    }
     c->K_params = K;
     return DPMM_OK;
 }
@@ -570,7 +577,7 @@ extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final
         if (e != cudaSuccess) s = cuda_status(e, "dpmm_create_clusters_labels");
     }
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     return s;
 }
 
@@ -611,11 +618,8 @@ extern "C" dpmm_status dpmm_create_sufficient_statistics(dpmm_ctx* c, int n, con
     // statistics are (re)computed for every current cluster, so that the Hastings launches
     // that follow see all of them; each cluster's accumulation is shifted by its mean parameter
     const int Keff = std::min(c->k_max, std::max(K, c->K_params));
-    if (c->stats_K < Keff) {
-        PhaseTimer pt(c, PH_STATS);
-        DPMM_TRY(launch_sub_labels_and_stats(c, Keff, nullptr, nullptr, false));
-    }
-    g_d2h_bytes += sizeof(double) * 3 * (size_t)Keff * c->stat_len;
+    DPMM_TRY(ensure_stats(c, Keff));
+    g_d2h_bytes += sizeof(double) * 3 * (size_t)K * c->stat_len;
     const int L = c->stat_len, D = c->D;
     double* h = c->h_pinned;
     DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_stats, sizeof(double) * 3 * (size_t)K * L, cudaMemcpyDeviceToHost, c->stream));
@@ -671,7 +675,10 @@ extern "C" dpmm_status dpmm_split_clusters(dpmm_ctx* c, int n, const int32_t* in
         table[index[i] + 1] = new_index[i] + 1;
         if (seq || i == n - 1) DPMM_TRY(launch_relabel(c, 0, 0, table.data(), tlen, db));
     }
-    c->stats_K = -1;
+    for (int i = 0; i < n; ++i) {
+        invalidate_stats(c, index[i]);
+        invalidate_stats(c, new_index[i]);
+    }
     return DPMM_OK;
 }
 
@@ -690,7 +697,10 @@ extern "C" dpmm_status dpmm_merge_clusters(dpmm_ctx* c, int n, const int32_t* in
         table[new_index[i] + 1] = -(index[i] + 1);
         if (seq || i == n - 1) DPMM_TRY(launch_relabel(c, 1, 0, table.data(), tlen, nullptr));
     }
-    c->stats_K = -1;
+    for (int i = 0; i < n; ++i) {
+        invalidate_stats(c, index[i]);
+        invalidate_stats(c, new_index[i]);
+    }
     return DPMM_OK;
 }
 
@@ -716,7 +726,7 @@ extern "C" dpmm_status dpmm_reset_bad_clusters(dpmm_ctx* c, int n, const int32_t
     } else {
         DPMM_TRY(launch_relabel(c, 2, 0, table.data(), tlen, db));
     }
-    c->stats_K = -1;
+    for (int i = 0; i < n; ++i) invalidate_stats(c, index[i]);
     return DPMM_OK;
 }
 
@@ -733,7 +743,7 @@ extern "C" dpmm_status dpmm_remove_empty_clusters(dpmm_ctx* c, int n, const int3
         table[v] = x;
     }
     DPMM_TRY(launch_relabel(c, 3, 0, table.data(), tlen, nullptr));
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -785,7 +795,7 @@ extern "C" dpmm_status dpmm_sample_log_cat_array(dpmm_ctx* c, int K, const doubl
     }
     cudaFree(d_r);
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     return s;
 }
 
@@ -815,7 +825,7 @@ extern "C" dpmm_status dpmm_sample_log_cat_array_sub_cluster(dpmm_ctx* c, int m,
     }
     cudaFree(d_r);
     if (d_idx) cudaFree(d_idx);
-    c->stats_K = -1;
+    invalidate_stats(c);
     return s;
 }
 
@@ -889,7 +899,7 @@ dpmm_status launch_fill_labels(dpmm_ctx* c, int32_t value)
     k_fill_i32<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->d_labels, c->N, value);
     DPMM_CUDA_TRY(cudaGetLastError());
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     return DPMM_OK;
 }
 
@@ -911,18 +921,54 @@ dpmm_status all_points_stats(dpmm_ctx* c, int64_t* count, double* sum, double* S
     int64_t cnt[3];
     const int D = c->D;
     std::vector<double> sm(3 * (size_t)D), SS(c->prior == DPMM_PRIOR_GAUSSIAN ? 3 * (size_t)D * D : 0);
-    c->stats_K = -1;
+    invalidate_stats(c);
     dpmm_status st = dpmm_create_sufficient_statistics(c, 1, &idx, cnt, sm.data(), SS.empty() ? nullptr : SS.data());
     c->K_params = kp;
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, keep.data(), sizeof(float) * c->Dp, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_labels, saved, sizeof(int32_t) * c->N, cudaMemcpyDeviceToDevice, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->perm_K = -1;
-    c->stats_K = -1;
+    invalidate_stats(c);
     DPMM_TRY(st);
     if (count) *count = cnt[0];
     if (sum) std::memcpy(sum, sm.data(), sizeof(double) * D);
     if (S && !SS.empty()) std::memcpy(S, SS.data(), sizeof(double) * D * D);
+    return DPMM_OK;
+}
+
+}  // namespace dpmm
+
+namespace dpmm {
+
+void invalidate_stats(dpmm_ctx* c)
+{
+    c->stats_K = -1;
+    std::fill(c->stats_ok.begin(), c->stats_ok.end(), 0);
+}
+
+void invalidate_stats(dpmm_ctx* c, int k)
+{
+    if (k >= 0 && k < (int)c->stats_ok.size()) c->stats_ok[k] = 0;
+}
+
+dpmm_status ensure_stats(dpmm_ctx* c, int K)
+{
+    if (K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K above capacity");
+    int missing = 0;
+    for (int k = 0; k < K; ++k) missing += !c->stats_ok[k];
+    if (!missing) return DPMM_OK;
+    PhaseTimer pt(c, PH_STATS);
+    if (c->stats_K < 0 || missing == K) {
+        DPMM_TRY(launch_sub_labels_and_stats(c, K, nullptr, nullptr, false));
+        return DPMM_OK;
+    }
+    std::vector<uint8_t> m(K);
+    for (int k = 0; k < K; ++k) m[k] = !c->stats_ok[k];
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mask, m.data(), K, cudaMemcpyHostToDevice, c->stream));
+    DPMM_TRY(launch_sub_labels_and_stats(c, K, nullptr, nullptr, false, c->d_mask));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));   // the host mask must outlive the copy
+    for (int k = 0; k < K; ++k) c->stats_ok[k] = 1;
+    c->stats_K = std::max(c->stats_K, K);
     return DPMM_OK;
 }
 

@@ -121,9 +121,10 @@ __global__ void __launch_bounds__(kHThreads) k_slot_lml(const double* __restrict
                                                         double* __restrict__ lml)
 {
     extern __shared__ double sh[];
-    double* psi = sh;                 // D*D
-    double* mp = psi + (size_t)D * D; // D
-    double* red = mp + D;             // 33
+    // NIW: psi'[D*D], m'[D], reduction[33]; multinomial: reduction[33] only
+    double* psi = sh;
+    double* mp = gauss ? psi + (size_t)D * D : sh;
+    double* red = gauss ? mp + D : sh;
     const double* st = stats + (size_t)blockIdx.x * stat_len;
     double v;
     if (gauss)
@@ -152,9 +153,9 @@ __global__ void __launch_bounds__(kHThreads) k_merge_hr(const double* __restrict
                                                         double* __restrict__ hr)
 {
     extern __shared__ double sh[];
-    double* psi = sh;                     // D*D
-    double* mp = psi + (size_t)D * D;     // D
-    double* red = mp + D;                 // 33
+    double* psi = sh;
+    double* mp = gauss ? psi + (size_t)D * D : sh;
+    double* red = gauss ? mp + D : sh;
     // unrank pair b -> (i, j), i < j, row-major over the strict upper triangle
     long long b = blockIdx.x;
     int i = 0;
@@ -185,14 +186,14 @@ static size_t hastings_smem(const dpmm_ctx* c, bool merge)
 {
     (void)merge;
     const size_t D = c->D;
-    size_t s = c->prior == DPMM_PRIOR_GAUSSIAN ? D * D + D + 33 : D + 33;
+    size_t s = c->prior == DPMM_PRIOR_GAUSSIAN ? D * D + D + 33 : 33;
     return s * sizeof(double);
 }
 
 dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha)
 {
     if (!c->prior_set) return fail(DPMM_ERR_STATE, "prior hyper-parameters not set");
-    if (c->stats_K < K) return fail(DPMM_ERR_STATE, "statistics not computed for K clusters");
+    DPMM_TRY(ensure_stats(c, K));
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     const double ld0 = c->prior_logdet;
     size_t sm = hastings_smem(c, false);
@@ -208,7 +209,7 @@ dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha)
 dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha)
 {
     if (!c->prior_set) return fail(DPMM_ERR_STATE, "prior hyper-parameters not set");
-    if (c->stats_K < K) return fail(DPMM_ERR_STATE, "statistics not computed for K clusters");
+    DPMM_TRY(ensure_stats(c, K));
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     const double ld0 = c->prior_logdet;
     // cluster-level lml of every cluster (slots 3k only are needed; all 3K are cheap)

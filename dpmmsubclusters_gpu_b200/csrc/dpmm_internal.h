@@ -100,6 +100,8 @@ struct dpmm_ctx {
                                    // 0 for the multinomial prior (no weight term)
     float* d_lrw = nullptr;        // [2*k_max] log lr_weights
     float* d_mu = nullptr;         // [3*k_max][Dp], mu - shift (Gaussian) / log theta (multinomial)
+    uint8_t* d_Btc = nullptr;      // tensor-core B operand: per pair of clusters a 32 KB split-bf16,
+                                   // K-major 128-byte-swizzled tile (Gaussian, Dp = 32 or 64)
     std::vector<float> h_param_stage;
 
     // label-ordered permutation of the points and the per-cluster chunk table
@@ -116,7 +118,9 @@ struct dpmm_ctx {
     double* d_part = nullptr;      // [max_chunks][2][stat_len]
     double* d_stats = nullptr;     // [3*k_max][stat_len]: count, sum[D], S[D*D] (col-major)
     int stat_len = 0;              // 1 + D + D*D (Gaussian) / 1 + D (multinomial)
-    int stats_K = -1;
+    int stats_K = -1;              // clusters 0..stats_K-1 have statistics on the device ...
+    std::vector<uint8_t> stats_ok; // ... and stats_ok[k] says whether they are still current
+    uint8_t* d_mask = nullptr;     // [k_max] clusters selected for a partial recompute
 
     // uniforms / random bits supplied by the caller, staged on the device
     float* d_u = nullptr;          // 2N
@@ -175,8 +179,13 @@ dpmm_status launch_labels_init(dpmm_ctx* c, int initial_clusters, double outlier
 dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u);
 dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 dpmm_status build_permutation(dpmm_ctx* c, int K);
-dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw);
-dpmm_status launch_stats_finalize(dpmm_ctx* c, int K);
+dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw,
+                                        const uint8_t* d_mask = nullptr);
+dpmm_status launch_stats_finalize(dpmm_ctx* c, int K, const uint8_t* d_mask);
+// recompute the statistics of every cluster k < K that is not current (all of them if none is)
+dpmm_status ensure_stats(dpmm_ctx* c, int K);
+void invalidate_stats(dpmm_ctx* c);
+void invalidate_stats(dpmm_ctx* c, int k);
 dpmm_status launch_relabel(dpmm_ctx* c, int mode, int K, const int32_t* h_table, int table_len,
                            const uint32_t* d_bits);
 dpmm_status launch_sub_count(dpmm_ctx* c, int32_t* h_l, int32_t* h_r);
@@ -191,6 +200,7 @@ dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha);
 // tensor-core label kernel (dpmm_tc.cu); returns DPMM_ERR_INVALID_ARG when the shape is unsupported
 bool tc_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
+dpmm_status pack_tc_params(dpmm_ctx* c, int K);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)

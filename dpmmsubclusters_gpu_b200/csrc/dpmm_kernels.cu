@@ -453,7 +453,8 @@ __global__ void __launch_bounds__(256) k_gauss_sub_stats(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const float* __restrict__ Wt, const float* __restrict__ bvec,
     const float* __restrict__ cvec, const float* __restrict__ lrw, const float* __restrict__ muv, int draw,
-    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part)
+    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part,
+    const uint8_t* __restrict__ mask)
 {
     constexpr int T = tri(DP);
     constexpr int E = (T + 255) / 256;       // scatter entries per thread
@@ -471,6 +472,7 @@ __global__ void __launch_bounds__(256) k_gauss_sub_stats(
     const int ch = blockIdx.x;
     if (ch >= *nchunks) return;
     const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    if (mask && !mask[k]) return;
     const int tid = threadIdx.x;
 
     if (draw) {
@@ -619,7 +621,8 @@ __global__ void __launch_bounds__(256) k_gauss_sub_stats(
 __global__ void __launch_bounds__(256) k_mult_sub_stats(
     const float* __restrict__ x, int Dp, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const float* __restrict__ logtheta, const float* __restrict__ lrw, int draw,
-    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part, int SL)
+    RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part, int SL,
+    const uint8_t* __restrict__ mask)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     float* tl = reinterpret_cast<float*>(smem);   // Dp
@@ -630,6 +633,7 @@ __global__ void __launch_bounds__(256) k_mult_sub_stats(
     const int ch = blockIdx.x;
     if (ch >= *nchunks) return;
     const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    if (mask && !mask[k]) return;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     for (int e = tid; e < Dp; e += 256) {
         tl[e] = logtheta[(size_t)(3 * k + 1) * Dp + e];
@@ -685,7 +689,7 @@ __global__ void __launch_bounds__(256) k_mult_sub_stats(
 }
 
 template <int DP>
-static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout)
+static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout, const uint8_t* d_mask)
 {
     constexpr int TP = DP >= 128 ? 128 : 256;
     size_t sm = sizeof(float) * (2 * DP * DP + 3 * DP + TP * (DP + 1)) + sizeof(int32_t) * TP +
@@ -693,23 +697,24 @@ static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, fl
     auto kern = k_gauss_sub_stats<DP, TP>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c,
-                                                c->d_lrw, c->d_mu, draw, r, c->d_sub, d_rout, c->d_part);
+                                                c->d_lrw, c->d_mu, draw, r, c->d_sub, d_rout, c->d_part, d_mask);
     DPMM_LAUNCHED();
     return DPMM_OK;
 }
 
-dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw)
+dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw,
+                                        const uint8_t* d_mask)
 {
     if (c->perm_K != K) DPMM_TRY(build_permutation(c, K));
     RngArgs r = rng_args(c, d_u);
     if (c->prior == DPMM_PRIOR_GAUSSIAN) {
         switch (c->Dp) {
-            case 4: DPMM_TRY(launch_gauss_sub_stats_t<4>(c, draw, r, d_rout)); break;
-            case 8: DPMM_TRY(launch_gauss_sub_stats_t<8>(c, draw, r, d_rout)); break;
-            case 16: DPMM_TRY(launch_gauss_sub_stats_t<16>(c, draw, r, d_rout)); break;
-            case 32: DPMM_TRY(launch_gauss_sub_stats_t<32>(c, draw, r, d_rout)); break;
-            case 64: DPMM_TRY(launch_gauss_sub_stats_t<64>(c, draw, r, d_rout)); break;
-            case 128: DPMM_TRY(launch_gauss_sub_stats_t<128>(c, draw, r, d_rout)); break;
+            case 4: DPMM_TRY(launch_gauss_sub_stats_t<4>(c, draw, r, d_rout, d_mask)); break;
+            case 8: DPMM_TRY(launch_gauss_sub_stats_t<8>(c, draw, r, d_rout, d_mask)); break;
+            case 16: DPMM_TRY(launch_gauss_sub_stats_t<16>(c, draw, r, d_rout, d_mask)); break;
+            case 32: DPMM_TRY(launch_gauss_sub_stats_t<32>(c, draw, r, d_rout, d_mask)); break;
+            case 64: DPMM_TRY(launch_gauss_sub_stats_t<64>(c, draw, r, d_rout, d_mask)); break;
+            case 128: DPMM_TRY(launch_gauss_sub_stats_t<128>(c, draw, r, d_rout, d_mask)); break;
             default: return fail(DPMM_ERR_INVALID_ARG, "unsupported padded dimension");
         }
     } else {
@@ -718,10 +723,10 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
             DPMM_CUDA_TRY(cudaFuncSetAttribute(k_mult_sub_stats, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         k_mult_sub_stats<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->Dp, c->d_perm, c->d_chunk, c->d_nchunks,
                                                                  c->d_mu, c->d_lrw, draw ? 1 : 0, r, c->d_sub, d_rout,
-                                                                 c->d_part, 1 + c->Dp);
+                                                                 c->d_part, 1 + c->Dp, d_mask);
         DPMM_LAUNCHED();
     }
-    return launch_stats_finalize(c, K);
+    return launch_stats_finalize(c, K, d_mask);
 }
 
 // One block per cluster: chunk partials summed in chunk order (FP64), shifted back to the
@@ -730,9 +735,10 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
 __global__ void k_stats_finalize(const double* __restrict__ part, const int32_t* __restrict__ chunk,
                                  const int32_t* __restrict__ nchunks, const float* __restrict__ muv,
                                  const double* __restrict__ gshift, int D, int Dp, int gauss, int SL, int out_len,
-                                 double* __restrict__ stats)
+                                 double* __restrict__ stats, const uint8_t* __restrict__ mask)
 {
     const int k = blockIdx.x;
+    if (mask && !mask[k]) return;
     const int nc = *nchunks;
     // first chunk of this cluster (chunks are ordered by cluster)
     int lo = 0, hi = nc;
@@ -794,7 +800,7 @@ __global__ void k_stats_finalize(const double* __restrict__ part, const int32_t*
     }
 }
 
-dpmm_status launch_stats_finalize(dpmm_ctx* c, int K)
+dpmm_status launch_stats_finalize(dpmm_ctx* c, int K, const uint8_t* d_mask)
 {
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     const int SL = gauss ? 1 + c->Dp + tri(c->Dp) : 1 + c->Dp;
@@ -802,9 +808,13 @@ dpmm_status launch_stats_finalize(dpmm_ctx* c, int K)
     if (sm > 48 * 1024)
         DPMM_CUDA_TRY(cudaFuncSetAttribute(k_stats_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_stats_finalize<<<K, 256, sm, c->stream>>>(c->d_part, c->d_chunk, c->d_nchunks, c->d_mu, c->d_gshift, c->D,
-                                                c->Dp, gauss, SL, c->stat_len, c->d_stats);
+                                                c->Dp, gauss, SL, c->stat_len, c->d_stats, d_mask);
     DPMM_LAUNCHED();
-    c->stats_K = K;
+    if (!d_mask) {
+        c->stats_K = K;
+        std::fill(c->stats_ok.begin(), c->stats_ok.end(), 0);
+        std::fill(c->stats_ok.begin(), c->stats_ok.begin() + K, 1);
+    }
     return DPMM_OK;
 }
 
@@ -849,7 +859,7 @@ dpmm_status launch_relabel(dpmm_ctx* c, int mode, int K, const int32_t* h_table,
     k_relabel<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(mode, c->N, tlen, c->d_remap, r, d_bits, c->d_labels,
                                                              c->d_sub);
     DPMM_LAUNCHED();
-    c->perm_K = -1;
+    if (mode != 2) c->perm_K = -1;   // a reset changes sub-labels only
     return DPMM_OK;
 }
 

@@ -386,3 +386,49 @@ def test_hastings_parity_multinomial():
             lij = O.mult_lml(a0, O.mult_posterior(a0, sm[i, 0] + sm[j, 0], 1))
             ref = O.merge_log_hr(5.0, cnt[i, 0], cnt[j, 0], lml[i, 0], lml[j, 0], lij)
             assert abs(mhr_g[i, j] - ref) <= 1e-8 * max(1, abs(ref))
+
+
+# ------------------------------------------------------------------ tensor-core label phase
+@pytest.mark.parametrize("D,K,N", [(64, 1, 300), (64, 2, 128), (64, 3, 5000), (64, 37, 6001), (64, 100, 3000),
+                                   (64, 150, 1500), (48, 7, 2000), (32, 20, 4000)])
+def test_gaussian_labels_tensor_core_parity(D, K, N):
+    """split-BF16 tcgen05 contraction: r within 2e-4 relative of FP64 (the stated tolerance of the
+    mixed-precision path), labels exact against the oracle's draw on the GPU's own r."""
+    from dpmmsubclusters_gpu_b200 import LL_TC_BF16X3
+    rng = np.random.default_rng(1000 + D * 7 + K)
+    x, z, mus, covs = _gauss_mixture(rng, N, D, K)
+    x += 3.0
+    mu, inv, logdet, w = _params(rng, mus + 3.0, covs)
+    ck = CudaKernel(prior_type.Gaussian, loglik_mode=LL_TC_BF16X3, k_max=160).init(N, x, 7, points_major=True)
+    ck.set_gaussian_params(mu, inv, logdet, w)
+    u = uniforms(2 * N, D + K + 1)
+    r = ck.create_clusters_labels(K, uniforms=u, return_loglik=True).astype(np.float64)
+    r64 = np.stack([O.gauss_loglik(x, mu[k], inv[k], logdet[k], w[k]) for k in range(K)], 1)
+    rf = r - D * D * LOG2PI / 2
+    err = np.abs(rf - r64) / np.maximum(np.abs(r64), 32)
+    assert err.max() <= 2e-4, err.max()
+    lab = ck.get_labels()
+    lab_o, mg = O.sample_labels(r, u.reshape(N, 2).astype(np.float64))
+    _mismatch_ok(lab, lab_o, mg)
+    # argmax (final iterations)
+    rr = ck.create_clusters_labels(K, bFinal=True, return_loglik=True).astype(np.float64)
+    lab_f = ck.get_labels()
+    lab_of, gap = O.sample_labels(rr, np.zeros((N, 2)), final=True)
+    assert np.all((lab_f == lab_of) | (gap < 1e-5))
+
+
+def test_tensor_core_matches_fp32_form():
+    from dpmmsubclusters_gpu_b200 import LL_TC_BF16X3
+    rng = np.random.default_rng(77)
+    N, D, K = 20000, 64, 25
+    x, z, mus, covs = _gauss_mixture(rng, N, D, K)
+    mu, inv, logdet, w = _params(rng, mus, covs)
+    u = uniforms(2 * N, 5)
+    out = []
+    for mode in (LL_FP32, LL_TC_BF16X3):
+        ck = CudaKernel(prior_type.Gaussian, loglik_mode=mode).init(N, x, 7, points_major=True)
+        ck.set_gaussian_params(mu, inv, logdet, w)
+        r = ck.create_clusters_labels(K, uniforms=u, return_loglik=True)
+        out.append((r, ck.get_labels()))
+    assert np.abs(out[0][0] - out[1][0]).max() < 0.05
+    assert np.mean(out[0][1] != out[1][1]) < 1e-3
