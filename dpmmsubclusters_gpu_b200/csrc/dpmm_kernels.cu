@@ -449,7 +449,7 @@ __host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
 // per sub-cluster: count, sum(x - s) and the upper triangle of sum (x - s)(x - s)^T, shift
 // s = the cluster's mean parameter.  FP32 products, FP32 runs of 32 points, FP64 totals.
 template <int DP, int TP>
-__global__ void __launch_bounds__(256) k_gauss_sub_stats(
+__global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const float* __restrict__ Wt, const float* __restrict__ bvec,
     const float* __restrict__ cvec, const float* __restrict__ lrw, const float* __restrict__ muv, int draw,
@@ -522,18 +522,47 @@ __global__ void __launch_bounds__(256) k_gauss_sub_stats(
             if (draw) {
                 float ql = 0.f, qr = 0.f;
                 const float* xp = sx + tid * (DP + 1);
-                for (int j = 0; j < DP; ++j) {
-                    const float* wl = sWl + j * DP;
-                    const float* wr = sWr + j * DP;
-                    float zl = -sbl[j], zr = -sbr[j];
-#pragma unroll 8
-                    for (int i = 0; i < DP; ++i) {
-                        float xv = xp[i];
-                        zl = fmaf(wl[i], xv, zl);
-                        zr = fmaf(wr[i], xv, zr);
+                if constexpr (DP <= 64) {
+                    // x in registers, factor rows broadcast as float4 from shared memory
+                    float xr[DP];
+#pragma unroll
+                    for (int i = 0; i < DP; ++i) xr[i] = xp[i];
+#pragma unroll 2
+                    for (int j = 0; j < DP; ++j) {
+                        const float4* wl4 = reinterpret_cast<const float4*>(sWl + j * DP);
+                        const float4* wr4 = reinterpret_cast<const float4*>(sWr + j * DP);
+                        float zl = -sbl[j], zr = -sbr[j], zl2 = 0.f, zr2 = 0.f;
+#pragma unroll
+                        for (int i4 = 0; i4 < DP / 4; ++i4) {
+                            const float4 a = wl4[i4], b = wr4[i4];
+                            zl = fmaf(a.x, xr[4 * i4 + 0], zl);
+                            zr = fmaf(b.x, xr[4 * i4 + 0], zr);
+                            zl2 = fmaf(a.y, xr[4 * i4 + 1], zl2);
+                            zr2 = fmaf(b.y, xr[4 * i4 + 1], zr2);
+                            zl = fmaf(a.z, xr[4 * i4 + 2], zl);
+                            zr = fmaf(b.z, xr[4 * i4 + 2], zr);
+                            zl2 = fmaf(a.w, xr[4 * i4 + 3], zl2);
+                            zr2 = fmaf(b.w, xr[4 * i4 + 3], zr2);
+                        }
+                        zl += zl2;
+                        zr += zr2;
+                        ql = fmaf(zl, zl, ql);
+                        qr = fmaf(zr, zr, qr);
                     }
-                    ql = fmaf(zl, zl, ql);
-                    qr = fmaf(zr, zr, qr);
+                } else {
+                    for (int j = 0; j < DP; ++j) {
+                        const float* wl = sWl + j * DP;
+                        const float* wr = sWr + j * DP;
+                        float zl = -sbl[j], zr = -sbr[j];
+#pragma unroll 8
+                        for (int i = 0; i < DP; ++i) {
+                            float xv = xp[i];
+                            zl = fmaf(wl[i], xv, zl);
+                            zr = fmaf(wr[i], xv, zr);
+                        }
+                        ql = fmaf(zl, zl, ql);
+                        qr = fmaf(zr, zr, qr);
+                    }
                 }
                 float rl = cl - 0.5f * ql, rr = cr - 0.5f * qr;
                 if (r_out) { r_out[2 * pt] = rl; r_out[2 * pt + 1] = rr; }

@@ -38,7 +38,8 @@ constexpr int A_BYTES = BM * KD * 2;       // 16 KB (one of hi / lo)
 constexpr int B_BYTES = BN * KD * 2;       // 16 KB (one of hi / lo)
 constexpr int STAGE_BYTES = 2 * B_BYTES;   // 32 KB: hi then lo
 constexpr uint32_t TMEM_COLS = 2 * BN;     // 256: double-buffered accumulator
-constexpr int THREADS = 192;
+constexpr int EPI_WARPS = 8;               // two per TMEM lane quarter, one cluster each
+constexpr int THREADS = 32 * (2 + EPI_WARPS);
 
 enum : int { ERR_TIMEOUT_FULL = 1, ERR_TIMEOUT_EMPTY = 2, ERR_TIMEOUT_TFULL = 3, ERR_TIMEOUT_TEMPTY = 4 };
 
@@ -160,16 +161,23 @@ __device__ __forceinline__ void umma_commit(uint64_t* bar)
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32])
+// 64 consecutive accumulator columns of this thread's TMEM lane (warp-collective)
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64])
 {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, "
+        "%32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, "
+        "%48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];"
         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
           "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
           "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]),
+          "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]),
+          "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -265,7 +273,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
         }
         for (int t = 0; t < 2; ++t) {
             mbar_init(&tfull[t], 1);
-            mbar_init(&tempty[t], 4 * 32);
+            mbar_init(&tempty[t], EPI_WARPS * 32);
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -356,8 +364,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
             if (issued > 0) mbar_wait_bounded(&tfull[(issued - 1) & 1], ((issued - 1) >> 1) & 1, nullptr);
         }
     } else {
-        // ---------------- epilogue: TMEM -> r table
-        const int quarter = warp & 3;                  // warps 2,3,4,5 -> lanes 64,96,0,32
+        // ---------------- epilogue: TMEM -> r table.  Epilogue warp e handles TMEM lane quarter
+        // (warp % 4) -- the quarter a warp may access -- and cluster c = e / 4 of each N tile.
+        const int e = warp - 2;
+        const int quarter = warp & 3;
+        const int c = e >> 2;
         const int p = quarter * 32 + lane;             // point row within the tile
         const int64_t pt = pt0 + p;
         const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
@@ -370,32 +381,34 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
                 break;
             }
             tc_fence_after();
+            const int k = nt * CPT + c;
+            if (k < K) {
+                uint32_t v[64];
+                tmem_ld64(tmem_base + lane_addr + (uint32_t)(t * BN + c * KD), v);
+                const float4* bk = reinterpret_cast<const float4*>(bvec + (size_t)3 * k * Dp);
+                float q0 = 0.f, q1 = 0.f;
 #pragma unroll
-            for (int c = 0; c < CPT; ++c) {
-                const int k = nt * CPT + c;
-                if (k >= K) break;
-                const float* bk = bvec + (size_t)3 * k * Dp;
-                float q = 0.f;
-#pragma unroll
-                for (int half = 0; half < KD / 32; ++half) {
-                    uint32_t v[32];
-                    tmem_ld32(tmem_base + lane_addr + (uint32_t)(t * BN + c * KD + half * 32), v);
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        const int jj = half * 32 + j;
-                        const float bj = jj < Dp ? __ldg(bk + jj) : 0.f;
-                        const float z = __uint_as_float(v[j]) - bj;
-                        q = fmaf(z, z, q);
-                    }
+                for (int j4 = 0; j4 < KD / 4; ++j4) {
+                    const float4 b4 = j4 * 4 < Dp ? __ldg(bk + j4) : make_float4(0.f, 0.f, 0.f, 0.f);
+                    const float z0 = __uint_as_float(v[4 * j4 + 0]) - b4.x;
+                    const float z1 = __uint_as_float(v[4 * j4 + 1]) - b4.y;
+                    const float z2 = __uint_as_float(v[4 * j4 + 2]) - b4.z;
+                    const float z3 = __uint_as_float(v[4 * j4 + 3]) - b4.w;
+                    q0 = fmaf(z0, z0, q0);
+                    q1 = fmaf(z1, z1, q1);
+                    q0 = fmaf(z2, z2, q0);
+                    q1 = fmaf(z3, z3, q1);
                 }
-                const float r = __ldg(cvec + 3 * k) - 0.5f * q;
+                const float r = __ldg(cvec + 3 * k) - 0.5f * (q0 + q1);
                 sr[k * BM + p] = r;
                 if (r_out && pt < N) r_out[pt * K + k] = r;
             }
             tc_fence_before();
             mbar_arrive(&tempty[t]);
         }
-        if (!*abort_flag && pt < N) {
+        // the draw reads every cluster's r of its point: both epilogue halves must be done
+        asm volatile("bar.sync 1, %0;" ::"r"(EPI_WARPS * 32) : "memory");
+        if (c == 0 && !*abort_flag && pt < N) {   // one thread per point draws
             // softmax + alias draw (or argmax) per point
             labels[pt] = [&]() {
                 if (final_) {
@@ -411,9 +424,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
                 for (int k = 1; k < K; ++k) mx = fmaxf(mx, sr[k * BM + p]);
                 float sum = 0.f;
                 for (int k = 0; k < K; ++k) {
-                    float e = __expf(sr[k * BM + p] - mx);
-                    sr[k * BM + p] = e;
-                    sum += e;
+                    float ex = __expf(sr[k * BM + p] - mx);
+                    sr[k * BM + p] = ex;
+                    sum += ex;
                 }
                 const float inv = 1.0f / sum, fk = (float)K;
                 for (int k = K - 1; k >= 0; --k) sr[(k + 1) * BM + p] = (sr[k * BM + p] * inv) * fk;
