@@ -110,6 +110,8 @@ SIGNATURES = {
     "dpmm_kernel_launch_count": (c_uint64, []),
     "dpmm_transfer_bytes": (None, [POINTER(c_uint64), POINTER(c_uint64)]),
     "dpmm_phase_times": (c_int, [_CTX, c_int, _PD, _PI64]),
+    "dpmm_merge_hastings_static": (c_int, [c_int32, c_int32, c_int32, c_double, c_double, c_double, c_void_p,
+                                           c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

@@ -230,3 +230,153 @@ dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha)
 }
 
 }  // namespace dpmm
+
+// ============================================================================= allocation-free variant
+// The all-pairs merge ratio for callers that cannot allocate device memory.  Its only scratch --
+// the prior's log-determinant and each cluster's log marginal likelihood, written by the first
+// two kernels and read by the pair kernel -- lives in the file-scope array below, sized for
+// kStaticMaxClusters clusters.  Every device that loads this library holds the array until exit.
+// All calls on a device share it: calls whose work overlaps on the GPU (different streams, or
+// different host threads) race on it and must be serialised by the caller.
+namespace dpmm {
+
+constexpr int kStaticMaxClusters = 1024;
+static __device__ __align__(256) double g_merge_scratch[1 + kStaticMaxClusters];
+
+// scratch[0] = log det psi0 (NIW prior)
+__global__ void __launch_bounds__(kHThreads) k_static_prior_logdet(const double* __restrict__ prior, int D,
+                                                                    double* __restrict__ scratch)
+{
+    extern __shared__ double sh[];
+    double* A = sh;                       // D*D
+    double* red = A + (size_t)D * D;      // 33
+    for (int e = threadIdx.x; e < D * D; e += blockDim.x) A[e] = prior[D + e];
+    __syncthreads();
+    const double ld = chol_logdet(A, D, red);
+    if (threadIdx.x == 0) scratch[0] = ld;
+}
+
+// scratch[1 + k] = log marginal likelihood of cluster k (statistics slot 3k)
+__global__ void __launch_bounds__(kHThreads) k_static_cluster_lml(const double* __restrict__ stats, int stat_len, int D,
+                                                                   int gauss, double k0, double v0,
+                                                                   const double* __restrict__ prior,
+                                                                   double* __restrict__ scratch)
+{
+    extern __shared__ double sh[];
+    double* psi = sh;
+    double* mp = gauss ? psi + (size_t)D * D : sh;
+    double* red = gauss ? mp + D : sh;
+    const double* st = stats + (size_t)(3 * blockIdx.x) * stat_len;
+    double v;
+    if (gauss)
+        v = niw_lml_from_stats(D, st[0], st + 1, st + 1 + D, nullptr, nullptr, k0, v0, prior, prior + D, scratch[0],
+                               psi, mp, red);
+    else
+        v = mult_lml_from_stats(D, st[0], st + 1, nullptr, prior, red);
+    if (threadIdx.x == 0) scratch[1 + blockIdx.x] = v;
+}
+
+// one block per pair i < j, as k_merge_hr, with the per-cluster terms read from the scratch
+__global__ void __launch_bounds__(kHThreads) k_static_merge_hr(const double* __restrict__ stats, int stat_len, int D,
+                                                                int gauss, double k0, double v0,
+                                                                const double* __restrict__ prior,
+                                                                const double* __restrict__ scratch, int K,
+                                                                double alpha, double* __restrict__ hr)
+{
+    extern __shared__ double sh[];
+    double* psi = sh;
+    double* mp = gauss ? psi + (size_t)D * D : sh;
+    double* red = gauss ? mp + D : sh;
+    long long b = blockIdx.x;
+    int i = 0;
+    long long rowlen = K - 1;
+    while (b >= rowlen) { b -= rowlen; ++i; --rowlen; }
+    const int j = i + 1 + (int)b;
+    const double* si = stats + (size_t)(3 * i) * stat_len;
+    const double* sj = stats + (size_t)(3 * j) * stat_len;
+    const double ni = si[0], nj = sj[0];
+    if (ni == 0 || nj == 0) return;       // stays NaN
+    double lij;
+    if (gauss)
+        lij = niw_lml_from_stats(D, ni + nj, si + 1, si + 1 + D, sj + 1, sj + 1 + D, k0, v0, prior, prior + D,
+                                 scratch[0], psi, mp, red);
+    else
+        lij = mult_lml_from_stats(D, ni + nj, si + 1, sj + 1, prior, red);
+    if (threadIdx.x != 0) return;
+    const double n = ni + nj;
+    hr[(size_t)i * K + j] = -log(alpha) + lgamma(alpha) - 2 * lgamma(0.5 * alpha) + lgamma(n) - lgamma(n + alpha) +
+                            lgamma(ni + 0.5 * alpha) - lgamma(ni) - lgamma(nj) + lgamma(nj + 0.5 * alpha) + lij -
+                            scratch[1 + i] - scratch[1 + j];
+}
+
+}  // namespace dpmm
+
+#include <mutex>
+
+// Device address of g_merge_scratch, looked up once per device (with that device current) on the
+// first call made on it.
+static double* static_scratch_for_current_device(dpmm_status* st)
+{
+    static std::mutex mu;
+    static double* ptr[128] = {nullptr};
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= 128) {
+        *st = e != cudaSuccess ? dpmm::cuda_status(e, "cudaGetDevice") : dpmm::fail(DPMM_ERR_NO_DEVICE, "device ordinal");
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptr[dev]) {
+        double* p = nullptr;
+        e = cudaGetSymbolAddress((void**)&p, dpmm::g_merge_scratch);
+        if (e != cudaSuccess || !p) {
+            *st = dpmm::cuda_status(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(g_merge_scratch)");
+            return nullptr;
+        }
+        ptr[dev] = p;
+    }
+    *st = DPMM_OK;
+    return ptr[dev];
+}
+
+extern "C" dpmm_status dpmm_merge_hastings_static(int32_t prior_type, int32_t D, int32_t K, double alpha, double k0,
+                                                  double v0, const double* prior, const double* stats,
+                                                  double* merge_log_hr, void* stream)
+{
+    using namespace dpmm;
+    const bool gauss = prior_type == DPMM_PRIOR_GAUSSIAN;
+    if (prior_type != DPMM_PRIOR_GAUSSIAN && prior_type != DPMM_PRIOR_MULTINOMIAL)
+        return fail(DPMM_ERR_INVALID_ARG, "unknown prior_type");
+    if (!prior || !stats || !merge_log_hr) return fail(DPMM_ERR_INVALID_ARG, "null device pointer");
+    if (K < 1 || K > kStaticMaxClusters)
+        return fail(DPMM_ERR_INVALID_ARG, "dpmm_merge_hastings_static: K must be in [1, " +
+                                              std::to_string(kStaticMaxClusters) + "], got " + std::to_string(K));
+    if (D < 1 || (gauss && D > kMaxGaussDim) || (!gauss && D > kMaxMultDim))
+        return fail(DPMM_ERR_INVALID_ARG, "dpmm_merge_hastings_static: dimension out of range");
+    if (!(alpha > 0)) return fail(DPMM_ERR_INVALID_ARG, "alpha must be positive");
+    dpmm_status st;
+    double* scratch = static_scratch_for_current_device(&st);
+    if (!scratch) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const int stat_len = gauss ? 1 + D + D * D : 1 + D;
+    const size_t sm = sizeof(double) * (gauss ? (size_t)D * D + D + 33 : 33);
+    if (sm > 48 * 1024) {
+        DPMM_CUDA_TRY(cudaFuncSetAttribute(k_static_prior_logdet, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        DPMM_CUDA_TRY(cudaFuncSetAttribute(k_static_cluster_lml, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        DPMM_CUDA_TRY(cudaFuncSetAttribute(k_static_merge_hr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    }
+    DPMM_CUDA_TRY(cudaMemsetAsync(merge_log_hr, 0xff, sizeof(double) * (size_t)K * K, s));   // NaN
+    if (gauss) {
+        k_static_prior_logdet<<<1, kHThreads, sm, s>>>(prior, D, scratch);
+        DPMM_LAUNCHED();
+    }
+    k_static_cluster_lml<<<K, kHThreads, sm, s>>>(stats, stat_len, D, gauss ? 1 : 0, k0, v0, prior, scratch);
+    DPMM_LAUNCHED();
+    const long long pairs = (long long)K * (K - 1) / 2;
+    if (pairs > 0) {
+        k_static_merge_hr<<<(unsigned)pairs, kHThreads, sm, s>>>(stats, stat_len, D, gauss ? 1 : 0, k0, v0, prior,
+                                                                 scratch, K, alpha, merge_log_hr);
+        DPMM_LAUNCHED();
+    }
+    return DPMM_OK;
+}

@@ -226,6 +226,24 @@ dpmm_status dpmm_split_hastings(dpmm_ctx* ctx, int K, double alpha, double* lml,
  * are NaN).  Uses the cluster-level statistics on the device. */
 dpmm_status dpmm_merge_hastings(dpmm_ctx* ctx, int K, double alpha, double* merge_log_hr);
 
+/* Allocation-free form of dpmm_merge_hastings, with no counterpart in the reference.  For callers
+ * that cannot call cudaMalloc: host programs whose device memory is owned by another framework's
+ * pool or fixed budget, and latency-critical loops that cannot afford cudaMalloc's implicit device
+ * synchronisation.  It needs no dpmm_ctx: the caller passes device pointers to the inputs
+ *   prior  NIW: m[D] then psi[D*D] (col-major); multinomial: alpha[D]   (k0, v0: NIW kappa, nu)
+ *   stats  3K slots of (count, sum[D], S[D*D]) (NIW) or (count, sum[D]) (multinomial), FP64, in the
+ *          layout dpmm_create_sufficient_statistics returns; slot 3k is cluster k
+ * and the output merge_log_hr[K*K] (row-major; entries i >= j or with an empty cluster are NaN), and
+ * the work is queued on `stream` (a cudaStream_t; NULL = the default stream) without waiting for it.
+ * The kernels' scratch is a file-scope device array for at most 1024 clusters (K > 1024 is rejected
+ * with DPMM_ERR_INVALID_ARG); every device that loads the library holds it (8 KB) until exit.  The
+ * first call on a device looks up the array's device address, so make that first call before any
+ * stream capture.  All calls on a device share the array: calls that overlap on the GPU race.
+ * It calls no cudaMalloc, cudaFree or other allocating routine. */
+dpmm_status dpmm_merge_hastings_static(int32_t prior_type, int32_t D, int32_t K, double alpha, double k0, double v0,
+                                       const double* prior, const double* stats, double* merge_log_hr,
+                                       void* stream);
+
 /* Synchronise the context's stream; returns any pending device error. */
 dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
