@@ -171,4 +171,85 @@ __device__ __forceinline__ int alias_draw2(float p1, float p2, float u1, float u
     return alias_draw<float, uint8_t>(2, acc, u1, u2);
 }
 
+// ---------------------------------------------------------------------------------------------
+// Streamed form of the same alias draw (one thread, no index tables).  y[(k - 1) * stride] =
+// p_k * K for the 1-based categories k = 1..K; returns the label drawn with (u1, u2).
+//
+// Only the drawn column's final (y, alias) matter, and the reference's two loops
+// (cudaKernel.cu:56-111) determine them as a merge of two streams:
+//  * the partition leaves the smalls (y < 1) at positions 1..ns: a small at q <= ns stays, and
+//    the larges of [1, ns] trade places with the smalls of (ns, K], the i-th large from the
+//    left with the i-th small from the right;
+//  * the pairing consumes smalls from position ns downwards (a displaced large's slot yields
+//    the next small of (ns, K] walking upwards) and larges from position ns + 1 upwards (a
+//    displaced small's slot yields the next large of [1, ns] walking downwards);
+//  * with D the deficit (1 - y) consumed so far and C the excess (y - 1) of the larges taken so
+//    far, a small is aliased to the current large, which is replaced by the next one with
+//    positive excess while C <= D; a large whose C is reached by D ends at y = 1 + C - D and,
+//    when D > C, is aliased to the next large with positive excess.
+// The merge stops as soon as the drawn column is settled.  D and C are FP64 running sums in the
+// reference's consumption order.
+template <typename T>
+__device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int stride, int K, float u1, float u2)
+{
+    auto y = [&](int i) -> T { return ys[(size_t)i * stride]; };
+    int ns = 0;
+    for (int k = 0; k < K; ++k) ns += y(k) < (T)1 ? 1 : 0;
+    const int col = alias_column(K, u1);
+    const T yc = y(col - 1);
+    if (yc == (T)1) return col;          // a large without excess is never consumed
+
+    int P = ns + 1;     // small-stream position (descending)
+    int sr = ns;        // last small of (ns, K] taken (ascending)
+    int Q = ns;         // large-stream position (ascending)
+    int ll = ns + 1;    // last large of [1, ns] taken (descending)
+    double D = 0.0, C = 0.0, Ccol = 0.0;
+    bool col_taken = false;
+
+    // next large with positive excess in consumption order (0 if none); adds its excess to C
+    auto next_large = [&]() -> int {
+        while (++Q <= K) {
+            int e = Q;
+            if (y(Q - 1) < (T)1) {
+                do { --ll; } while (ll > 1 && y(ll - 1) < (T)1);
+                e = ll;
+            }
+            const double ex = (double)y(e - 1) - 1.0;
+            if (ex > 0.0) {
+                C += ex;
+                return e;
+            }
+        }
+        return 0;
+    };
+    // the large that col passes its deficit to, once D has reached col's C
+    auto settle_col = [&]() -> int {
+        if (!(1.0 + Ccol - D < (double)u2)) return col;
+        const int a = next_large();
+        return a != 0 ? a : col;
+    };
+
+    int cur = 0;
+    for (;;) {
+        if (--P < 1) return col;          // every small paired: col keeps itself
+        int s = P;
+        if (y(P - 1) >= (T)1) {
+            do { ++sr; } while (sr < K && y(sr - 1) >= (T)1);
+            s = sr;
+        }
+        while (C <= D) {                  // the current large is used up: take the next
+            cur = next_large();
+            if (cur == 0) return col;     // no large left: this and later smalls keep themselves
+            if (cur == col) {
+                col_taken = true;
+                Ccol = C;
+                if (Ccol <= D) return settle_col();   // used up at once by the carried deficit
+            }
+        }
+        if (s == col) return yc < (T)u2 ? cur : col;
+        D += 1.0 - (double)y(s - 1);
+        if (col_taken && D >= Ccol) return settle_col();
+    }
+}
+
 }  // namespace dpmm

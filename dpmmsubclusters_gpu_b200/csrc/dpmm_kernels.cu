@@ -82,8 +82,7 @@ dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u)
 // ----------------------------------------------------------------------------- label phase
 // Shared epilogue: r values of one point (stride P in shared memory) -> label.
 template <int P>
-__device__ __forceinline__ int draw_from_r(float* sr, uint16_t* sa, uint16_t* sb, int p, int K, int final_,
-                                           const RngArgs& rng, int64_t pt)
+__device__ __forceinline__ int draw_from_r(float* sr, int p, int K, int final_, const RngArgs& rng, int64_t pt)
 {
     if (final_) {
         // update_labels_by_max_index_kernel (cudaKernel.cu:405-424): first maximum wins
@@ -106,12 +105,10 @@ __device__ __forceinline__ int draw_from_r(float* sr, uint16_t* sa, uint16_t* sb
     }
     const float inv = 1.0f / sum;
     const float fk = (float)K;
-    // y[k+1] = p_k * K, written from the top so y[k+1] never overwrites an unread e[k+1]
-    for (int k = K - 1; k >= 0; --k) sr[(k + 1) * P + p] = (sr[k * P + p] * inv) * fk;
+    for (int k = 0; k < K; ++k) sr[k * P + p] = (sr[k * P + p] * inv) * fk;   // y_k = p_k * K
     float u1, u2;
     draw_uniform2(rng, pt, u1, u2);
-    AliasAcc<float, uint16_t> acc{sr + p, sa + p, sb + p, P};
-    return alias_draw<float, uint16_t>(K, acc, u1, u2);
+    return alias_draw_stream(sr + p, P, K, u1, u2);
 }
 
 // Gaussian label phase, FP32 SIMT: one thread per point, x in registers, each cluster's
@@ -127,9 +124,7 @@ __global__ void __launch_bounds__(P) k_gauss_labels_simt(
     float* sW = reinterpret_cast<float*>(smem);          // DP*DP
     float* sbv = sW + DP * DP;                            // DP
     float* sx = sbv + DP;                                 // P*(DP+1)
-    float* sr = sx + P * (DP + 1);                        // (K+2)*P
-    uint16_t* sa = reinterpret_cast<uint16_t*>(sr + (size_t)(K + 2) * P);
-    uint16_t* sb = sa + (size_t)(K + 2) * P;
+    float* sr = sx + P * (DP + 1);                        // K*P
 
     const int p = threadIdx.x;
     const int64_t pt0 = (int64_t)blockIdx.x * P;
@@ -183,7 +178,7 @@ __global__ void __launch_bounds__(P) k_gauss_labels_simt(
         if (r_out && valid) r_out[pt * K + k] = r;
     }
     if (!valid) return;
-    labels[pt] = draw_from_r<P>(sr, sa, sb, p, K, final_, rng, pt);
+    labels[pt] = draw_from_r<P>(sr, p, K, final_, rng, pt);
 }
 
 // Multinomial label phase, FP32 SIMT: tiled dot products r[p][k] = sum_d x[p][d] * logtheta[k][d]
@@ -197,9 +192,7 @@ __global__ void __launch_bounds__(256) k_mult_labels_simt(
     extern __shared__ __align__(16) unsigned char smem[];
     float* sX = reinterpret_cast<float*>(smem);          // P x (DC+1)
     float* sT = sX + P * (DC + 1);                        // KG x (DC+1)
-    float* sr = sT + KG * (DC + 1);                       // (K+2)*P
-    uint16_t* sa = reinterpret_cast<uint16_t*>(sr + (size_t)(K + 2) * P);
-    uint16_t* sb = sa + (size_t)(K + 2) * P;
+    float* sr = sT + KG * (DC + 1);                       // K*P
 
     const int tid = threadIdx.x;
     const int64_t pt0 = (int64_t)blockIdx.x * P;
@@ -250,26 +243,24 @@ __global__ void __launch_bounds__(256) k_mult_labels_simt(
     __syncthreads();
     if (tid >= P || tid >= rows) return;
     const int64_t pt = pt0 + tid;
-    labels[pt] = draw_from_r<P>(sr, sa, sb, tid, K, final_, rng, pt);
+    labels[pt] = draw_from_r<P>(sr, tid, K, final_, rng, pt);
+}
+
+static size_t gauss_label_smem(int DP, int P, int K)
+{
+    return sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)K * P);
 }
 
 template <int DP, int P>
 static dpmm_status launch_gauss_labels_t(dpmm_ctx* c, int K, int final_, RngArgs r, float* d_rout)
 {
-    size_t sm = sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)(K + 2) * P) +
-                sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
+    const size_t sm = gauss_label_smem(DP, P, K);
     auto kern = k_gauss_labels_simt<DP, P>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<blocks_for(c->N, P), P, sm, c->stream>>>(c->d_x, c->N, c->d_Wt, c->d_b, c->d_c, K, final_, r,
                                                      c->d_labels, d_rout);
     DPMM_LAUNCHED();
     return DPMM_OK;
-}
-
-static size_t gauss_label_smem(int DP, int P, int K)
-{
-    return sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)(K + 2) * P) +
-           sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
 }
 
 template <int DP>
@@ -297,7 +288,7 @@ dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d
         }
     }
     constexpr int P = 64;
-    size_t sm = sizeof(float) * (P * 33 + 64 * 33 + (size_t)(K + 2) * P) + sizeof(uint16_t) * 2 * (size_t)(K + 2) * P;
+    size_t sm = sizeof(float) * (P * 33 + 64 * 33 + (size_t)K * P);
     if (sm > 220 * 1024) return fail(DPMM_ERR_INVALID_ARG, "too many clusters for the multinomial label kernel");
     DPMM_CUDA_TRY(cudaFuncSetAttribute(k_mult_labels_simt<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k_mult_labels_simt<P><<<blocks_for(c->N, P), 256, sm, c->stream>>>(c->d_x, c->N, c->Dp, c->d_mu, K, final_, r,
@@ -448,7 +439,48 @@ __host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
 // sub-labels (unless draw == 0, in which case the current sub-labels are used) and accumulates
 // per sub-cluster: count, sum(x - s) and the upper triangle of sum (x - s)(x - s)^T, shift
 // s = the cluster's mean parameter.  FP32 products, FP32 runs of 32 points, FP64 totals.
-template <int DP, int TP>
+//
+// DP <= 64 ("blocked" form, 128 points per tile):
+//   draw  - two threads per point, one per side: warps 0-3 evaluate the l factor, warps 4-7 the r
+//           factor, x in registers, factor rows broadcast from shared memory as float4;
+//   stats - each thread of a warp-aligned group owns one 4 x 4 block of the upper triangle and
+//           does 16 FMAs per point from two float4 loads; G groups take every G-th point of the
+//           tile; FP64 totals per thread live in shared memory and are summed over the groups at
+//           the end.
+// DP = 128: one thread per point for the draw, one matrix entry per thread through a pair table.
+__host__ __device__ constexpr int tri_index(int dp, int i, int j)   // row-major upper triangle, i <= j
+{
+    return i * dp - i * (i - 1) / 2 + (j - i);
+}
+
+template <int DP>
+struct SubStatsShape {
+    static constexpr bool BLOCKED = DP <= 64;
+    static constexpr int TP = 128;                                   // points per tile
+    static constexpr int SX = DP + 4;                                // shared row stride (16-byte rows)
+    static constexpr int NB = DP / 4;
+    static constexpr int NBLK = NB * (NB + 1) / 2;                   // 4 x 4 blocks of the triangle
+    static constexpr int GS = (NBLK + 31) / 32 * 32;                 // threads per group (whole warps)
+    static constexpr int G = BLOCKED ? 256 / GS : 1;                 // groups
+    static constexpr int NTOT = G * NBLK;                            // owners of FP64 totals
+    // shared layout in bytes
+    static constexpr size_t off_wl = 0;
+    static constexpr size_t off_wr = off_wl + sizeof(float) * DP * DP;
+    static constexpr size_t off_bl = off_wr + sizeof(float) * DP * DP;
+    static constexpr size_t off_br = off_bl + sizeof(float) * DP;
+    static constexpr size_t off_s = off_br + sizeof(float) * DP;
+    static constexpr size_t off_x = (off_s + sizeof(float) * DP + 15) / 16 * 16;
+    static constexpr size_t off_q = off_x + sizeof(float) * TP * SX;
+    static constexpr size_t off_sub = off_q + sizeof(float) * 2 * TP;
+    static constexpr size_t off_tail = (off_sub + sizeof(int32_t) * TP + 15) / 16 * 16;
+    // blocked: FP64 block totals [32][NTOT] then sums [G][2][DP]; DP = 128: pair table
+    static constexpr size_t off_tot = off_tail;
+    static constexpr size_t off_sum = off_tot + (BLOCKED ? sizeof(double) * 32 * NTOT : 0);
+    static constexpr size_t bytes = BLOCKED ? off_sum + sizeof(double) * G * 2 * DP
+                                            : off_tail + sizeof(uint16_t) * tri(DP);
+};
+
+template <int DP>
 __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const float* __restrict__ Wt, const float* __restrict__ bvec,
@@ -456,18 +488,23 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
     RngArgs rng, int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part,
     const uint8_t* __restrict__ mask)
 {
+    using S = SubStatsShape<DP>;
     constexpr int T = tri(DP);
-    constexpr int E = (T + 255) / 256;       // scatter entries per thread
     constexpr int SL = 1 + DP + T;            // partial record length per sub-cluster
+    constexpr int TP = S::TP, SX = S::SX;
+    constexpr int E = S::BLOCKED ? 1 : (T + 255) / 256;
     extern __shared__ __align__(16) unsigned char smem[];
-    float* sWl = reinterpret_cast<float*>(smem);   // DP*DP
-    float* sWr = sWl + DP * DP;                    // DP*DP
-    float* sbl = sWr + DP * DP;                    // DP
-    float* sbr = sbl + DP;                         // DP
-    float* ss = sbr + DP;                          // DP (shift)
-    float* sx = ss + DP;                           // TP*(DP+1)
-    int32_t* ssub = reinterpret_cast<int32_t*>(sx + TP * (DP + 1));   // TP
-    uint16_t* spair = reinterpret_cast<uint16_t*>(ssub + TP);         // T (i<<8 | j)
+    float* sWl = reinterpret_cast<float*>(smem + S::off_wl);
+    float* sWr = reinterpret_cast<float*>(smem + S::off_wr);
+    float* sbl = reinterpret_cast<float*>(smem + S::off_bl);
+    float* sbr = reinterpret_cast<float*>(smem + S::off_br);
+    float* ss = reinterpret_cast<float*>(smem + S::off_s);
+    float* sx = reinterpret_cast<float*>(smem + S::off_x);
+    float* sq = reinterpret_cast<float*>(smem + S::off_q);
+    int32_t* ssub = reinterpret_cast<int32_t*>(smem + S::off_sub);
+    double* stot = reinterpret_cast<double*>(smem + S::off_tot);
+    double* ssum = reinterpret_cast<double*>(smem + S::off_sum);
+    uint16_t* spair = reinterpret_cast<uint16_t*>(smem + S::off_tail);
 
     const int ch = blockIdx.x;
     if (ch >= *nchunks) return;
@@ -488,83 +525,153 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
         }
     }
     for (int e = tid; e < DP; e += 256) ss[e] = muv[(size_t)(3 * k) * DP + e];
-    for (int e = tid; e < T; e += 256) {
-        // row-major upper triangle: (i, j), i <= j
-        int i = 0, rem = e;
-        while (rem >= DP - i) { rem -= DP - i; ++i; }
-        spair[e] = (uint16_t)((i << 8) | (i + rem));
+    if constexpr (!S::BLOCKED) {
+        for (int e = tid; e < T; e += 256) {
+            int i = 0, rem = e;
+            while (rem >= DP - i) { rem -= DP - i; ++i; }
+            spair[e] = (uint16_t)((i << 8) | (i + rem));
+        }
     }
     const float cl = draw ? cvec[3 * k + 1] : 0.f, cr = draw ? cvec[3 * k + 2] : 0.f;
     const float wl = draw ? lrw[2 * k] : 0.f, wr = draw ? lrw[2 * k + 1] : 0.f;
 
+    // blocked form: this thread's group, 4 x 4 block (bi <= bj) and FP64 total column
+    const int grp = tid / S::GS, tb = tid % S::GS;
+    const bool has_blk = S::BLOCKED && grp < S::G && tb < S::NBLK;
+    int bi = 0, bj = 0;
+    if (has_blk) {
+        int rem = tb;
+        while (rem >= S::NB - bi) { rem -= S::NB - bi; ++bi; }
+        bj = bi + rem;
+    }
+    const bool diag = has_blk && bi == bj;
+    const int tcol = grp * S::NBLK + tb;
+    if constexpr (S::BLOCKED) {
+        if (has_blk)
+            for (int m = 0; m < 32; ++m) stot[m * S::NTOT + tcol] = 0.0;
+        for (int e = tid; e < S::G * 2 * DP; e += 256) ssum[e] = 0.0;
+    }
+    float bf[2][16];
+    float sf[2][4];
     float accf[2][E];
     double accd[2][E];
 #pragma unroll
-    for (int s = 0; s < 2; ++s)
+    for (int s2 = 0; s2 < 2; ++s2) {
 #pragma unroll
-        for (int m = 0; m < E; ++m) { accf[s][m] = 0.f; accd[s][m] = 0.0; }
-    // sums: threads [0, DP) -> l, [DP, 2DP) -> r
-    float sumf = 0.f;
+        for (int m = 0; m < 16; ++m) bf[s2][m] = 0.f;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) sf[s2][m] = 0.f;
+#pragma unroll
+        for (int m = 0; m < E; ++m) { accf[s2][m] = 0.f; accd[s2][m] = 0.0; }
+    }
+    float sumf = 0.f;     // DP = 128: threads [0, DP) -> l sums, [DP, 2DP) -> r sums
     double sumd = 0.0;
     int cnt_l = 0, cnt_r = 0;
+
+    auto flush = [&]() {
+        if constexpr (S::BLOCKED) {
+            if (has_blk) {
+#pragma unroll
+                for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+                    for (int m = 0; m < 16; ++m) {
+                        stot[(16 * s2 + m) * S::NTOT + tcol] += (double)bf[s2][m];
+                        bf[s2][m] = 0.f;
+                    }
+                if (diag) {
+#pragma unroll
+                    for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) {
+                            ssum[(grp * 2 + s2) * DP + 4 * bi + a] += (double)sf[s2][a];
+                            sf[s2][a] = 0.f;
+                        }
+                }
+            }
+        } else {
+#pragma unroll
+            for (int s2 = 0; s2 < 2; ++s2)
+#pragma unroll
+                for (int m = 0; m < E; ++m) { accd[s2][m] += (double)accf[s2][m]; accf[s2][m] = 0.f; }
+            sumd += (double)sumf;
+            sumf = 0.f;
+        }
+    };
 
     for (int t0 = 0; t0 < len; t0 += TP) {
         const int nt = min(TP, len - t0);
         __syncthreads();
-        for (int e = tid; e < TP * DP; e += 256) {
-            int pp = e / DP, i = e % DP;
-            sx[pp * (DP + 1) + i] = pp < nt ? x[(size_t)perm[start + t0 + pp] * DP + i] : 0.f;
+        for (int e = tid; e < TP * DP / 4; e += 256) {
+            const int pp = e / (DP / 4), i4 = e % (DP / 4);
+            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (pp < nt) v = reinterpret_cast<const float4*>(x + (size_t)perm[start + t0 + pp] * DP)[i4];
+            *reinterpret_cast<float4*>(sx + pp * SX + 4 * i4) = v;
         }
         __syncthreads();
-        if (tid < nt) {
-            const int64_t pt = perm[start + t0 + tid];
-            int sv;
-            if (draw) {
-                float ql = 0.f, qr = 0.f;
-                const float* xp = sx + tid * (DP + 1);
-                if constexpr (DP <= 64) {
-                    // x in registers, factor rows broadcast as float4 from shared memory
-                    float xr[DP];
+        if (draw) {
+            if constexpr (S::BLOCKED) {
+                // quadratic form of one side for one point
+                const int side = tid >> 7, pp = tid & 127;
+                const float* W = side ? sWr : sWl;
+                const float* bb = side ? sbr : sbl;
+                float xr[DP];
 #pragma unroll
-                    for (int i = 0; i < DP; ++i) xr[i] = xp[i];
+                for (int i4 = 0; i4 < DP / 4; ++i4) {
+                    const float4 v = *reinterpret_cast<const float4*>(sx + pp * SX + 4 * i4);
+                    xr[4 * i4] = v.x; xr[4 * i4 + 1] = v.y; xr[4 * i4 + 2] = v.z; xr[4 * i4 + 3] = v.w;
+                }
+                float q0 = 0.f, q1 = 0.f;
 #pragma unroll 2
-                    for (int j = 0; j < DP; ++j) {
-                        const float4* wl4 = reinterpret_cast<const float4*>(sWl + j * DP);
-                        const float4* wr4 = reinterpret_cast<const float4*>(sWr + j * DP);
-                        float zl = -sbl[j], zr = -sbr[j], zl2 = 0.f, zr2 = 0.f;
+                for (int j = 0; j < DP; j += 2) {
+                    const float4* w0 = reinterpret_cast<const float4*>(W + j * DP);
+                    const float4* w1 = reinterpret_cast<const float4*>(W + (j + 1) * DP);
+                    float z0 = -bb[j], z1 = -bb[j + 1], z0b = 0.f, z1b = 0.f;
 #pragma unroll
-                        for (int i4 = 0; i4 < DP / 4; ++i4) {
-                            const float4 a = wl4[i4], b = wr4[i4];
-                            zl = fmaf(a.x, xr[4 * i4 + 0], zl);
-                            zr = fmaf(b.x, xr[4 * i4 + 0], zr);
-                            zl2 = fmaf(a.y, xr[4 * i4 + 1], zl2);
-                            zr2 = fmaf(b.y, xr[4 * i4 + 1], zr2);
-                            zl = fmaf(a.z, xr[4 * i4 + 2], zl);
-                            zr = fmaf(b.z, xr[4 * i4 + 2], zr);
-                            zl2 = fmaf(a.w, xr[4 * i4 + 3], zl2);
-                            zr2 = fmaf(b.w, xr[4 * i4 + 3], zr2);
-                        }
-                        zl += zl2;
-                        zr += zr2;
-                        ql = fmaf(zl, zl, ql);
-                        qr = fmaf(zr, zr, qr);
+                    for (int i4 = 0; i4 < DP / 4; ++i4) {
+                        const float4 a = w0[i4], c = w1[i4];
+                        z0 = fmaf(a.x, xr[4 * i4 + 0], z0);
+                        z1 = fmaf(c.x, xr[4 * i4 + 0], z1);
+                        z0b = fmaf(a.y, xr[4 * i4 + 1], z0b);
+                        z1b = fmaf(c.y, xr[4 * i4 + 1], z1b);
+                        z0 = fmaf(a.z, xr[4 * i4 + 2], z0);
+                        z1 = fmaf(c.z, xr[4 * i4 + 2], z1);
+                        z0b = fmaf(a.w, xr[4 * i4 + 3], z0b);
+                        z1b = fmaf(c.w, xr[4 * i4 + 3], z1b);
                     }
-                } else {
+                    z0 += z0b;
+                    z1 += z1b;
+                    q0 = fmaf(z0, z0, q0);
+                    q1 = fmaf(z1, z1, q1);
+                }
+                sq[side * TP + pp] = q0 + q1;
+                __syncthreads();
+            } else {
+                if (tid < nt) {
+                    const float* xp = sx + tid * SX;
+                    float ql = 0.f, qr = 0.f;
                     for (int j = 0; j < DP; ++j) {
-                        const float* wl = sWl + j * DP;
-                        const float* wr = sWr + j * DP;
+                        const float* wlp = sWl + j * DP;
+                        const float* wrp = sWr + j * DP;
                         float zl = -sbl[j], zr = -sbr[j];
 #pragma unroll 8
                         for (int i = 0; i < DP; ++i) {
                             float xv = xp[i];
-                            zl = fmaf(wl[i], xv, zl);
-                            zr = fmaf(wr[i], xv, zr);
+                            zl = fmaf(wlp[i], xv, zl);
+                            zr = fmaf(wrp[i], xv, zr);
                         }
                         ql = fmaf(zl, zl, ql);
                         qr = fmaf(zr, zr, qr);
                     }
+                    sq[tid] = ql;
+                    sq[TP + tid] = qr;
                 }
-                float rl = cl - 0.5f * ql, rr = cr - 0.5f * qr;
+            }
+        }
+        int sv = 0;
+        if (tid < nt) {
+            const int64_t pt = perm[start + t0 + tid];
+            if (draw) {
+                float rl = cl - 0.5f * sq[tid], rr = cr - 0.5f * sq[TP + tid];
                 if (r_out) { r_out[2 * pt] = rl; r_out[2 * pt + 1] = rr; }
                 // + log lr_weights, then the 2-way softmax (cudaKernel.cu:352-372)
                 rl += wl;
@@ -581,66 +688,106 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
             }
             ssub[tid] = sv;
         }
-        __syncthreads();
+        cnt_l += __syncthreads_count(sv == 1);
+        cnt_r += __syncthreads_count(sv == 2);
         for (int e = tid; e < nt * DP; e += 256) {
             int pp = e / DP, i = e % DP;
-            sx[pp * (DP + 1) + i] -= ss[i];
+            sx[pp * SX + i] -= ss[i];
         }
         __syncthreads();
-        for (int pp = 0; pp < nt; ++pp) {
-            const int sv = ssub[pp];
-            if (sv != 1 && sv != 2) continue;
-            const float* xp = sx + pp * (DP + 1);
-            if (sv == 1) {
-                ++cnt_l;
+        if constexpr (S::BLOCKED) {
+            if (grp < S::G) {
+                int run = 0;
+                for (int pp = grp; pp < nt; pp += S::G) {
+                    const int sv2 = ssub[pp];
+                    if (sv2 != 1 && sv2 != 2) continue;
+                    if (has_blk) {
+                        const float* xp = sx + pp * SX;
+                        const float4 xi = *reinterpret_cast<const float4*>(xp + 4 * bi);
+                        const float4 xj = *reinterpret_cast<const float4*>(xp + 4 * bj);
+                        const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+                        const float vj[4] = {xj.x, xj.y, xj.z, xj.w};
+                        if (sv2 == 1) {
 #pragma unroll
-                for (int m = 0; m < E; ++m) {
-                    int e = tid + 256 * m;
-                    if (e < T) {
-                        uint16_t pr = spair[e];
-                        int i = pr >> 8, j = pr & 0xff;
-                        accf[0][m] = fmaf(xp[i], xp[j], accf[0][m]);
-                    }
-                }
-                if (tid < DP) sumf += xp[tid];
-            } else {
-                ++cnt_r;
+                            for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int m = 0; m < E; ++m) {
-                    int e = tid + 256 * m;
-                    if (e < T) {
-                        uint16_t pr = spair[e];
-                        int i = pr >> 8, j = pr & 0xff;
-                        accf[1][m] = fmaf(xp[i], xp[j], accf[1][m]);
+                                for (int c = 0; c < 4; ++c) bf[0][4 * a + c] = fmaf(vi[a], vj[c], bf[0][4 * a + c]);
+                            if (diag) {
+#pragma unroll
+                                for (int a = 0; a < 4; ++a) sf[0][a] += vi[a];
+                            }
+                        } else {
+#pragma unroll
+                            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                                for (int c = 0; c < 4; ++c) bf[1][4 * a + c] = fmaf(vi[a], vj[c], bf[1][4 * a + c]);
+                            if (diag) {
+#pragma unroll
+                                for (int a = 0; a < 4; ++a) sf[1][a] += vi[a];
+                            }
+                        }
                     }
+                    if (++run == 32) { flush(); run = 0; }
                 }
-                if (tid >= DP && tid < 2 * DP) sumf += xp[tid - DP];
             }
-            if ((pp & 31) == 31) {
+        } else {
+            for (int pp = 0; pp < nt; ++pp) {
+                const int sv2 = ssub[pp];
+                if (sv2 != 1 && sv2 != 2) continue;
+                const float* xp = sx + pp * SX;
+                const int slot = sv2 - 1;
 #pragma unroll
-                for (int s = 0; s < 2; ++s)
-#pragma unroll
-                    for (int m = 0; m < E; ++m) { accd[s][m] += (double)accf[s][m]; accf[s][m] = 0.f; }
-                sumd += (double)sumf;
-                sumf = 0.f;
+                for (int m = 0; m < E; ++m) {
+                    int e = tid + 256 * m;
+                    if (e < T) {
+                        uint16_t pr = spair[e];
+                        int i = pr >> 8, j = pr & 0xff;
+                        if (slot == 0) accf[0][m] = fmaf(xp[i], xp[j], accf[0][m]);
+                        else accf[1][m] = fmaf(xp[i], xp[j], accf[1][m]);
+                    }
+                }
+                if (slot == 0 && tid < DP) sumf += xp[tid];
+                if (slot == 1 && tid >= DP && tid < 2 * DP) sumf += xp[tid - DP];
+                if ((pp & 31) == 31) flush();
             }
         }
-#pragma unroll
-        for (int s = 0; s < 2; ++s)
-#pragma unroll
-            for (int m = 0; m < E; ++m) { accd[s][m] += (double)accf[s][m]; accf[s][m] = 0.f; }
-        sumd += (double)sumf;
-        sumf = 0.f;
+        flush();
     }
     double* pl = part + (size_t)ch * 2 * SL;
     double* pr = pl + SL;
     if (tid == 0) { pl[0] = (double)cnt_l; pr[0] = (double)cnt_r; }
-    if (tid < DP) pl[1 + tid] = sumd;
-    else if (tid < 2 * DP) pr[1 + tid - DP] = sumd;
+    if constexpr (S::BLOCKED) {
+        __syncthreads();
+        // sum the groups' FP64 totals; thread b < NBLK writes block b
+        if (tid < S::NBLK) {
+            int ri = 0, rem = tid;
+            while (rem >= S::NB - ri) { rem -= S::NB - ri; ++ri; }
+            const int rj = ri + rem;
+#pragma unroll 1
+            for (int s2 = 0; s2 < 2; ++s2) {
+                double* po = s2 ? pr : pl;
+                for (int m = 0; m < 16; ++m) {
+                    const int i = 4 * ri + (m >> 2), j = 4 * rj + (m & 3);
+                    if (i > j) continue;
+                    double v = 0.0;
+                    for (int g = 0; g < S::G; ++g) v += stot[(16 * s2 + m) * S::NTOT + g * S::NBLK + tid];
+                    po[1 + DP + tri_index(DP, i, j)] = v;
+                }
+            }
+        }
+        for (int e = tid; e < 2 * DP; e += 256) {
+            double v = 0.0;
+            for (int g = 0; g < S::G; ++g) v += ssum[g * 2 * DP + e];
+            (e < DP ? pl : pr)[1 + (e % DP)] = v;
+        }
+    } else {
+        if (tid < DP) pl[1 + tid] = sumd;
+        else if (tid < 2 * DP) pr[1 + tid - DP] = sumd;
 #pragma unroll
-    for (int m = 0; m < E; ++m) {
-        int e = tid + 256 * m;
-        if (e < T) { pl[1 + DP + e] = accd[0][m]; pr[1 + DP + e] = accd[1][m]; }
+        for (int m = 0; m < E; ++m) {
+            int e = tid + 256 * m;
+            if (e < T) { pl[1 + DP + e] = accd[0][m]; pr[1 + DP + e] = accd[1][m]; }
+        }
     }
 }
 
@@ -720,10 +867,8 @@ __global__ void __launch_bounds__(256) k_mult_sub_stats(
 template <int DP>
 static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout, const uint8_t* d_mask)
 {
-    constexpr int TP = DP >= 128 ? 128 : 256;
-    size_t sm = sizeof(float) * (2 * DP * DP + 3 * DP + TP * (DP + 1)) + sizeof(int32_t) * TP +
-                sizeof(uint16_t) * tri(DP);
-    auto kern = k_gauss_sub_stats<DP, TP>;
+    const size_t sm = SubStatsShape<DP>::bytes;
+    auto kern = k_gauss_sub_stats<DP>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c,
                                                 c->d_lrw, c->d_mu, draw, r, c->d_sub, d_rout, c->d_part, d_mask);

@@ -10,10 +10,10 @@
 // into a shared-memory table, and finishes with the softmax + Walker alias draw (or argmax)
 // of the reference (cudaKernel.cu:374-424, 27-124), one thread per point.
 //
-// CTA roles (192 threads): warp 0 streams B tiles (2 clusters = 128 columns, hi + lo, 32 KB,
+// CTA roles (320 threads): warp 0 streams B tiles (2 clusters = 128 columns, hi + lo, 32 KB,
 // stored pre-swizzled in global memory) with cp.async.bulk into a 2-3 stage ring; warp 1
 // allocates TMEM and issues tcgen05.mma (M=128, N=128, K=16; 12 per tile) into a
-// double-buffered accumulator (2 x 128 columns); warps 2-5 are the epilogue.  Every mbarrier
+// double-buffered accumulator (2 x 128 columns); warps 2-9 are the epilogue.  Every mbarrier
 // wait is bounded: on timeout the CTA records an error code, stops issuing work, drains what it
 // issued (bounded) and frees its TMEM.
 //
@@ -215,9 +215,13 @@ __global__ void k_pack_b(const float* __restrict__ Wt, int K, int Dp, int NT, ui
 }
 
 // ------------------------------------------------------------------------- label kernel
+// r table: one row of KS = K rounded up to odd floats per point.  The drain (32 points x one
+// cluster) and the per-point draw (32 points x the same cluster) both hit 32 distinct banks.
+__host__ __device__ constexpr int r_stride(int K) { return K | 1; }
+
 struct SmemLayout {
     int stages;
-    size_t a, b, r, ia, ib, bar, total;
+    size_t a, b, r, bar, total;
 };
 
 __host__ __device__ inline SmemLayout smem_layout(int K, int stages)
@@ -226,10 +230,8 @@ __host__ __device__ inline SmemLayout smem_layout(int K, int stages)
     L.stages = stages;
     L.a = 0;                                   // A hi, A lo (1024-aligned)
     L.b = 2 * A_BYTES;                         // stages x 32 KB
-    L.r = L.b + (size_t)stages * STAGE_BYTES;  // (K+2) x BM floats
-    L.ia = L.r + (size_t)(K + 2) * BM * 4;     // (K+2) x BM bytes
-    L.ib = L.ia + (size_t)(K + 2) * BM;
-    L.bar = (L.ib + (size_t)(K + 2) * BM + 15) / 16 * 16;
+    L.r = L.b + (size_t)stages * STAGE_BYTES;  // BM x r_stride(K) floats
+    L.bar = (L.r + (size_t)BM * r_stride(K) * 4 + 15) / 16 * 16;
     L.total = L.bar + 16 * 8 + 16 + 1024;      // barriers, tmem slot + flags, alignment slack
     return L;
 }
@@ -245,8 +247,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
     uint8_t* sA = smem + L.a;
     uint8_t* sB = smem + L.b;
     float* sr = reinterpret_cast<float*>(smem + L.r);
-    uint8_t* sia = smem + L.ia;
-    uint8_t* sib = smem + L.ib;
+    const int KS = r_stride(K);
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L.bar);
     uint64_t* full = bars;           // [stages]
     uint64_t* empty = bars + 4;      // [stages]
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
                     q1 = fmaf(z3, z3, q1);
                 }
                 const float r = __ldg(cvec + 3 * k) - 0.5f * (q0 + q1);
-                sr[k * BM + p] = r;
+                sr[p * KS + k] = r;
                 if (r_out && pt < N) r_out[pt * K + k] = r;
             }
             tc_fence_before();
@@ -409,32 +410,32 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
         // the draw reads every cluster's r of its point: both epilogue halves must be done
         asm volatile("bar.sync 1, %0;" ::"r"(EPI_WARPS * 32) : "memory");
         if (c == 0 && !*abort_flag && pt < N) {   // one thread per point draws
-            // softmax + alias draw (or argmax) per point
-            labels[pt] = [&]() {
-                if (final_) {
-                    float best = sr[p];
-                    int arg = 0;
-                    for (int k = 1; k < K; ++k) {
-                        float v = sr[k * BM + p];
-                        if (best < v) { best = v; arg = k; }
-                    }
-                    return arg + 1;
+            float* row = sr + (size_t)p * KS;
+            if (final_) {
+                // update_labels_by_max_index_kernel (cudaKernel.cu:405-424): first maximum wins
+                float best = row[0];
+                int arg = 0;
+                for (int k = 1; k < K; ++k) {
+                    const float v = row[k];
+                    if (best < v) { best = v; arg = k; }
                 }
-                float mx = sr[p];
-                for (int k = 1; k < K; ++k) mx = fmaxf(mx, sr[k * BM + p]);
+                labels[pt] = arg + 1;
+            } else {
+                // build_log_likelihood_array_kernel (cudaKernel.cu:374-403): max, exp, normalise
+                float mx = row[0];
+                for (int k = 1; k < K; ++k) mx = fmaxf(mx, row[k]);
                 float sum = 0.f;
                 for (int k = 0; k < K; ++k) {
-                    float ex = __expf(sr[k * BM + p] - mx);
-                    sr[k * BM + p] = ex;
+                    const float ex = __expf(row[k] - mx);
+                    row[k] = ex;
                     sum += ex;
                 }
                 const float inv = 1.0f / sum, fk = (float)K;
-                for (int k = K - 1; k >= 0; --k) sr[(k + 1) * BM + p] = (sr[k * BM + p] * inv) * fk;
+                for (int k = 0; k < K; ++k) row[k] = (row[k] * inv) * fk;
                 float u1, u2;
                 draw_uniform2(rng, pt, u1, u2);
-                AliasAcc<float, uint8_t> acc{sr + p, sia + p, sib + p, BM};
-                return alias_draw<float, uint8_t>(K, acc, u1, u2);
-            }();
+                labels[pt] = alias_draw_stream(row, 1, K, u1, u2);
+            }
         }
     }
     tc_fence_before();

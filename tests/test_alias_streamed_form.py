@@ -1,0 +1,121 @@
+"""The label kernels draw from the Walker alias table through a streamed form of the
+reference's construction (alias_draw_stream in dpmmsubclusters_gpu_b200/csrc/dpmm_device.cuh)
+instead of building the whole table (cudaKernel.cu:27-124).  This CPU test restates the
+streamed form in Python, line for line with the device function, and checks it against the
+oracle's sequential construction on random distributions, including exact ties (y == 1) and
+degenerate ones."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+
+def alias_stream(y, u1, u2):
+    """y[k-1] = p_k * K (float64).  Returns the 1-based label drawn with uniforms (u1, u2)."""
+    K = len(y)
+    ns = int(np.count_nonzero(y < 1.0))
+    col = min(max(int(u1 * (K - 1 + 0.999999) + 1), 1), K)
+    yc = y[col - 1]
+    if yc == 1.0:
+        return col
+    st = {"P": ns + 1, "sr": ns, "Q": ns, "ll": ns + 1, "D": 0.0, "C": 0.0, "Ccol": 0.0}
+
+    def next_large():
+        while True:
+            st["Q"] += 1
+            Q = st["Q"]
+            if Q > K:
+                return 0
+            e = Q
+            if y[Q - 1] < 1.0:
+                st["ll"] -= 1
+                while st["ll"] > 1 and y[st["ll"] - 1] < 1.0:
+                    st["ll"] -= 1
+                e = st["ll"]
+            ex = y[e - 1] - 1.0
+            if ex > 0.0:
+                st["C"] += ex
+                return e
+
+    def settle_col():
+        if not (1.0 + st["Ccol"] - st["D"] < u2):
+            return col
+        a = next_large()
+        return a if a != 0 else col
+
+    col_taken = False
+    cur = 0
+    while True:
+        st["P"] -= 1
+        P = st["P"]
+        if P < 1:
+            return col
+        s = P
+        if y[P - 1] >= 1.0:
+            st["sr"] += 1
+            while st["sr"] < K and y[st["sr"] - 1] >= 1.0:
+                st["sr"] += 1
+            s = st["sr"]
+        while st["C"] <= st["D"]:
+            cur = next_large()
+            if cur == 0:
+                return col
+            if cur == col:
+                col_taken = True
+                st["Ccol"] = st["C"]
+                if st["Ccol"] <= st["D"]:
+                    return settle_col()
+        if s == col:
+            return cur if yc < u2 else col
+        st["D"] += 1.0 - y[s - 1]
+        if col_taken and st["D"] >= st["Ccol"]:
+            return settle_col()
+
+
+def _cases(rng, n):
+    for it in range(n):
+        K = int(rng.integers(1, 48))
+        kind = it % 4
+        if kind == 0:
+            p = rng.dirichlet(np.ones(K))
+        elif kind == 1:
+            p = rng.dirichlet(np.ones(K) * 0.1)
+        elif kind == 2:      # many entries at exactly y = 1
+            p = np.full(K, 1.0 / K)
+            j = rng.integers(0, K, size=max(1, K // 3))
+            p[j] *= rng.uniform(0.5, 2, size=j.size)
+            p /= p.sum()
+        else:                # rational probabilities: exact cancellations in the pairing
+            q = rng.integers(0, 4, size=K).astype(float)
+            q[0] += 1
+            p = q / q.sum()
+        u1, u2 = rng.uniform(1e-7, 1, size=2)
+        yield p, u1, u2
+
+
+def test_streamed_form_matches_sequential_construction():
+    rng = np.random.default_rng(0)
+    tight = 0
+    n = 4000
+    for p, u1, u2 in _cases(rng, n):
+        lab, mg = O.alias_draw(p, u1, u2)
+        got = alias_stream(p * len(p), u1, u2)
+        if got != lab:
+            # the two orders of summation can only part at exact ties of the construction
+            assert mg < 1e-9, (p, u1, u2, lab, got, mg)
+            tight += 1
+    assert tight <= n // 500
+
+
+@pytest.mark.parametrize("K", [1, 2, 3, 200, 255])
+def test_streamed_form_edge_sizes(K):
+    rng = np.random.default_rng(K)
+    for _ in range(200):
+        p = rng.dirichlet(np.ones(K) * (0.2 if K > 3 else 1.0))
+        u1, u2 = rng.uniform(1e-7, 1, size=2)
+        lab, mg = O.alias_draw(p, u1, u2)
+        got = alias_stream(p * K, u1, u2)
+        assert got == lab or mg < 1e-9
+    # uniform distribution: every y is exactly 1, the draw is the column
+    for u1 in (1e-7, 0.5, 1.0):
+        assert alias_stream(np.ones(K), u1, 0.999) == min(max(int(u1 * (K - 1 + 0.999999) + 1), 1), K)
