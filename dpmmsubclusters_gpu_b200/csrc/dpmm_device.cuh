@@ -189,12 +189,12 @@ __device__ __forceinline__ int alias_draw2(float p1, float p2, float u1, float u
 //    when D > C, is aliased to the next large with positive excess.
 // The merge stops as soon as the drawn column is settled.  D and C are FP64 running sums in the
 // reference's consumption order.
+// ns = the number of categories with y < 1 (counted by the caller while it writes y).
 template <typename T>
-__device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int stride, int K, float u1, float u2)
+__device__ __forceinline__ int alias_draw_stream_ns(const T* __restrict__ ys, int stride, int K, int ns, float u1,
+                                                    float u2)
 {
     auto y = [&](int i) -> T { return ys[(size_t)i * stride]; };
-    int ns = 0;
-    for (int k = 0; k < K; ++k) ns += y(k) < (T)1 ? 1 : 0;
     const int col = alias_column(K, u1);
     const T yc = y(col - 1);
     if (yc == (T)1) return col;          // a large without excess is never consumed
@@ -212,6 +212,7 @@ __device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int s
             int e = Q;
             if (y(Q - 1) < (T)1) {
                 do { --ll; } while (ll > 1 && y(ll - 1) < (T)1);
+                if (ll < 1) return 0;     // unreachable: (ns, K] holds as many smalls as [1, ns] larges
                 e = ll;
             }
             const double ex = (double)y(e - 1) - 1.0;
@@ -235,6 +236,7 @@ __device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int s
         int s = P;
         if (y(P - 1) >= (T)1) {
             do { ++sr; } while (sr < K && y(sr - 1) >= (T)1);
+            if (sr > K) return col;       // unreachable, as above
             s = sr;
         }
         while (C <= D) {                  // the current large is used up: take the next
@@ -250,6 +252,14 @@ __device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int s
         D += 1.0 - (double)y(s - 1);
         if (col_taken && D >= Ccol) return settle_col();
     }
+}
+
+template <typename T>
+__device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int stride, int K, float u1, float u2)
+{
+    int ns = 0;
+    for (int k = 0; k < K; ++k) ns += ys[(size_t)k * stride] < (T)1 ? 1 : 0;
+    return alias_draw_stream_ns(ys, stride, K, ns, u1, u2);
 }
 
 }  // namespace dpmm

@@ -80,6 +80,7 @@ struct dpmm_ctx {
     bool points_ready = false;
     bool tc_ok = false;            // tensor-core kernel usable for this shape
     cudaStream_t stream = nullptr;
+    int num_sms = 0;               // streaming multiprocessors of the device (persistent grids)
 
     // points: N x Dp row-major FP32.  Gaussian points are stored shifted by `shift`
     // (their FP64 mean), which leaves every log-likelihood unchanged and keeps the FP32
@@ -102,6 +103,8 @@ struct dpmm_ctx {
     float* d_mu = nullptr;         // [3*k_max][Dp], mu - shift (Gaussian) / log theta (multinomial)
     uint8_t* d_Btc = nullptr;      // tensor-core B operand: per pair of clusters a 32 KB split-bf16,
                                    // K-major 128-byte-swizzled tile (Gaussian, Dp = 32 or 64)
+    uint8_t* d_Atc = nullptr;      // tensor-core A operand: per 128 points the same 32 KB split-bf16
+                                   // swizzled tile, packed once when the points are uploaded
     std::vector<float> h_param_stage;
 
     // label-ordered permutation of the points and the per-cluster chunk table
@@ -201,6 +204,7 @@ dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha);
 bool tc_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 dpmm_status pack_tc_params(dpmm_ctx* c, int K);
+dpmm_status pack_tc_points(dpmm_ctx* c);   // A operand from the uploaded points
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)
