@@ -147,7 +147,8 @@ static void free_ctx(dpmm_ctx* c)
     void* bufs[] = {c->d_x, c->d_gshift, c->d_labels, c->d_sub, c->d_curand, c->d_Wt, c->d_b, c->d_c, c->d_lrw,
                     c->d_mu, c->d_perm, c->d_blk_hist, c->d_seg, c->d_chunk, c->d_nchunks, c->d_part, c->d_stats,
                     c->d_u, c->d_bits, c->d_remap, c->d_aux, c->d_r64, c->d_dbl_scratch, c->d_prior, c->d_lml,
-                    c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc};
+                    c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc, c->d_rbuf,
+                    c->d_rpart};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -225,8 +226,10 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
         chk(dev_alloc(&c->d_Wt, (size_t)3 * KM * Dp * Dp));
         chk(dev_alloc(&c->d_b, (size_t)3 * KM * Dp));
         if ((Dp == 32 || Dp == 64) && c->ll_mode != DPMM_LL_FP32) {
-            chk(dev_alloc(&c->d_Btc, (size_t)(KM + 1) / 2 * 32768));
+            chk(dev_alloc(&c->d_Btc, tc_param_bytes(KM)));
             chk(dev_alloc(&c->d_Atc, (size_t)((N + 127) / 128) * 32768));
+            chk(dev_alloc(&c->d_rbuf, (size_t)N * KM));
+            chk(dev_alloc(&c->d_rpart, (size_t)4 * N));
         }
     }
     chk(dev_alloc(&c->d_c, (size_t)3 * KM));

@@ -189,15 +189,78 @@ __device__ __forceinline__ int alias_draw2(float p1, float p2, float u1, float u
 //    when D > C, is aliased to the next large with positive excess.
 // The merge stops as soon as the drawn column is settled.  D and C are FP64 running sums in the
 // reference's consumption order.
-// ns = the number of categories with y < 1 (counted by the caller while it writes y).
-template <typename T>
-__device__ __forceinline__ int alias_draw_stream_ns(const T* __restrict__ ys, int stride, int K, int ns, float u1,
-                                                    float u2)
+// Small/large flags of up to 256 categories as a bitmask in registers: bit (q - 1) % 32 of word
+// (q - 1) / 32 is set when category q is small.  The walks of the merge become bit scans.
+struct SmallMask {
+    uint32_t w[8];
+    int K;
+
+    __device__ __forceinline__ uint32_t word(int i) const
+    {
+        uint32_t v = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            if (j == i) v = w[j];
+        return v;
+    }
+    __device__ __forceinline__ bool small(int q) const { return (word((q - 1) >> 5) >> ((q - 1) & 31)) & 1u; }
+    // smallest small q > x (K + 1 if none)
+    __device__ __forceinline__ int next_small_after(int x) const
+    {
+        int res = K + 1;
+#pragma unroll
+        for (int j = 7; j >= 0; --j) {
+            uint32_t m = w[j];
+            const int lo = x - 32 * j;   // clear bits b with 32j + b + 1 <= x
+            m = lo <= 0 ? m : (lo >= 32 ? 0u : m & (~0u << lo));
+            if (m) res = 32 * j + __ffs(m);
+        }
+        return res;
+    }
+    // largest large q < x (0 if none)
+    __device__ __forceinline__ int prev_large_before(int x) const
+    {
+        int res = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int nv = K - 32 * j;   // valid bits in word j
+            uint32_t m = ~w[j] & (nv >= 32 ? ~0u : (nv <= 0 ? 0u : (1u << nv) - 1u));
+            const int hi = x - 1 - 32 * j;   // keep bits b with 32j + b + 1 < x
+            m = hi >= 32 ? m : (hi <= 0 ? 0u : m & ((1u << hi) - 1u));
+            if (m) res = 32 * j + 32 - __clz(m);
+        }
+        return res;
+    }
+};
+
+// The same flags read from y itself (any K): linear walks.  YF: y(i) for 0-based i.
+template <typename YF>
+struct ReadFlags {
+    YF y;
+    int K;
+    __device__ __forceinline__ bool small(int q) const { return y(q - 1) < 1.f; }
+    __device__ __forceinline__ int next_small_after(int x) const
+    {
+        int q = x + 1;
+        while (q <= K && !small(q)) ++q;
+        return q;
+    }
+    __device__ __forceinline__ int prev_large_before(int x) const
+    {
+        int q = x - 1;
+        while (q >= 1 && small(q)) --q;
+        return q;
+    }
+};
+
+// The merge of the two consumption streams (see above).  y(i) returns y of category i + 1 and
+// must return the same value on every call.
+template <typename YF, typename Flags>
+__device__ __forceinline__ int alias_merge(const YF& y, int K, int ns, const Flags& fl, float u1, float u2)
 {
-    auto y = [&](int i) -> T { return ys[(size_t)i * stride]; };
     const int col = alias_column(K, u1);
-    const T yc = y(col - 1);
-    if (yc == (T)1) return col;          // a large without excess is never consumed
+    const float yc = y(col - 1);
+    if (yc == 1.f) return col;           // a large without excess is never consumed
 
     int P = ns + 1;     // small-stream position (descending)
     int sr = ns;        // last small of (ns, K] taken (ascending)
@@ -210,8 +273,8 @@ __device__ __forceinline__ int alias_draw_stream_ns(const T* __restrict__ ys, in
     auto next_large = [&]() -> int {
         while (++Q <= K) {
             int e = Q;
-            if (y(Q - 1) < (T)1) {
-                do { --ll; } while (ll > 1 && y(ll - 1) < (T)1);
+            if (fl.small(Q)) {
+                ll = fl.prev_large_before(ll);
                 if (ll < 1) return 0;     // unreachable: (ns, K] holds as many smalls as [1, ns] larges
                 e = ll;
             }
@@ -232,10 +295,32 @@ __device__ __forceinline__ int alias_draw_stream_ns(const T* __restrict__ ys, in
 
     int cur = 0;
     for (;;) {
+        // Fast path: the next 8 positions of the small stream hold their own smalls (no displaced
+        // large among them), col is not one of them, and the current large still has capacity
+        // after all 8: none of these steps can change the outcome, so take them at once (same
+        // summation order as single steps).
+        if (cur != 0 && P > 8 && (col >= P || col < P - 8)) {
+            float v[8];
+#pragma unroll
+            for (int i = 0; i < 8; ++i) v[i] = y(P - 2 - i);
+            bool all_small = true;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) all_small = all_small && v[i] < 1.f;
+            if (all_small) {
+                double Dn = D;
+#pragma unroll
+                for (int i = 0; i < 8; ++i) Dn += 1.0 - (double)v[i];
+                if (Dn < C) {
+                    D = Dn;
+                    P -= 8;
+                    continue;
+                }
+            }
+        }
         if (--P < 1) return col;          // every small paired: col keeps itself
         int s = P;
-        if (y(P - 1) >= (T)1) {
-            do { ++sr; } while (sr < K && y(sr - 1) >= (T)1);
+        if (!fl.small(P)) {
+            sr = fl.next_small_after(sr);
             if (sr > K) return col;       // unreachable, as above
             s = sr;
         }
@@ -248,18 +333,42 @@ __device__ __forceinline__ int alias_draw_stream_ns(const T* __restrict__ ys, in
                 if (Ccol <= D) return settle_col();   // used up at once by the carried deficit
             }
         }
-        if (s == col) return yc < (T)u2 ? cur : col;
+        if (s == col) return yc < u2 ? cur : col;
         D += 1.0 - (double)y(s - 1);
         if (col_taken && D >= Ccol) return settle_col();
     }
 }
 
-template <typename T>
-__device__ __forceinline__ int alias_draw_stream(const T* __restrict__ ys, int stride, int K, float u1, float u2)
+// Alias draw over K categories given y(i) = p_{i+1} * K (FP32): register bitmask walks for
+// K <= 256, reads otherwise.
+template <typename YF>
+__device__ __forceinline__ int alias_draw_y(const YF& y, int K, float u1, float u2)
 {
+    if (K <= 256) {
+        SmallMask sm;
+        sm.K = K;
+        int ns = 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            uint32_t m = 0;
+            const int kend = min(K, 32 * j + 32);
+            for (int k = 32 * j; k < kend; ++k) m |= (y(k) < 1.f ? 1u : 0u) << (k - 32 * j);
+            sm.w[j] = m;
+            ns += __popc(m);
+        }
+        return alias_merge(y, K, ns, sm, u1, u2);
+    }
     int ns = 0;
-    for (int k = 0; k < K; ++k) ns += ys[(size_t)k * stride] < (T)1 ? 1 : 0;
-    return alias_draw_stream_ns(ys, stride, K, ns, u1, u2);
+    for (int k = 0; k < K; ++k) ns += y(k) < 1.f ? 1 : 0;
+    return alias_merge(y, K, ns, ReadFlags<YF>{y, K}, u1, u2);
+}
+
+// y stored in memory: ys[(k - 1) * stride] for category k.
+__device__ __forceinline__ int alias_draw_stream(const float* __restrict__ ys, int64_t stride, int K, float u1,
+                                                 float u2)
+{
+    auto y = [=](int i) -> float { return ys[(size_t)i * stride]; };
+    return alias_draw_y(y, K, u1, u2);
 }
 
 }  // namespace dpmm

@@ -105,6 +105,8 @@ struct dpmm_ctx {
                                    // K-major 128-byte-swizzled tile (Gaussian, Dp = 32 or 64)
     uint8_t* d_Atc = nullptr;      // tensor-core A operand: per 128 points the same 32 KB split-bf16
                                    // swizzled tile, packed once when the points are uploaded
+    float* d_rbuf = nullptr;       // tensor-core label phase: r cluster-major [k_max][N]
+    float* d_rpart = nullptr;      // per point and half: running max, sum of exp (or best, arg) [4][N]
     std::vector<float> h_param_stage;
 
     // label-ordered permutation of the points and the per-cluster chunk table
@@ -205,6 +207,7 @@ bool tc_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 dpmm_status pack_tc_params(dpmm_ctx* c, int K);
 dpmm_status pack_tc_points(dpmm_ctx* c);   // A operand from the uploaded points
+size_t tc_param_bytes(int k_max);          // B tiles + bias records for k_max clusters
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)

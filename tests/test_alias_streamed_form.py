@@ -20,6 +20,21 @@ def alias_stream(y, u1, u2):
         return col
     st = {"P": ns + 1, "sr": ns, "Q": ns, "ll": ns + 1, "D": 0.0, "C": 0.0, "Ccol": 0.0}
 
+    def small(q):
+        return y[q - 1] < 1.0
+
+    def next_small_after(x):          # SmallMask::next_small_after / LoadFlags
+        q = x + 1
+        while q <= K and not small(q):
+            q += 1
+        return q
+
+    def prev_large_before(x):         # SmallMask::prev_large_before / LoadFlags
+        q = x - 1
+        while q >= 1 and small(q):
+            q -= 1
+        return q
+
     def next_large():
         while True:
             st["Q"] += 1
@@ -27,10 +42,10 @@ def alias_stream(y, u1, u2):
             if Q > K:
                 return 0
             e = Q
-            if y[Q - 1] < 1.0:
-                st["ll"] -= 1
-                while st["ll"] > 1 and y[st["ll"] - 1] < 1.0:
-                    st["ll"] -= 1
+            if small(Q):
+                st["ll"] = prev_large_before(st["ll"])
+                if st["ll"] < 1:
+                    return 0
                 e = st["ll"]
             ex = y[e - 1] - 1.0
             if ex > 0.0:
@@ -46,15 +61,27 @@ def alias_stream(y, u1, u2):
     col_taken = False
     cur = 0
     while True:
+        # fast path: 8 own smalls ahead, col not among them, the current large covers them all
+        P = st["P"]
+        if cur != 0 and P > 8 and (col >= P or col < P - 8):
+            v = [y[P - 2 - i] for i in range(8)]
+            if all(t < 1.0 for t in v):
+                Dn = st["D"]
+                for t in v:
+                    Dn += 1.0 - t
+                if Dn < st["C"]:
+                    st["D"] = Dn
+                    st["P"] -= 8
+                    continue
         st["P"] -= 1
         P = st["P"]
         if P < 1:
             return col
         s = P
-        if y[P - 1] >= 1.0:
-            st["sr"] += 1
-            while st["sr"] < K and y[st["sr"] - 1] >= 1.0:
-                st["sr"] += 1
+        if not small(P):
+            st["sr"] = next_small_after(st["sr"])
+            if st["sr"] > K:
+                return col
             s = st["sr"]
         while st["C"] <= st["D"]:
             cur = next_large()
@@ -74,12 +101,16 @@ def alias_stream(y, u1, u2):
 
 def _cases(rng, n):
     for it in range(n):
-        K = int(rng.integers(1, 48))
+        K = int(rng.integers(1, 48)) if it % 8 else int(rng.integers(48, 160))
         kind = it % 4
         if kind == 0:
             p = rng.dirichlet(np.ones(K))
         elif kind == 1:
             p = rng.dirichlet(np.ones(K) * 0.1)
+            if it % 3 == 0:      # one dominant cluster: long runs of smalls (the chunked path)
+                p = np.full(K, 1e-7)
+                p[rng.integers(0, K)] = 1.0
+                p /= p.sum()
         elif kind == 2:      # many entries at exactly y = 1
             p = np.full(K, 1.0 / K)
             j = rng.integers(0, K, size=max(1, K // 3))
@@ -104,10 +135,11 @@ def test_streamed_form_matches_sequential_construction():
             # the two orders of summation can only part at exact ties of the construction
             assert mg < 1e-9, (p, u1, u2, lab, got, mg)
             tight += 1
-    assert tight <= n // 500
+    # one dominant cluster puts the total deficit and its excess within rounding of each other
+    assert tight <= n // 100
 
 
-@pytest.mark.parametrize("K", [1, 2, 3, 200, 255])
+@pytest.mark.parametrize("K", [1, 2, 3, 200, 255, 256, 300])
 def test_streamed_form_edge_sizes(K):
     rng = np.random.default_rng(K)
     for _ in range(200):

@@ -451,6 +451,41 @@ def test_tensor_core_alias_diffuse(K):
     assert np.mean(out[0][1] != out[1][1]) < 5e-3
 
 
+@pytest.mark.parametrize("K", [25, 130, 200])
+def test_tensor_core_persistent_many_tiles(K):
+    """About four tiles per CTA, so the persistent loop, the A / B / bias rings and the TMEM r
+    buffer all wrap (K = 25: three accumulators; 130: two; 200: one A slot).  r against the FP32
+    form (2e-4 relative), labels exact against the oracle's draw on the GPU's own r except at
+    margins below 1e-4, argmax labels against the oracle's argmax."""
+    from dpmmsubclusters_gpu_b200 import LL_TC_BF16X3
+    rng = np.random.default_rng(900 + K)
+    N, D = 148 * 128 * 4 + 77, 64
+    x = rng.normal(size=(N, D)) * 2.0
+    mu = rng.normal(size=(K, D)) * 0.5
+    A = rng.normal(size=(K, D, D)) / np.sqrt(D)
+    inv = np.einsum("kij,klj->kil", A, A) * 0.05 + np.eye(D)[None] * 0.05
+    logdet = -np.array([np.linalg.slogdet(m)[1] for m in inv])
+    w = rng.dirichlet(np.ones(K) * 3)
+    u = uniforms(2 * N, 40 + K)
+    out = {}
+    for mode in (LL_FP32, LL_TC_BF16X3):
+        ck = CudaKernel(prior_type.Gaussian, loglik_mode=mode, k_max=256).init(N, x, 3, points_major=True)
+        ck.set_gaussian_params(mu, inv, logdet, w)
+        r = ck.create_clusters_labels(K, uniforms=u, return_loglik=True).astype(np.float64)
+        lab = ck.get_labels()
+        rf = ck.create_clusters_labels(K, bFinal=True, return_loglik=True).astype(np.float64)
+        out[mode] = (r, lab, rf, ck.get_labels())
+        ck.release()
+    r_tc, lab_tc, rf_tc, labf_tc = out[LL_TC_BF16X3]
+    r_32 = out[LL_FP32][0]
+    err = np.abs(r_tc - r_32) / np.maximum(np.abs(r_32), 32)
+    assert err.max() <= 2e-4, err.max()
+    lab_o, mg = O.sample_labels(r_tc, u.reshape(N, 2).astype(np.float64))
+    _mismatch_ok(lab_tc, lab_o, mg, frac=5e-3)
+    lab_of, gap = O.sample_labels(rf_tc, np.zeros((N, 2)), final=True)
+    assert np.all((labf_tc == lab_of) | (gap < 1e-5))
+
+
 def test_tensor_core_matches_fp32_form():
     from dpmmsubclusters_gpu_b200 import LL_TC_BF16X3
     rng = np.random.default_rng(77)
