@@ -52,6 +52,29 @@ def peaks():
 
 
 # ----------------------------------------------------------------------------- workload
+LABEL_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
+                             "k_gauss_labels_tc_N1e6_D64.md")
+
+
+def label_kernel_traffic(N, K):
+    """DRAM bytes per launch of the tensor-core label kernel: the ncu capture in LABEL_PROFILE
+    (a smaller case of the same kernel), scaled to (N, K) by the kernel's traffic model
+    N * (256 B packed points + 4 K B r + 16 B partials)."""
+    vals = {}
+    try:
+        with open(LABEL_PROFILE) as f:
+            for line in f:
+                for key in ("dram_bytes_per_launch", "capture_N", "capture_K"):
+                    if line.strip().startswith(key + ":"):
+                        vals[key] = float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    if len(vals) != 3:
+        return None
+    model = lambda n, k: n * (256.0 + 4.0 * k + 16.0)
+    return vals["dram_bytes_per_launch"] * model(N, K) / model(vals["capture_N"], vals["capture_K"])
+
+
 def c5_config(args):
     return dict(N=args.n, D=args.d, K_true=args.k_true, alpha=10.0, nu=args.d + 3.0, kappa=1.0, iterations=300,
                 mean_sd=5.0, dirichlet=2.0)
@@ -332,16 +355,23 @@ def main():
     value = world * N * args.steps / (elapsed_ms / 1e3)
     pk, pk_src = peaks()
     k_mean = float(np.mean(ks)) if ks else float(k_before.value)
-    label_ms = ph_ms[0] / max(1, ph_calls[0])
+    # dominant kernel: the tensor-core label kernel alone (slot 7), else the whole label phase
+    tc_kernel = ph_calls[7] > 0
+    label_ms = ph_ms[7] / ph_calls[7] if tc_kernel else ph_ms[0] / max(1, ph_calls[0])
     flops = 2.0 * N * k_mean * D * D
     achieved = flops / (label_ms / 1e3) / 1e12 if label_ms > 0 else None
     peak = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
-    roofline = {"kernel": "label phase (fused N x K contraction + softmax + alias draw)",
+    roofline = {"kernel": ("k_gauss_labels_tc (N x K whitened contraction, split-BF16 tcgen05, + drain to r)"
+                           if tc_kernel else "label phase (FP32 SIMT contraction + softmax + alias draw)"),
                 "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "frac": (achieved / peak) if achieved else None,
+                "traffic": label_kernel_traffic(N, k_mean) if tc_kernel else None,
                 "peak_source": f"bf16_tflops of {pk_src}",
-                "algorithmic": f"2*N*K*D^2 FLOP per launch, K mean {k_mean:.1f}"}
-    phases = ["labels", "sub_labels_stats", "stats", "split_hastings", "merge_hastings", "relabel", "params", "-"]
+                "launch_ms": label_ms, "launches": int(ph_calls[7] if tc_kernel else ph_calls[0]),
+                "algorithmic": f"2*N*K*D^2 FLOP per launch (one product; the split form issues 3), "
+                               f"K mean {k_mean:.1f}"}
+    phases = ["labels", "sub_labels_stats", "stats", "split_hastings", "merge_hastings", "relabel", "params",
+              "label_tc_kernel"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3" if mode != capi.LL_FP32 else "f32",

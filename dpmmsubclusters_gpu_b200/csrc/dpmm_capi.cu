@@ -154,6 +154,8 @@ static void free_ctx(dpmm_ctx* c)
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->kev0) cudaEventDestroy(c->kev0);
+    if (c->kev1) cudaEventDestroy(c->kev1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -206,6 +208,8 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
         c->num_sms = 1;
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
+    cudaEventCreate(&c->kev0);
+    cudaEventCreate(&c->kev1);
     const int64_t N = c->N;
     const int Dp = c->Dp, KM = c->k_max;
     const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;

@@ -45,7 +45,7 @@ extern std::atomic<uint64_t> g_launches, g_h2d_bytes, g_d2h_bytes;
     } while (0)
 
 enum Phase { PH_LABELS = 0, PH_SUB_STATS = 1, PH_STATS = 2, PH_SPLIT_HR = 3, PH_MERGE_HR = 4, PH_RELABEL = 5,
-             PH_PARAMS = 6, PH_COUNT = 8 };
+             PH_PARAMS = 6, PH_LABEL_KERNEL = 7, PH_COUNT = 8 };
 
 #define DPMM_TRY(expr)                         \
     do {                                       \
@@ -149,6 +149,7 @@ struct dpmm_ctx {
 
     // events for phase timing (bench): device time per phase while `timing` is set
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // one kernel inside a phase (PH_LABEL_KERNEL)
     bool timing = false;
     double phase_ms[dpmm::PH_COUNT] = {0};
     int64_t phase_calls[dpmm::PH_COUNT] = {0};
@@ -170,6 +171,27 @@ struct PhaseTimer {
         if (cudaEventSynchronize(c->ev1) == cudaSuccess) {
             float ms = 0.f;
             cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+            c->phase_ms[ph] += ms;
+            c->phase_calls[ph] += 1;
+        }
+    }
+};
+
+// The same for one kernel launch inside a phase, with its own events.
+struct KernelTimer {
+    dpmm_ctx* c;
+    int ph;
+    KernelTimer(dpmm_ctx* ctx, int phase) : c(ctx), ph(phase)
+    {
+        if (c && c->timing) cudaEventRecord(c->kev0, c->stream);
+    }
+    ~KernelTimer()
+    {
+        if (!c || !c->timing) return;
+        cudaEventRecord(c->kev1, c->stream);
+        if (cudaEventSynchronize(c->kev1) == cudaSuccess) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->kev0, c->kev1);
             c->phase_ms[ph] += ms;
             c->phase_calls[ph] += 1;
         }

@@ -678,10 +678,13 @@ dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float
     const int64_t ntiles = (c->N + tc::BM - 1) / tc::BM;
     const int64_t nst = (ntiles + tc::HALVES - 1) / tc::HALVES;
     const unsigned grid = (unsigned)std::min<int64_t>(nst, c->num_sms);
-    tc::k_gauss_labels_tc<<<grid, tc::THREADS, L.total, c->stream>>>(c->d_Atc, c->N, (int)ntiles, c->d_Btc,
-                                                                     tc_bias_base(c), c->Dp, K, bstages, final_,
-                                                                     c->d_rbuf, c->d_rpart, d_rout, err);
-    DPMM_LAUNCHED();
+    {
+        KernelTimer kt(c, PH_LABEL_KERNEL);
+        tc::k_gauss_labels_tc<<<grid, tc::THREADS, L.total, c->stream>>>(c->d_Atc, c->N, (int)ntiles, c->d_Btc,
+                                                                         tc_bias_base(c), c->Dp, K, bstages, final_,
+                                                                         c->d_rbuf, c->d_rpart, d_rout, err);
+        DPMM_LAUNCHED();
+    }
     RngArgs r = rng_args(c, d_u);
     tc::k_draw_labels<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->d_rbuf, c->d_rpart, c->N, K, final_,
                                                                             r, c->d_labels);

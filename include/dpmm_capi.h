@@ -250,8 +250,8 @@ dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 /* Diagnostics (no counterpart in the reference, which prints per-iteration wall times only):
  * kernels this library has launched in this process; bytes it copied host->device and
  * device->host; device time per phase of a context (ms[8], calls[8]: labels, sub-labels +
- * statistics, statistics only, split ratios, merge ratios, relabels, parameters, -) accumulated
- * while timing is on.  enable = 1 / 0 switches timing on / off and clears the counters, -1 only
+ * statistics, statistics only, split ratios, merge ratios, relabels, parameters, and the
+ * tensor-core label kernel alone inside the label phase) accumulated while timing is on.  enable = 1 / 0 switches timing on / off and clears the counters, -1 only
  * reads them.  Timing adds one event synchronisation per phase. */
 uint64_t dpmm_kernel_launch_count(void);
 void dpmm_transfer_bytes(uint64_t* h2d, uint64_t* d2h);
