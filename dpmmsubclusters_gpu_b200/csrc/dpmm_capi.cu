@@ -214,7 +214,13 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     const int Dp = c->Dp, KM = c->k_max;
     const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     c->nblk_hist = (int)((N + 2047) / 2048);
-    c->max_chunks = (int)(N / kChunk) + KM + 1;
+    {
+        // about four waves of two blocks per SM over N points, in whole units, at most kChunkMax
+        const int64_t want = N / ((int64_t)c->num_sms * 2 * 4);
+        const int64_t units = std::max<int64_t>(1, std::min<int64_t>(kChunkMax / kChunkUnit, (want + kChunkUnit - 1) / kChunkUnit));
+        c->chunk_len = (int)(units * kChunkUnit);
+    }
+    c->max_chunks = (int)(N / c->chunk_len) + KM + 1;
     const int T = Dp * (Dp + 1) / 2;
     const int SL = gauss ? 1 + Dp + T : 1 + Dp;
     c->stat_len = gauss ? 1 + c->D + c->D * c->D : 1 + c->D;
@@ -464,34 +470,53 @@ static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, con
     float* hmu = hc + 3 * K;
     std::vector<float> hlrw(2 * K, 0.f);
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));   // the pinned stage may still be in flight
-    std::vector<double> W;
-    for (int k = 0; k < K; ++k) {
-        for (int s = 0; s < 3; ++s) {
+    // every slot is independent: pack them in parallel, keep the first error
+    int err_slot = -1;
+    dpmm_status err_status = DPMM_OK;
+#pragma omp parallel
+    {
+        std::vector<double> W;
+#pragma omp for schedule(dynamic, 4)
+        for (int q = 0; q < 3 * K; ++q) {
+            const int k = q / 3, s = q % 3;
             const bool sub = s > 0;
             if (sub && !mu_lr) {
                 // no sub-cluster parameters: zero slots (sub-label phase then needs them set later)
-                std::fill(hWt + (size_t)(3 * k + s) * Dp * Dp, hWt + (size_t)(3 * k + s + 1) * Dp * Dp, 0.f);
-                std::fill(hb + (size_t)(3 * k + s) * Dp, hb + (size_t)(3 * k + s + 1) * Dp, 0.f);
-                std::fill(hmu + (size_t)(3 * k + s) * Dp, hmu + (size_t)(3 * k + s + 1) * Dp, 0.f);
-                hc[3 * k + s] = 0.f;
+                std::fill(hWt + (size_t)q * Dp * Dp, hWt + (size_t)(q + 1) * Dp * Dp, 0.f);
+                std::fill(hb + (size_t)q * Dp, hb + (size_t)(q + 1) * Dp, 0.f);
+                std::fill(hmu + (size_t)q * Dp, hmu + (size_t)(q + 1) * Dp, 0.f);
+                hc[q] = 0.f;
                 continue;
             }
             const int idx = sub ? 2 * k + (s - 1) : k;
             const double* m = sub ? mu_lr + (size_t)idx * D : mu + (size_t)k * D;
             const double* A = sub ? mat_lr + (size_t)idx * D * D : mat + (size_t)k * D * D;
             const double ld = sub ? logdet_lr[idx] : logdet[k];
+            dpmm_status st = DPMM_OK;
             if (is_factor) {
                 W.assign(A, A + (size_t)D * D);
             } else if (!la::cholesky(A, D, W)) {
-                return fail(DPMM_ERR_NOT_PD, "inv_sigma of cluster " + std::to_string(k) + (sub ? " (sub)" : "") +
-                                                 " is not positive definite");
+                st = DPMM_ERR_NOT_PD;
             }
             double cval = -ld / 2;
             if (!sub) cval += std::log(weights[k]);
-            if (!std::isfinite(cval) && !(cval < 0)) return fail(DPMM_ERR_NUMERIC, "non-finite log-likelihood constant");
-            pack_gauss_slot(c, 3 * k + s, m, W, cval, hWt, hb, hc, hmu);
+            if (st == DPMM_OK && !std::isfinite(cval) && !(cval < 0)) st = DPMM_ERR_NUMERIC;
+            if (st != DPMM_OK) {
+#pragma omp critical(dpmm_pack_err)
+                if (err_slot < 0 || q < err_slot) { err_slot = q; err_status = st; }
+                continue;
+            }
+            pack_gauss_slot(c, q, m, W, cval, hWt, hb, hc, hmu);
             if (sub) hlrw[idx] = lr_weights ? (float)std::log(lr_weights[idx]) : 0.f;
         }
+    }
+    if (err_slot >= 0) {
+        const int k = err_slot / 3;
+        const bool sub = err_slot % 3 != 0;
+        if (err_status == DPMM_ERR_NOT_PD)
+            return fail(DPMM_ERR_NOT_PD, "inv_sigma of cluster " + std::to_string(k) + (sub ? " (sub)" : "") +
+                                             " is not positive definite");
+        return fail(DPMM_ERR_NUMERIC, "non-finite log-likelihood constant");
     }
     // relocate packed arrays to their device buffers
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_Wt, hWt, sizeof(float) * 3 * K * (size_t)Dp * Dp, cudaMemcpyHostToDevice, c->stream));

@@ -19,8 +19,10 @@ namespace dpmm {
 constexpr int kMaxGaussDim = 128;
 // Largest dimension of the multinomial kernels (count vectors).
 constexpr int kMaxMultDim = 4096;
-// Points per chunk of the segmented (per-cluster) passes.
-constexpr int kChunk = 4096;
+// Points per chunk of the segmented (per-cluster) passes: a multiple of kChunkUnit between
+// kChunkUnit and kChunkMax, the smallest that still gives about four waves of blocks.
+constexpr int kChunkUnit = 1024;
+constexpr int kChunkMax = 4096;
 
 int padded_dim(int d);  // 4, 8, 16, 32, 64, 128 (Gaussian); d rounded up to 32 (multinomial)
 
@@ -117,6 +119,7 @@ struct dpmm_ctx {
     int32_t* d_chunk = nullptr;    // [max_chunks][3] (cluster, start, len)
     int32_t* d_nchunks = nullptr;
     int max_chunks = 0;
+    int chunk_len = dpmm::kChunkMax;   // points per chunk (see kChunkUnit)
     int perm_K = -1;               // K the permutation was built for (-1: stale)
 
     // statistics: chunk partials (FP64) and per-slot results in original coordinates

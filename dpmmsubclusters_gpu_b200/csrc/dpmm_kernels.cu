@@ -357,9 +357,10 @@ __global__ void k_scan_bins(int32_t* __restrict__ blk_hist, int nblk, int K, int
     if (threadIdx.x == 0) total[k] = carry;
 }
 
-// single block: segment starts and the chunk table (cluster, start, len) of <= kChunk points
+// single block: segment starts and the chunk table (cluster, start, len) of <= chunk_len points
 __global__ void k_segments(const int32_t* __restrict__ total, int K, int32_t* __restrict__ seg,
-                           int32_t* __restrict__ chunk, int32_t* __restrict__ nchunks, int max_chunks)
+                           int32_t* __restrict__ chunk, int32_t* __restrict__ nchunks, int max_chunks,
+                           int chunk_len)
 {
     if (threadIdx.x != 0) return;
     int32_t acc = 0, nc = 0;
@@ -367,10 +368,10 @@ __global__ void k_segments(const int32_t* __restrict__ total, int K, int32_t* __
         seg[k] = acc;
         int32_t t = total[k];
         if (k < K) {
-            for (int32_t s = 0; s < t && nc < max_chunks; s += kChunk) {
+            for (int32_t s = 0; s < t && nc < max_chunks; s += chunk_len) {
                 chunk[3 * nc + 0] = k;
                 chunk[3 * nc + 1] = acc + s;
-                chunk[3 * nc + 2] = min(kChunk, t - s);
+                chunk[3 * nc + 2] = min(chunk_len, t - s);
                 ++nc;
             }
         }
@@ -421,7 +422,8 @@ dpmm_status build_permutation(dpmm_ctx* c, int K)
     int32_t* total = c->d_aux + 8;   // K+1 entries
     k_scan_bins<<<K + 1, 1024, 0, c->stream>>>(c->d_blk_hist, nblk, K, total);
     DPMM_LAUNCHED();
-    k_segments<<<1, 32, 0, c->stream>>>(total, K, c->d_seg, c->d_chunk, c->d_nchunks, c->max_chunks);
+    k_segments<<<1, 32, 0, c->stream>>>(total, K, c->d_seg, c->d_chunk, c->d_nchunks, c->max_chunks,
+                                         c->chunk_len);
     DPMM_LAUNCHED();
     size_t sm = sizeof(int32_t) * 9 * (K + 1);
     if (sm > 48 * 1024) DPMM_CUDA_TRY(cudaFuncSetAttribute(k_scatter, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -438,7 +440,7 @@ __host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
 // Gaussian: one block per chunk of one cluster (points in permutation order).  Draws the
 // sub-labels (unless draw == 0, in which case the current sub-labels are used) and accumulates
 // per sub-cluster: count, sum(x - s) and the upper triangle of sum (x - s)(x - s)^T, shift
-// s = the cluster's mean parameter.  FP32 products, FP32 runs of 32 points, FP64 totals.
+// s = the cluster's mean parameter.  FP32 products, FP32 runs of at most 33 points, FP64 totals.
 //
 // DP <= 64 ("blocked" form, 128 points per tile):
 //   draw  - two threads per point, one per side: warps 0-3 evaluate the l factor, warps 4-7 the r
@@ -525,6 +527,18 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
         }
     }
     for (int e = tid; e < DP; e += 256) ss[e] = muv[(size_t)(3 * k) * DP + e];
+    if (draw) {
+        // the points are staged centred on s = the cluster's mean: z = W^T (x - s) - b' with
+        // b' = b - W^T s (thread j: row j of the l factor; thread DP + j: of the r factor)
+        __syncthreads();
+        if (tid < 2 * DP) {
+            const int j = tid % DP;
+            const float* wrow = (tid < DP ? sWl : sWr) + j * DP;
+            float acc = 0.f;
+            for (int i = 0; i < DP; ++i) acc = fmaf(wrow[i], ss[i], acc);
+            (tid < DP ? sbl : sbr)[j] -= acc;
+        }
+    }
     if constexpr (!S::BLOCKED) {
         for (int e = tid; e < T; e += 256) {
             int i = 0, rem = e;
@@ -598,14 +612,38 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
         }
     };
 
+    // tile staging: each thread holds NPF float4 of the next tile in registers, loaded while the
+    // current tile's statistics accumulate, and stores them centred on s at the next tile's start
+    constexpr int NV = TP * DP / 4;                 // float4 per tile
+    constexpr int NPF = (NV + 255) / 256;
+    float4 pf[NPF];
+    auto load_tile = [&](int t0) {
+        const int ntn = min(TP, len - t0);
+#pragma unroll
+        for (int u = 0; u < NPF; ++u) {
+            const int e = tid + 256 * u;
+            const int pp = e / (DP / 4), i4 = e % (DP / 4);
+            pf[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (e < NV && pp < ntn)
+                pf[u] = __ldg(reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + pp) * DP) + i4);
+        }
+    };
+    constexpr bool PREFETCH = DP <= 64;             // DP = 128: too many registers, load at the tile start
+    if (PREFETCH) load_tile(0);
     for (int t0 = 0; t0 < len; t0 += TP) {
         const int nt = min(TP, len - t0);
+        if (!PREFETCH) load_tile(t0);
         __syncthreads();
-        for (int e = tid; e < TP * DP / 4; e += 256) {
-            const int pp = e / (DP / 4), i4 = e % (DP / 4);
-            float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (pp < nt) v = reinterpret_cast<const float4*>(x + (size_t)perm[start + t0 + pp] * DP)[i4];
-            *reinterpret_cast<float4*>(sx + pp * SX + 4 * i4) = v;
+#pragma unroll
+        for (int u = 0; u < NPF; ++u) {
+            const int e = tid + 256 * u;
+            if (e < NV) {
+                const int pp = e / (DP / 4), i4 = e % (DP / 4);
+                const float4 sv4 = *reinterpret_cast<const float4*>(ss + 4 * i4);
+                float4 v = pf[u];
+                if (pp < nt) { v.x -= sv4.x; v.y -= sv4.y; v.z -= sv4.z; v.w -= sv4.w; }
+                *reinterpret_cast<float4*>(sx + pp * SX + 4 * i4) = v;
+            }
         }
         __syncthreads();
         if (draw) {
@@ -690,44 +728,50 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
         }
         cnt_l += __syncthreads_count(sv == 1);
         cnt_r += __syncthreads_count(sv == 2);
-        for (int e = tid; e < nt * DP; e += 256) {
-            int pp = e / DP, i = e % DP;
-            sx[pp * SX + i] -= ss[i];
-        }
-        __syncthreads();
+        if (PREFETCH && t0 + TP < len) load_tile(t0 + TP);
         if constexpr (S::BLOCKED) {
             if (grp < S::G) {
-                int run = 0;
-                for (int pp = grp; pp < nt; pp += S::G) {
-                    const int sv2 = ssub[pp];
-                    if (sv2 != 1 && sv2 != 2) continue;
-                    if (has_blk) {
-                        const float* xp = sx + pp * SX;
-                        const float4 xi = *reinterpret_cast<const float4*>(xp + 4 * bi);
-                        const float4 xj = *reinterpret_cast<const float4*>(xp + 4 * bj);
-                        const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
-                        const float vj[4] = {xj.x, xj.y, xj.z, xj.w};
-                        if (sv2 == 1) {
+                // two points per iteration: both points' loads issue before either's FMAs
+                auto acc = [&](int sv2, const float4 xi, const float4 xj) {
+                    const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+                    const float vj[4] = {xj.x, xj.y, xj.z, xj.w};
+                    if (sv2 == 1) {
 #pragma unroll
-                            for (int a = 0; a < 4; ++a)
+                        for (int a = 0; a < 4; ++a)
 #pragma unroll
-                                for (int c = 0; c < 4; ++c) bf[0][4 * a + c] = fmaf(vi[a], vj[c], bf[0][4 * a + c]);
-                            if (diag) {
+                            for (int c = 0; c < 4; ++c) bf[0][4 * a + c] = fmaf(vi[a], vj[c], bf[0][4 * a + c]);
+                        if (diag) {
 #pragma unroll
-                                for (int a = 0; a < 4; ++a) sf[0][a] += vi[a];
-                            }
-                        } else {
+                            for (int a = 0; a < 4; ++a) sf[0][a] += vi[a];
+                        }
+                    } else if (sv2 == 2) {
 #pragma unroll
-                            for (int a = 0; a < 4; ++a)
+                        for (int a = 0; a < 4; ++a)
 #pragma unroll
-                                for (int c = 0; c < 4; ++c) bf[1][4 * a + c] = fmaf(vi[a], vj[c], bf[1][4 * a + c]);
-                            if (diag) {
+                            for (int c = 0; c < 4; ++c) bf[1][4 * a + c] = fmaf(vi[a], vj[c], bf[1][4 * a + c]);
+                        if (diag) {
 #pragma unroll
-                                for (int a = 0; a < 4; ++a) sf[1][a] += vi[a];
-                            }
+                            for (int a = 0; a < 4; ++a) sf[1][a] += vi[a];
                         }
                     }
-                    if (++run == 32) { flush(); run = 0; }
+                };
+                int run = 0;
+                for (int pp = grp; pp < nt; pp += 2 * S::G) {
+                    const int pq = pp + S::G;
+                    const int sa = ssub[pp];
+                    const int sb2 = pq < nt ? ssub[pq] : 0;
+                    if (has_blk) {
+                        const float* xa = sx + pp * SX;
+                        const float* xb = sx + (pq < nt ? pq : pp) * SX;
+                        const float4 xia = *reinterpret_cast<const float4*>(xa + 4 * bi);
+                        const float4 xja = *reinterpret_cast<const float4*>(xa + 4 * bj);
+                        const float4 xib = *reinterpret_cast<const float4*>(xb + 4 * bi);
+                        const float4 xjb = *reinterpret_cast<const float4*>(xb + 4 * bj);
+                        acc(sa, xia, xja);
+                        acc(sb2, xib, xjb);
+                    }
+                    run += ((sa == 1 || sa == 2) ? 1 : 0) + ((sb2 == 1 || sb2 == 2) ? 1 : 0);
+                    if (run >= 32) { flush(); run = 0; }   // FP32 runs of at most 33 points
                 }
             }
         } else {

@@ -329,6 +329,7 @@ dpmm_status Sampler::upload_params(const std::vector<double>& weights)
     }
     std::vector<double> mu((size_t)K * D), W((size_t)K * D * D), ld(K), mu_lr((size_t)2 * K * D),
         W_lr((size_t)2 * K * D * D), ld_lr(2 * (size_t)K);
+#pragma omp parallel for schedule(static)
     for (int k = 0; k < K; ++k) {
         const Dist* ds[3] = {&clusters_[k].c.dist, &clusters_[k].l.dist, &clusters_[k].r.dist};
         std::memcpy(&mu[(size_t)k * D], ds[0]->mu.data(), sizeof(double) * D);
@@ -383,17 +384,25 @@ void Sampler::sample_cluster_params_all()
     const uint64_t base = draw_ctr_;
     draw_ctr_ += 3 * (uint64_t)K;
     std::vector<double> lml_lr(K, 0.0);
+    // one task per draw (3 per cluster) and per sub-cluster marginal likelihood: the tasks of a
+    // cluster are independent, so they balance over the threads better than whole clusters
+    const int nt = (int)todo.size();
+    std::vector<double> lml_s(2 * (size_t)nt, 0.0);
 #pragma omp parallel for schedule(dynamic)
-    for (int t = 0; t < (int)todo.size(); ++t) {
+    for (int q = 0; q < 5 * nt; ++q) {
+        const int t = q / 5, s = q % 5;
         const int i = todo[t];
         Splittable& sc = clusters_[i];
-        ClusterParams* cp[3] = {&sc.c, &sc.l, &sc.r};
-        for (int s = 0; s < 3; ++s) {
+        if (s < 3) {
+            ClusterParams* cp = s == 0 ? &sc.c : (s == 1 ? &sc.l : &sc.r);
             std::mt19937_64 g = draw_gen(base + 3 * (uint64_t)i + s);
-            cp[s]->dist = sample(cp[s]->post, g);
+            cp->dist = sample(cp->post, g);
+        } else {
+            const ClusterParams& cp = s == 3 ? sc.l : sc.r;
+            lml_s[2 * (size_t)t + (s - 3)] = lml(cp.prior, cp.post, cp.stats);
         }
-        lml_lr[i] = lml(sc.l.prior, sc.l.post, sc.l.stats) + lml(sc.r.prior, sc.r.post, sc.r.stats);
     }
+    for (int t = 0; t < nt; ++t) lml_lr[todo[t]] = lml_s[2 * (size_t)t] + lml_s[2 * (size_t)t + 1];
     const int B = cfg_.burnout;
     for (int i : todo) {
         Splittable& sc = clusters_[i];
