@@ -13,21 +13,25 @@ inline double& at(std::vector<double>& a, int n, int i, int j) { return a[(size_
 inline double at(const std::vector<double>& a, int n, int i, int j) { return a[(size_t)j * n + i]; }
 
 // Lower Cholesky factor L (A = L L^T) of a symmetric matrix, reading A's lower triangle.
-// Returns false if A is not positive definite.
+// Returns false if A is not positive definite.  Left-looking by columns: column j of L is A's
+// column j minus L(j, q) times column q of L for q < j, each a contiguous AXPY (the terms are
+// subtracted in the same order, q ascending, as in the dot-product form).
 inline bool cholesky(const double* A, int n, std::vector<double>& L)
 {
     L.assign((size_t)n * n, 0.0);
     for (int j = 0; j < n; ++j) {
-        double s = A[(size_t)j * n + j];
-        for (int q = 0; q < j; ++q) s -= L[(size_t)q * n + j] * L[(size_t)q * n + j];
+        double* cj = &L[(size_t)j * n];
+        for (int i = j; i < n; ++i) cj[i] = A[(size_t)j * n + i];
+        for (int q = 0; q < j; ++q) {
+            const double* cq = &L[(size_t)q * n];
+            const double f = cq[j];
+            for (int i = j; i < n; ++i) cj[i] -= f * cq[i];
+        }
+        const double s = cj[j];
         if (!(s > 0) || !std::isfinite(s)) return false;
         const double d = std::sqrt(s);
-        L[(size_t)j * n + j] = d;
-        for (int i = j + 1; i < n; ++i) {
-            double t = A[(size_t)j * n + i];
-            for (int q = 0; q < j; ++q) t -= L[(size_t)q * n + i] * L[(size_t)q * n + j];
-            L[(size_t)j * n + i] = t / d;
-        }
+        cj[j] = d;
+        for (int i = j + 1; i < n; ++i) cj[i] /= d;
     }
     return true;
 }

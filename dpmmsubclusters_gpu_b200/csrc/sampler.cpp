@@ -203,16 +203,24 @@ private:
             std::chi_squared_distribution<double> cs(h.v - i);
             A[(size_t)i * D + i] = std::sqrt(cs(g));
         }
-        // W = L^-T A: solve L^T W = A column by column (back substitution; A is lower-triangular)
-        d.W.assign((size_t)D * D, 0.0);
-        for (int c = 0; c < D; ++c) {
-            double* w = &d.W[(size_t)c * D];
-            for (int i = D - 1; i >= 0; --i) {
-                double s = i >= c ? A[(size_t)c * D + i] : 0.0;
-                for (int q = i + 1; q < D; ++q) s -= L[(size_t)i * D + q] * w[q];
-                w[i] = s / L[(size_t)i * D + i];
+        // W = L^-T A: solve L^T W = A by back substitution over rows, all columns at once (A is
+        // lower-triangular); each update is a contiguous AXPY over a row of W, with the terms
+        // subtracted in the same order (q ascending) as a per-column solve
+        std::vector<double> Wr((size_t)D * D);   // row-major: Wr[i * D + c] = W(i, c)
+        for (int i = D - 1; i >= 0; --i) {
+            double* wi = &Wr[(size_t)i * D];
+            for (int c = 0; c < D; ++c) wi[c] = i >= c ? A[(size_t)c * D + i] : 0.0;
+            for (int q = i + 1; q < D; ++q) {
+                const double f = L[(size_t)i * D + q];   // L(q, i)
+                const double* wq = &Wr[(size_t)q * D];
+                for (int c = 0; c < D; ++c) wi[c] -= f * wq[c];
             }
+            const double dii = L[(size_t)i * D + i];
+            for (int c = 0; c < D; ++c) wi[c] /= dii;
         }
+        d.W.resize((size_t)D * D);
+        for (int c = 0; c < D; ++c)
+            for (int i = 0; i < D; ++i) d.W[(size_t)c * D + i] = Wr[(size_t)i * D + c];
         double ldl = 0, lda = 0;
         for (int i = 0; i < D; ++i) {
             ldl += std::log(L[(size_t)i * D + i]);
