@@ -148,7 +148,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_mu, c->d_perm, c->d_blk_hist, c->d_seg, c->d_chunk, c->d_nchunks, c->d_part, c->d_stats,
                     c->d_u, c->d_bits, c->d_remap, c->d_aux, c->d_r64, c->d_dbl_scratch, c->d_prior, c->d_lml,
                     c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc, c->d_rbuf,
-                    c->d_rpart};
+                    c->d_rpart, c->d_Bsub};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -240,6 +240,7 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
             chk(dev_alloc(&c->d_Atc, (size_t)((N + 127) / 128) * 32768));
             chk(dev_alloc(&c->d_rbuf, (size_t)N * KM));
             chk(dev_alloc(&c->d_rpart, (size_t)4 * N));
+            chk(dev_alloc(&c->d_Bsub, (size_t)KM * 32768));
         }
     }
     chk(dev_alloc(&c->d_c, (size_t)3 * KM));

@@ -340,9 +340,11 @@ __device__ __forceinline__ int alias_merge(const YF& y, int K, int ns, const Fla
 }
 
 // Alias draw over K categories given y(i) = p_{i+1} * K (FP32): register bitmask walks for
-// K <= 256, reads otherwise.
-template <typename YF>
-__device__ __forceinline__ int alias_draw_y(const YF& y, int K, float u1, float u2)
+// K <= 256, reads otherwise.  SF: is_small(i), the small/large split the merge follows (y(i) < 1,
+// or an equivalent cheaper test; at an exact tie either answer keeps the walk consistent: a
+// small with y >= 1 adds no deficit and a large with y <= 1 has no excess to give).
+template <typename YF, typename SF>
+__device__ __forceinline__ int alias_draw_y(const YF& y, const SF& is_small, int K, float u1, float u2)
 {
     if (K <= 256) {
         SmallMask sm;
@@ -352,7 +354,7 @@ __device__ __forceinline__ int alias_draw_y(const YF& y, int K, float u1, float 
         for (int j = 0; j < 8; ++j) {
             uint32_t m = 0;
             const int kend = min(K, 32 * j + 32);
-            for (int k = 32 * j; k < kend; ++k) m |= (y(k) < 1.f ? 1u : 0u) << (k - 32 * j);
+            for (int k = 32 * j; k < kend; ++k) m |= (is_small(k) ? 1u : 0u) << (k - 32 * j);
             sm.w[j] = m;
             ns += __popc(m);
         }
@@ -368,7 +370,8 @@ __device__ __forceinline__ int alias_draw_stream(const float* __restrict__ ys, i
                                                  float u2)
 {
     auto y = [=](int i) -> float { return ys[(size_t)i * stride]; };
-    return alias_draw_y(y, K, u1, u2);
+    auto is_small = [=](int i) -> bool { return ys[(size_t)i * stride] < 1.f; };
+    return alias_draw_y(y, is_small, K, u1, u2);
 }
 
 }  // namespace dpmm

@@ -107,6 +107,8 @@ struct dpmm_ctx {
                                    // K-major 128-byte-swizzled tile (Gaussian, Dp = 32 or 64)
     uint8_t* d_Atc = nullptr;      // tensor-core A operand: per 128 points the same 32 KB split-bf16
                                    // swizzled tile, packed once when the points are uploaded
+    uint8_t* d_Bsub = nullptr;     // tensor-core sub-label phase: per cluster its two sub-cluster
+                                   // factors as one 32 KB split-bf16 swizzled B tile
     float* d_rbuf = nullptr;       // tensor-core label phase: r cluster-major [k_max][N]
     float* d_rpart = nullptr;      // per point and half: running max, sum of exp (or best, arg) [4][N]
     std::vector<float> h_param_stage;
@@ -233,6 +235,9 @@ dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float
 dpmm_status pack_tc_params(dpmm_ctx* c, int K);
 dpmm_status pack_tc_points(dpmm_ctx* c);   // A operand from the uploaded points
 size_t tc_param_bytes(int k_max);          // B tiles + bias records for k_max clusters
+// tensor-core sub-label kernel (dpmm_tc.cu): draws the sub-labels only (statistics separately)
+bool tc_sub_supported(const dpmm_ctx* c);
+dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)

@@ -925,6 +925,11 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
 {
     if (c->perm_K != K) DPMM_TRY(build_permutation(c, K));
     RngArgs r = rng_args(c, d_u);
+    if (draw && !d_mask && tc_sub_supported(c)) {
+        // sub-labels on the tensor cores, then the statistics of the drawn sub-labels
+        DPMM_TRY(launch_sub_labels_tc(c, r, d_rout));
+        draw = false;
+    }
     if (c->prior == DPMM_PRIOR_GAUSSIAN) {
         switch (c->Dp) {
             case 4: DPMM_TRY(launch_gauss_sub_stats_t<4>(c, draw, r, d_rout, d_mask)); break;

@@ -214,21 +214,25 @@ __device__ __forceinline__ void bf16_split(float v, __nv_bfloat16& hi, __nv_bflo
 // ------------------------------------------------------------------------- B packing
 // Bpack[t] = 32 KB: hi (16 KB) then lo (16 KB) of the 128 x 64 K-major swizzled tile holding
 // rows n = (c, j) -> W_{2t+c}(i, j) over i (zero outside the K clusters / the dimension).
-__global__ void k_pack_b(const float* __restrict__ Wt, int K, int Dp, int NT, uint8_t* __restrict__ Bpack)
+// sub = 1: tile t holds instead the two sub-cluster factors of cluster t (slots 3t+1, 3t+2),
+// the B operand of the sub-label contraction.
+__global__ void k_pack_b(const float* __restrict__ Wt, int K, int Dp, int NT, int sub, uint8_t* __restrict__ Bpack)
 {
     const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (t, n, chunk)
     if (e >= NT * BN * 8) return;
     const int t = e / (BN * 8);
     const int n = (e / 8) % BN;
     const int ch = e % 8;
-    const int k = CPT * t + n / KD;
+    const int half = n / KD;
+    const bool valid = sub ? t < K : CPT * t + half < K;
+    const int slot = sub ? 3 * t + 1 + half : 3 * (CPT * t + half);
     const int j = n % KD;
     __align__(16) __nv_bfloat16 hi[8], lo[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int i = ch * 8 + q;
         float w = 0.f;
-        if (k < K && j < Dp && i < Dp) w = Wt[((size_t)3 * k * Dp + j) * Dp + i];
+        if (valid && j < Dp && i < Dp) w = Wt[((size_t)slot * Dp + j) * Dp + i];
         bf16_split(w, hi[q], lo[q]);
     }
     uint8_t* base = Bpack + (size_t)t * STAGE_BYTES;
@@ -605,9 +609,190 @@ __global__ void __launch_bounds__(256) k_draw_labels(const float* __restrict__ r
     const float inv = 1.0f / sum, fk = (float)K;
     const float* rp = rbuf + pt;
     auto y = [=](int i) -> float { return (__expf(__ldg(rp + (size_t)i * N) - mx) * inv) * fk; };
+    // y < 1  <=>  r < max + log(sum / K): one compare per cluster for the small/large split
+    const float thr = mx + __logf(sum / fk);
+    auto is_small = [=](int i) -> bool { return __ldg(rp + (size_t)i * N) < thr; };
     float u1, u2;
     draw_uniform2(rng, pt, u1, u2);
-    labels[pt] = alias_draw_y(y, K, u1, u2);
+    labels[pt] = alias_draw_y(y, is_small, K, u1, u2);
+}
+
+// ------------------------------------------------------------------------- sub-label kernel
+// Sub-cluster labels of the points of one chunk (one cluster, in label order; cudaKernel.cu
+// create_subclusters_labels, :1299-1398): per tile of 128 points the A operand (split BF16,
+// swizzled) is built in shared memory from the gathered rows, and 12 tcgen05.mma against the
+// cluster's B tile [W_l | W_r] give z for both sub-clusters.  8 warps drain
+// r_s = c_s - |z_s - b_s|^2 / 2 (warp w: lane quarter w % 4, side w / 4); one thread per point then
+// adds log lr_weights, normalises and draws with the two-category alias (cudaKernel.cu:352-372).
+// Every wait is bounded and decided block-uniformly.
+struct SubSmem {
+    static constexpr size_t b = 0;                        // 32 KB B tile (hi, lo)
+    static constexpr size_t a = STAGE_BYTES;              // 32 KB A tile (hi, lo)
+    static constexpr size_t q = a + A_TILE;               // r of both sides [2][BM] floats
+    static constexpr size_t bias = q + 2 * BM * 4;        // b_l, b_r [2][KD] floats
+    static constexpr size_t bar = bias + 2 * KD * 4;      // mbarrier, tmem slot, flag
+    static constexpr size_t total = bar + 32 + 1024;      // + alignment slack
+};
+
+template <int DP>
+__global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const uint8_t* __restrict__ Bsub, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, const float* __restrict__ lrw, RngArgs rng, int32_t* __restrict__ sub,
+    float* __restrict__ r_out, int32_t* __restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sB = smem + SubSmem::b;
+    uint8_t* sA = smem + SubSmem::a;
+    float* sq = reinterpret_cast<float*>(smem + SubSmem::q);
+    float* sbias = reinterpret_cast<float*>(smem + SubSmem::bias);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + SubSmem::bar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+
+    // B tile of cluster k and the two sub-cluster biases
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(Bsub + (size_t)k * STAGE_BYTES);
+        uint4* dst = reinterpret_cast<uint4*>(sB);
+        for (int e = tid; e < STAGE_BYTES / 16; e += 256) dst[e] = src[e];
+        if (tid < 2 * KD) {
+            const int side = tid / KD, j = tid % KD;
+            sbias[tid] = j < DP ? bvec[(size_t)(3 * k + 1 + side) * DP + j] : 0.f;
+        }
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"((uint32_t)BN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const float cl = cvec[3 * k + 1], cr = cvec[3 * k + 2];
+    const float wl = lrw[2 * k], wr = lrw[2 * k + 1];
+
+    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8)
+    float4 pf[4][2];
+    auto load_rows = [&](int t0) {
+        const int ntn = min(BM, len - t0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pf[u][1] = pf[u][0];
+            if (row < ntn && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + row) * DP + c8 * 8);
+                pf[u][0] = __ldg(src);
+                pf[u][1] = __ldg(src + 1);
+            }
+        }
+    };
+    load_rows(0);
+    uint32_t phase = 0;
+    bool failed = false;
+    const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
+    const uint64_t db_h = sw128_desc(smem_u32(sB)), db_l = sw128_desc(smem_u32(sB + B_BYTES));
+    for (int t0 = 0; t0 < len && !failed; t0 += BM) {
+        const int nt = min(BM, len - t0);
+        // A tile: split BF16, 128-byte swizzle
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            const float v[8] = {pf[u][0].x, pf[u][0].y, pf[u][0].z, pf[u][0].w,
+                                pf[u][1].x, pf[u][1].y, pf[u][1].z, pf[u][1].w};
+            __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) bf16_split(v[q], hi[q], lo[q]);
+            const uint32_t off = sw128_offset(row, c8 * 8);
+            *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(hi);
+            *reinterpret_cast<uint4*>(sA + A_BYTES + off) = *reinterpret_cast<const uint4*>(lo);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+#pragma unroll
+            for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(tmem_base, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
+#pragma unroll
+            for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(tmem_base, da_l + 2 * ks, db_h + 2 * ks, 1u);
+#pragma unroll
+            for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(tmem_base, da_h + 2 * ks, db_l + 2 * ks, 1u);
+            umma_commit(bar);
+        }
+        if (t0 + BM < len) load_rows(t0 + BM);   // the next tile's rows load while the MMAs run
+        if (tid == 0) {
+            if (!mbar_wait_bounded(bar, phase & 1, gerr)) {
+                atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+                *flag = 1;
+            }
+        }
+        ++phase;
+        __syncthreads();
+        if (*flag) { failed = true; break; }
+        tc_fence_after();
+        {
+            const int quarter = warp & 3, side = warp >> 2;
+            const uint32_t lane_addr = (uint32_t)(quarter * 32) << 16;
+            const float* bs = sbias + side * KD;
+            float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (h == 1 && DP <= 32) break;   // columns past DP are zero
+                uint32_t v[32];
+                tmem_ld32(tmem_base + lane_addr + (uint32_t)(side * KD + 32 * h), v);
+#pragma unroll
+                for (int j4 = 0; j4 < 8; ++j4) {
+                    const float4 b4 = *reinterpret_cast<const float4*>(bs + 32 * h + 4 * j4);
+                    const float z0 = __uint_as_float(v[4 * j4 + 0]) - b4.x;
+                    const float z1 = __uint_as_float(v[4 * j4 + 1]) - b4.y;
+                    const float z2 = __uint_as_float(v[4 * j4 + 2]) - b4.z;
+                    const float z3 = __uint_as_float(v[4 * j4 + 3]) - b4.w;
+                    q0 = fmaf(z0, z0, q0);
+                    q1 = fmaf(z1, z1, q1);
+                    q2 = fmaf(z2, z2, q2);
+                    q3 = fmaf(z3, z3, q3);
+                }
+            }
+            sq[side * BM + quarter * 32 + lane] = (side ? cr : cl) - 0.5f * ((q0 + q1) + (q2 + q3));
+        }
+        tc_fence_before();
+        __syncthreads();
+        if (tid < nt) {
+            const int64_t pt = perm[start + t0 + tid];
+            float rl = sq[tid], rr = sq[BM + tid];
+            if (r_out) { r_out[2 * pt] = rl; r_out[2 * pt + 1] = rr; }
+            rl += wl;
+            rr += wr;
+            const float mx = fmaxf(rl, rr);
+            const float el = __expf(rl - mx), er = __expf(rr - mx);
+            const float s = el + er;
+            float u1, u2;
+            draw_uniform2(rng, pt, u1, u2);
+            sub[pt] = alias_draw2(el / s, er / s, u1, u2);
+        }
+    }
+    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"((uint32_t)BN));
+    }
 }
 
 }  // namespace tc
@@ -648,8 +833,13 @@ dpmm_status pack_tc_params(dpmm_ctx* c, int K)
     if (!c->d_Btc || !(c->Dp == 32 || c->Dp == 64)) return DPMM_OK;
     const int NT = (K + tc::CPT - 1) / tc::CPT;
     const int total = NT * tc::BN * 8;
-    tc::k_pack_b<<<(total + 255) / 256, 256, 0, c->stream>>>(c->d_Wt, K, c->Dp, NT, c->d_Btc);
+    tc::k_pack_b<<<(total + 255) / 256, 256, 0, c->stream>>>(c->d_Wt, K, c->Dp, NT, 0, c->d_Btc);
     DPMM_LAUNCHED();
+    if (c->d_Bsub) {
+        const int ts = K * tc::BN * 8;
+        tc::k_pack_b<<<(ts + 255) / 256, 256, 0, c->stream>>>(c->d_Wt, K, c->Dp, K, 1, c->d_Bsub);
+        DPMM_LAUNCHED();
+    }
     const int nb = NT * (tc::BIAS_REC / 4);
     tc::k_pack_bias<<<(nb + 255) / 256, 256, 0, c->stream>>>(c->d_b, c->d_c, K, c->Dp, NT, tc_bias_base(c));
     DPMM_LAUNCHED();
@@ -693,6 +883,37 @@ dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float
     DPMM_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core label kernel: bounded wait expired (code " +
+                                                 std::to_string(h_err) + ")");
+    return DPMM_OK;
+}
+
+bool tc_sub_supported(const dpmm_ctx* c)
+{
+    return c->prior == DPMM_PRIOR_GAUSSIAN && c->d_Bsub != nullptr && (c->Dp == 32 || c->Dp == 64) &&
+           c->ll_mode != DPMM_LL_FP32;
+}
+
+template <int DP>
+static dpmm_status launch_sub_labels_tc_t(dpmm_ctx* c, RngArgs r, float* d_rout, int32_t* err)
+{
+    auto kern = tc::k_sub_labels_tc<DP>;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SubSmem::total));
+    kern<<<c->max_chunks, 256, tc::SubSmem::total, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Bsub,
+                                                              c->d_b, c->d_c, c->d_lrw, r, c->d_sub, d_rout, err);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout)
+{
+    int32_t* err = c->d_aux + 5;
+    DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
+    if (c->Dp == 64) DPMM_TRY(launch_sub_labels_tc_t<64>(c, r, d_rout, err));
+    else DPMM_TRY(launch_sub_labels_tc_t<32>(c, r, d_rout, err));
+    int32_t h_err = 0;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core sub-label kernel: bounded wait expired (code " +
                                                  std::to_string(h_err) + ")");
     return DPMM_OK;
 }

@@ -219,6 +219,43 @@ def test_gaussian_sub_labels_and_stats_parity(D, K, N):
     np.testing.assert_allclose(S, S_o, atol=1e-6 * (np.abs(S_o).max() + 1), rtol=1e-6)
 
 
+@pytest.mark.parametrize("D,K,N", [(32, 5, 20000), (48, 7, 15000), (64, 6, 25000)])
+def test_gaussian_sub_labels_tensor_core_parity(D, K, N):
+    """Sub-labels on the tensor cores (split-BF16 contraction against each cluster's two
+    sub-cluster factors, several 128-point tiles per chunk and several chunks per cluster):
+    r within 2e-4 relative of FP64, draws exact against the oracle on the GPU's own r except at
+    margins below 1e-4, statistics of the drawn sub-labels exact / within 1e-6."""
+    from dpmmsubclusters_gpu_b200 import LL_TC_BF16X3
+    rng = np.random.default_rng(57 * D + K)
+    x, z, mu, inv, logdet, w, mu_lr, inv_lr, ld_lr, lrw = _gauss_sub_setup(rng, N, D, K)
+    x = x + 2.0
+    mu = mu + 2.0
+    mu_lr = mu_lr + 2.0
+    ck = CudaKernel(prior_type.Gaussian, loglik_mode=LL_TC_BF16X3, k_max=64).init(N, x, 11, points_major=True)
+    ck.set_gaussian_params(mu, inv, logdet, w, mu_lr, inv_lr, ld_lr, lrw)
+    labels = (z + 1).astype(np.int32)
+    ck.set_labels(labels)
+    u = uniforms(2 * N, 91)
+    r = ck.create_subclusters_labels(K, uniforms=u, return_loglik=True).astype(np.float64)
+    sub = ck.get_sub_labels()
+    _, _, r64 = O.gauss_sub_labels(x, labels, mu_lr, inv_lr, ld_lr, lrw, u.astype(np.float64))
+    rf = r - D * D * LOG2PI / 2
+    assert (np.abs(rf - r64) / np.maximum(np.abs(r64), 32)).max() <= 2e-4
+    u2 = u.reshape(N, 2).astype(np.float64)
+    sub_o = np.empty(N, np.int32)
+    mg = np.empty(N)
+    for k in range(K):
+        idx = np.where(labels == k + 1)[0]
+        s, m = O.sample_sub_from_loglik(r[idx], lrw[k], u2[idx])
+        sub_o[idx], mg[idx] = s, m
+    _mismatch_ok(sub, sub_o, mg)
+    cnt, sm, S = ck.create_sufficient_statistics(np.arange(K))
+    cnt_o, sm_o, S_o = O.suff_stats(x, labels, sub, K)
+    np.testing.assert_array_equal(cnt, cnt_o)
+    np.testing.assert_allclose(sm, sm_o, atol=1e-6 * (np.abs(sm_o).max() + 1) * 10, rtol=1e-6)
+    np.testing.assert_allclose(S, S_o, atol=1e-6 * (np.abs(S_o).max() + 1), rtol=1e-6)
+
+
 @pytest.mark.parametrize("D,K,N", [(20, 3, 8000), (1000, 6, 3000)])
 def test_multinomial_sub_labels_and_stats_parity(D, K, N):
     rng = np.random.default_rng(D)
