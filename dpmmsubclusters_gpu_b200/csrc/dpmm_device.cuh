@@ -358,6 +358,16 @@ __device__ __forceinline__ int alias_draw_y(const YF& y, const SF& is_small, int
             sm.w[j] = m;
             ns += __popc(m);
         }
+        if (ns == K - 1) {
+            // One large L: it absorbs every small's deficit (its excess equals their total up to
+            // rounding, well below 1e-3), so a drawn small with y < 0.999 is aliased to L wherever it
+            // sits in the consumption order.  Otherwise (col = L, or y near 1) walk the merge.
+            const int col = alias_column(K, u1);
+            if (sm.small(col)) {
+                const float yc = y(col - 1);
+                if (yc < 0.999f) return yc < u2 ? sm.prev_large_before(K + 1) : col;
+            }
+        }
         return alias_merge(y, K, ns, sm, u1, u2);
     }
     int ns = 0;

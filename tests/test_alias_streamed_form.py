@@ -16,6 +16,8 @@ def alias_stream(y, u1, u2):
     ns = int(np.count_nonzero(y < 1.0))
     col = min(max(int(u1 * (K - 1 + 0.999999) + 1), 1), K)
     yc = y[col - 1]
+    if ns == K - 1 and yc < 0.999:     # one large absorbs every small (alias_draw_y)
+        return int(np.flatnonzero(y >= 1.0)[0]) + 1 if yc < u2 else col
     if yc == 1.0:
         return col
     st = {"P": ns + 1, "sr": ns, "Q": ns, "ll": ns + 1, "D": 0.0, "C": 0.0, "Ccol": 0.0}
