@@ -835,6 +835,193 @@ __global__ void __launch_bounds__(256, (DP >= 128 ? 1 : 2)) k_gauss_sub_stats(
     }
 }
 
+// Statistics only (the sub-labels are given), DP <= 64: one pass per sub-cluster over the
+// chunk.  Per tile the points of the pass's sub-cluster are compacted into a list (warp
+// ballots), so the accumulation loop has no per-point branch; each thread of a warp-aligned
+// group owns a 4 x 4 block of the upper triangle (and the diagonal blocks the sums), adds FP32
+// runs of at most 33 points into FP64 totals held in registers, and the groups' totals meet in
+// shared memory once per pass.  Same partial records as k_gauss_sub_stats.
+template <int DP>
+struct SlotStatsShape {
+    static constexpr int TP = 128;
+    static constexpr int SX = DP + 4;
+    static constexpr int NB = DP / 4;
+    static constexpr int NBLK = NB * (NB + 1) / 2;
+    static constexpr int GS = (NBLK + 31) / 32 * 32;
+    static constexpr int G = 256 / GS;
+    static constexpr int NTOT = G * NBLK;
+    static constexpr size_t off_s = 0;                                           // DP floats (shift)
+    static constexpr size_t off_x = (off_s + sizeof(float) * DP + 15) / 16 * 16; // TP x SX floats
+    static constexpr size_t off_list = off_x + sizeof(float) * TP * SX;          // TP ints
+    static constexpr size_t off_wc = off_list + sizeof(int32_t) * TP;             // 8 warp counts
+    static constexpr size_t off_tot = (off_wc + sizeof(int32_t) * 8 + 15) / 16 * 16;   // [20][NTOT] doubles
+    static constexpr size_t bytes = off_tot + sizeof(double) * 20 * NTOT;
+};
+
+template <int DP>
+__global__ void __launch_bounds__(256, 2) k_gauss_slot_stats(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const float* __restrict__ muv, const int32_t* __restrict__ sub,
+    double* __restrict__ part, const uint8_t* __restrict__ mask)
+{
+    using S = SlotStatsShape<DP>;
+    constexpr int T = tri(DP);
+    constexpr int SL = 1 + DP + T;
+    constexpr int TP = S::TP, SX = S::SX;
+    constexpr int NV = TP * DP / 4;
+    constexpr int NPF = (NV + 255) / 256;
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* ss = reinterpret_cast<float*>(smem + S::off_s);
+    float* sx = reinterpret_cast<float*>(smem + S::off_x);
+    int32_t* slist = reinterpret_cast<int32_t*>(smem + S::off_list);
+    int32_t* swc = reinterpret_cast<int32_t*>(smem + S::off_wc);
+    double* stot = reinterpret_cast<double*>(smem + S::off_tot);
+
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    if (mask && !mask[k]) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    for (int e = tid; e < DP; e += 256) ss[e] = muv[(size_t)(3 * k) * DP + e];
+
+    const int grp = tid / S::GS, tb = tid % S::GS;
+    const bool has_blk = grp < S::G && tb < S::NBLK;
+    int bi = 0, bj = 0;
+    if (has_blk) {
+        int rem = tb;
+        while (rem >= S::NB - bi) { rem -= S::NB - bi; ++bi; }
+        bj = bi + rem;
+    }
+    const bool diag = has_blk && bi == bj;
+    const int tcol = grp * S::NBLK + tb;
+    double* out = part + (size_t)ch * 2 * SL;
+
+    float4 pf[NPF];
+    int pfs = 0;   // this thread's point's sub-label (threads < TP)
+    auto load_tile = [&](int t0) {
+        const int ntn = min(TP, len - t0);
+#pragma unroll
+        for (int u = 0; u < NPF; ++u) {
+            const int e = tid + 256 * u;
+            const int pp = e / (DP / 4), i4 = e % (DP / 4);
+            pf[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (e < NV && pp < ntn)
+                pf[u] = __ldg(reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + pp) * DP) + i4);
+        }
+        pfs = tid < ntn ? __ldg(sub + __ldg(perm + start + t0 + tid)) : 0;
+    };
+
+    for (int slot = 1; slot <= 2; ++slot) {
+        float bf[16], sf[4];
+        double bd[16], sd[4];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) { bf[m] = 0.f; bd[m] = 0.0; }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { sf[m] = 0.f; sd[m] = 0.0; }
+        auto flush = [&]() {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) { bd[m] += (double)bf[m]; bf[m] = 0.f; }
+#pragma unroll
+            for (int m = 0; m < 4; ++m) { sd[m] += (double)sf[m]; sf[m] = 0.f; }
+        };
+        int cnt = 0;
+        __syncthreads();   // ss written / the previous pass's totals read
+        load_tile(0);
+        for (int t0 = 0; t0 < len; t0 += TP) {
+            const int nt = min(TP, len - t0);
+            __syncthreads();   // the previous tile's list and rows are no longer read
+#pragma unroll
+            for (int u = 0; u < NPF; ++u) {
+                const int e = tid + 256 * u;
+                if (e < NV) {
+                    const int pp = e / (DP / 4), i4 = e % (DP / 4);
+                    const float4 sv4 = *reinterpret_cast<const float4*>(ss + 4 * i4);
+                    float4 v = pf[u];
+                    if (pp < nt) { v.x -= sv4.x; v.y -= sv4.y; v.z -= sv4.z; v.w -= sv4.w; }
+                    *reinterpret_cast<float4*>(sx + pp * SX + 4 * i4) = v;
+                }
+            }
+            // list of this tile's points in the pass's sub-cluster, in order
+            const bool in = tid < nt && pfs == slot;
+            const unsigned bal = __ballot_sync(0xffffffffu, in);
+            if (lane == 0 && warp < TP / 32) swc[warp] = __popc(bal);
+            __syncthreads();
+            int off = 0, n_in = 0;
+#pragma unroll
+            for (int w = 0; w < TP / 32; ++w) {
+                const int c = swc[w];
+                off += w < warp ? c : 0;
+                n_in += c;
+            }
+            if (in) slist[off + __popc(bal & ((1u << lane) - 1u))] = tid;
+            __syncthreads();
+            cnt += n_in;
+            if (t0 + TP < len) load_tile(t0 + TP);   // the next tile loads during the accumulation
+            if (has_blk) {
+                auto acc = [&](const float4 xi, const float4 xj) {
+                    const float vi[4] = {xi.x, xi.y, xi.z, xi.w};
+                    const float vj[4] = {xj.x, xj.y, xj.z, xj.w};
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int c = 0; c < 4; ++c) bf[4 * a + c] = fmaf(vi[a], vj[c], bf[4 * a + c]);
+                    if (diag) {
+#pragma unroll
+                        for (int a = 0; a < 4; ++a) sf[a] += vi[a];
+                    }
+                };
+                // two points per iteration: both points' loads are in flight together
+                int run = 0, q = grp;
+                for (; q + S::G < n_in; q += 2 * S::G) {
+                    const float* xa = sx + slist[q] * SX;
+                    const float* xb = sx + slist[q + S::G] * SX;
+                    const float4 xia = *reinterpret_cast<const float4*>(xa + 4 * bi);
+                    const float4 xja = *reinterpret_cast<const float4*>(xa + 4 * bj);
+                    const float4 xib = *reinterpret_cast<const float4*>(xb + 4 * bi);
+                    const float4 xjb = *reinterpret_cast<const float4*>(xb + 4 * bj);
+                    acc(xia, xja);
+                    acc(xib, xjb);
+                    run += 2;
+                    if (run >= 32) { flush(); run = 0; }   // FP32 runs of at most 33 points
+                }
+                if (q < n_in) {
+                    const float* xa = sx + slist[q] * SX;
+                    acc(*reinterpret_cast<const float4*>(xa + 4 * bi), *reinterpret_cast<const float4*>(xa + 4 * bj));
+                }
+                flush();
+            }
+        }
+        // the groups' totals meet in shared memory; thread b < NBLK writes block b
+        if (has_blk) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m) stot[m * S::NTOT + tcol] = bd[m];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) stot[(16 + m) * S::NTOT + tcol] = sd[m];
+        }
+        __syncthreads();
+        double* po = out + (size_t)(slot - 1) * SL;
+        if (tid == 0) po[0] = (double)cnt;
+        if (tid < S::NBLK) {
+            int ri = 0, rem = tid;
+            while (rem >= S::NB - ri) { rem -= S::NB - ri; ++ri; }
+            const int rj = ri + rem;
+            for (int m = 0; m < 16; ++m) {
+                const int i = 4 * ri + (m >> 2), j = 4 * rj + (m & 3);
+                if (i > j) continue;
+                double v = 0.0;
+                for (int g = 0; g < S::G; ++g) v += stot[m * S::NTOT + g * S::NBLK + tid];
+                po[1 + DP + tri_index(DP, i, j)] = v;
+            }
+            if (ri == rj)
+                for (int a = 0; a < 4; ++a) {
+                    double v = 0.0;
+                    for (int g = 0; g < S::G; ++g) v += stot[(16 + a) * S::NTOT + g * S::NBLK + tid];
+                    po[1 + 4 * ri + a] = v;
+                }
+        }
+    }
+}
+
 // Multinomial: warp per point; sub-label from two dot products with log theta_l / log theta_r,
 // count sums accumulated with shared-memory float atomics (exact for integer counts while a
 // chunk's per-category sum stays below 2^24).
@@ -911,6 +1098,17 @@ __global__ void __launch_bounds__(256) k_mult_sub_stats(
 template <int DP>
 static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout, const uint8_t* d_mask)
 {
+    if constexpr (DP <= 64) {
+        if (!draw) {
+            const size_t sm = SlotStatsShape<DP>::bytes;
+            auto kern = k_gauss_slot_stats<DP>;
+            DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu,
+                                                        c->d_sub, c->d_part, d_mask);
+            DPMM_LAUNCHED();
+            return DPMM_OK;
+        }
+    }
     const size_t sm = SubStatsShape<DP>::bytes;
     auto kern = k_gauss_sub_stats<DP>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
