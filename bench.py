@@ -191,7 +191,7 @@ def cpu_sample_payload(x_np, n, seed, K, D):
     return (x, mu, inv, logdet, w, u, mu_lr, inv_lr, ld_lr, lrw)
 
 
-def cpu_baseline(x_np, K, D, n=4000):
+def cpu_baseline(x_np, K, D, n=60000):
     t = _cpu_sample_worker(cpu_sample_payload(x_np, n, 1, K, D))
     return {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
             "sample": f"{n} points x 1 iteration of the per-point phases (K={K}, D={D}) through the FP64 C "
@@ -393,7 +393,7 @@ def main():
     if rank == 0 and not args.no_cpu:
         import numpy as np2
         rng = np2.random.default_rng(0)
-        xs = (rng.normal(size=(4000, D)) * 5).astype(np2.float32)
+        xs = (rng.normal(size=(60000, D)) * 5).astype(np2.float32)
         line["cpu_baseline"] = cpu_baseline(xs, cfg["K_true"], D)
     if not args.no_e2e:
         line["e2e"] = run_e2e(args, cfg, rank, local, world, dist, L, make_run)
