@@ -10,11 +10,11 @@
 // into a shared-memory table, and finishes with the softmax + Walker alias draw (or argmax)
 // of the reference (cudaKernel.cu:374-424, 27-124) in a second kernel, one thread per point.
 //
-// CTA roles (576 threads, persistent over 256-point super-tiles): warp 0 streams the A tiles
+// CTA roles (608 threads, persistent over 256-point super-tiles): warp 0 streams the A tiles
 // (points, packed at upload) and the B tiles (2 clusters = 128 columns, hi + lo, 32 KB, stored
-// pre-swizzled) with cp.async.bulk; warp 1 allocates TMEM and issues tcgen05.mma (M=128, N=128,
-// K=16; 2 x 12 per N tile, one set per 128-point half) into 2 accumulator pairs; warps 2-17 drain
-// the accumulators into r.
+// pre-swizzled) with cp.async.bulk; warp 1 allocates TMEM; warps 1-2 each issue the 12
+// tcgen05.mma (M=128, N=128, K=16) of one 128-point half per N tile into 2 accumulator pairs;
+// warps 3-18 drain the accumulators into r.
 // Every mbarrier wait is bounded: on timeout the CTA records an error code, stops issuing work,
 // drains what it issued (bounded) and frees its TMEM.
 //
@@ -46,9 +46,10 @@ constexpr int A_SLOT = HALVES * 2 * A_BYTES;   // 64 KB: tile 0 hi, lo, tile 1 h
 constexpr int MAX_BSTAGES = 4;
 constexpr int BIAS_REC = 528;              // per N tile: b (2 x 64 floats), c (2 floats), pad
 constexpr int BIAS_SLOTS = 8;              // bias ring depth
+constexpr int MMA_WARPS = 2;               // one MMA issuer per 128-point half
 constexpr int DRAIN_WARPS = 16;            // (lane quarter, cluster of the N tile, half)
-constexpr int WARP_DRAIN0 = 2;
-constexpr int THREADS = 32 * (2 + DRAIN_WARPS);
+constexpr int WARP_MMA0 = 1, WARP_DRAIN0 = WARP_MMA0 + MMA_WARPS;
+constexpr int THREADS = 32 * (1 + MMA_WARPS + DRAIN_WARPS);
 
 enum : int {
     ERR_TIMEOUT_FULL = 1, ERR_TIMEOUT_EMPTY = 2, ERR_TIMEOUT_TFULL = 3, ERR_TIMEOUT_TEMPTY = 4,
@@ -297,8 +298,8 @@ __global__ void k_pack_a(const float* __restrict__ x, int64_t N, int Dp, int64_t
 //
 //   warp 0      producer: A super-tile (64 KB, with an L2 prefetch of the next one), B tiles
 //               (32 KB) into a B ring, bias records into a bias ring
-//   warp 1      MMA issuer: per N tile 2 x 12 tcgen05.mma into accumulator pair g % 2
-//   warps 2-17  drain: TMEM accumulator -> r = c - |z|^2 / 2 for one (lane quarter, cluster,
+//   warps 1-2   MMA issuers: per N tile 12 tcgen05.mma each (one per half) into pair g % 2
+//   warps 3-18  drain: TMEM accumulator -> r = c - |z|^2 / 2 for one (lane quarter, cluster,
 //               half) per warp, written cluster-major to rbuf[k][point] (32 points per store),
 //               with a running max / sum of exp (or the first maximum, final mode) per point and
 //               cluster parity, written to part at the end of the super-tile
@@ -365,12 +366,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
         *abort_flag = *gerr ? 1 : 0;
         for (int s = 0; s < bstages; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty[s], MMA_WARPS);
         }
         mbar_init(afull, 1);
-        mbar_init(aempty, 1);
+        mbar_init(aempty, MMA_WARPS);
         for (int t = 0; t < NPAIR; ++t) {
-            mbar_init(&tfull[t], 1);
+            mbar_init(&tfull[t], MMA_WARPS);
             mbar_init(&tempty[t], DRAIN_WARPS);
         }
         for (int s = 0; s < BIAS_SLOTS; ++s) {
@@ -440,16 +441,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
             for (int q = gb > BIAS_SLOTS ? gb - BIAS_SLOTS : 0; q < gb; ++q)
                 mbar_wait_bounded(&bfull[q % BIAS_SLOTS], (q / BIAS_SLOTS) & 1, nullptr);
         }
-    } else if (warp == 1) {
-        // ---------------- MMA issuer
+    } else if (warp < WARP_DRAIN0) {
+        // ---------------- MMA issuers: warp WARP_MMA0 + h issues the half-h MMAs of every N tile
+        // into accumulator 2t + h and commits to the shared barriers (count MMA_WARPS); while one
+        // issuer waits or commits, the other's MMAs keep the tensor pipe fed
         if (lane == 0) {
+            const int h = warp - WARP_MMA0;
             int g = 0, la = 0, issued = 0;
-            uint64_t dah[HALVES], dal[HALVES];
-#pragma unroll
-            for (int h = 0; h < HALVES; ++h) {
-                dah[h] = sw128_desc(smem_u32(sA + (size_t)h * A_TILE));
-                dal[h] = sw128_desc(smem_u32(sA + (size_t)h * A_TILE + A_BYTES));
-            }
+            const uint64_t dah = sw128_desc(smem_u32(sA + (size_t)h * A_TILE));
+            const uint64_t dal = sw128_desc(smem_u32(sA + (size_t)h * A_TILE + A_BYTES));
             for (int st = blockIdx.x; st < nst && !*abort_flag; st += gridDim.x, ++la) {
                 if (!mbar_wait_bounded(afull, la & 1, gerr)) {
                     atomicCAS(err, 0, ERR_TIMEOUT_AFULL);
@@ -473,17 +473,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
                     const uint32_t b_hi = smem_u32(sB + (size_t)s * STAGE_BYTES), b_lo = b_hi + B_BYTES;
                     // descriptors: a K step of 16 elements (32 bytes) adds 2 to the start-address field
                     const uint64_t dbh = sw128_desc(b_hi), dbl = sw128_desc(b_lo);
+                    const uint32_t d = tmem_base + (uint32_t)((HALVES * t + h) * BN);
 #pragma unroll
-                    for (int h = 0; h < HALVES; ++h) {
-                        const uint32_t d = tmem_base + (uint32_t)((HALVES * t + h) * BN);
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(d, dah + 2 * ks, dbh + 2 * ks, ks != 0 ? 1u : 0u);
 #pragma unroll
-                        for (int ks = 0; ks < KD / 16; ++ks)
-                            umma_bf16(d, dah[h] + 2 * ks, dbh + 2 * ks, ks != 0 ? 1u : 0u);
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(d, dal + 2 * ks, dbh + 2 * ks, 1u);
 #pragma unroll
-                        for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(d, dal[h] + 2 * ks, dbh + 2 * ks, 1u);
-#pragma unroll
-                        for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(d, dah[h] + 2 * ks, dbl + 2 * ks, 1u);
-                    }
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(d, dah + 2 * ks, dbl + 2 * ks, 1u);
                     umma_commit(&empty[s]);
                     umma_commit(&tfull[t]);
                     issued = g + 1;
@@ -494,7 +490,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
                     break;
                 }
             }
-            // drain: the last MMAs issued have completed before TMEM is freed
+            // drain: the last MMAs issued have completed before TMEM is freed (the phase completes
+            // once both issuers' commits have arrived; bounded if the other one stopped early)
             if (issued > 0) mbar_wait_bounded(&tfull[(issued - 1) % NPAIR], ((issued - 1) / NPAIR) & 1, nullptr);
         }
     } else {
