@@ -33,13 +33,6 @@ __device__ double block_sum(double v, double* red)
     return red[32];
 }
 
-__device__ double log_multivariate_gamma_d(double x, int D)
-{
-    double res = D * (D - 1) / 4.0 * log(M_PI);
-    for (int d = 1; d <= D; ++d) res += lgamma(x + (1 - d) / 2.0);
-    return res;
-}
-
 // In-place Cholesky of the lower triangle of A (D x D, column-major, shared memory);
 // returns log det A, or NaN when A is not positive definite.
 __device__ double chol_logdet(double* A, int D, double* red)
@@ -57,11 +50,13 @@ __device__ double chol_logdet(double* A, int D, double* red)
         const double djj = A[(size_t)j * D + j];
         for (int i = j + 1 + threadIdx.x; i < D; i += blockDim.x) A[(size_t)j * D + i] /= djj;
         __syncthreads();
-        // trailing update of the lower triangle: A(i,k) -= L(i,j) L(k,j), j < k <= i
-        const int m = D - j - 1;
-        for (int e = threadIdx.x; e < m * m; e += blockDim.x) {
-            int kk = j + 1 + e / m, ii = j + 1 + e % m;
-            if (ii >= kk) A[(size_t)kk * D + ii] -= A[(size_t)j * D + ii] * A[(size_t)j * D + kk];
+        // trailing update of the lower triangle: A(i,k) -= L(i,j) L(k,j), j < k <= i; one column
+        // k per thread, walking its rows (no index division)
+        const double* cj = A + (size_t)j * D;
+        for (int kk = j + 1 + threadIdx.x; kk < D; kk += blockDim.x) {
+            const double lkj = cj[kk];
+            double* ck = A + (size_t)kk * D;
+            for (int ii = kk; ii < D; ++ii) ck[ii] -= cj[ii] * lkj;
         }
         __syncthreads();
     }
@@ -93,8 +88,13 @@ __device__ double niw_lml_from_stats(int D, double n, const double* sum, const d
     __syncthreads();
     const double ldp = chol_logdet(psi, D, red);
     const double logpi = log(M_PI);
-    return -n * D * 0.5 * logpi + log_multivariate_gamma_d(vp / 2.0, D) - log_multivariate_gamma_d(v0 / 2.0, D) +
-           (v0 / 2.0) * (D * log(v0) + ld0) - (vp / 2.0) * (D * log(vp) + ldp) + (D / 2.0) * (log(k0 / kp));
+    // log Gamma_D(vp / 2) - log Gamma_D(v0 / 2): the D(D-1)/4 log(pi) terms cancel; one lgamma
+    // pair per thread, then a block sum
+    double g = 0.0;
+    for (int d = 1 + threadIdx.x; d <= D; d += blockDim.x) g += lgamma(vp / 2.0 + (1 - d) / 2.0) - lgamma(v0 / 2.0 + (1 - d) / 2.0);
+    g = block_sum(g, red);
+    return -n * D * 0.5 * logpi + g + (v0 / 2.0) * (D * log(v0) + ld0) - (vp / 2.0) * (D * log(vp) + ldp) +
+           (D / 2.0) * (log(k0 / kp));
 }
 
 // Dirichlet-multinomial log marginal likelihood of statistics (n, sum)
