@@ -250,6 +250,8 @@ def main():
     ap.add_argument("--d", type=int, default=64)
     ap.add_argument("--k-true", type=int, default=100)
     ap.add_argument("--mode", default="auto", choices=["auto", "fp32", "tc"])
+    ap.add_argument("--screen", default="on", choices=["on", "off"],
+                    help="learned split/merge screen (exact ratios for the top 16 candidates of each kind)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-points-per-core", type=int, default=600)
@@ -280,6 +282,10 @@ def main():
     torch.cuda.synchronize()
 
     mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[args.mode]
+    screen_params = None
+    if args.screen == "on":
+        from dpmmsubclusters_gpu_b200.screen import load_params
+        screen_params = load_params()
 
     def make_run(iterations):
         rd = capi.dpmm_run_desc()
@@ -298,7 +304,10 @@ def main():
         rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
         rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        return rd, (m, psi)
+        if screen_params is not None:
+            rd.screen_mode = capi.SCREEN_ON
+            rd.screen_params = screen_params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        return rd, (m, psi, screen_params)
 
     rd, keep = make_run(cfg["iterations"])
     h = ctypes.c_void_p()
@@ -347,6 +356,8 @@ def main():
     mi = ctypes.c_void_p()
     check(L.dpmm_sampler_model_info(h, ctypes.byref(mi)))
     lab = np.ctypeslib.as_array(L.dpmm_model_info_labels(mi), shape=(N,)).copy()
+    scr = np.zeros(8, np.int64)
+    check(L.dpmm_model_info_screen_stats(mi, scr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
     L.dpmm_model_info_free(mi)
     check(L.dpmm_sampler_destroy(h))
     zt = z.cpu().numpy()
@@ -381,7 +392,8 @@ def main():
                        "N": N, "D": D, "initial_clusters": cfg["K_true"], "burnin_iterations": args.burnin,
                        "clusters_in_timed_steps": ks, "loglik_mode": args.mode,
                        "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
-                       "nmi_vs_generating_labels": nmi},
+                       "nmi_vs_generating_labels": nmi,
+                       "screen": screen_summary(args.screen, scr)},
             "gpu_launches": int(launches),
             "roofline": roofline,
             "phase_ms_per_step": {p: ph_ms[i] / args.steps for i, p in enumerate(phases) if ph_calls[i]},
@@ -442,6 +454,19 @@ def run_e2e(args, cfg, rank, local, world, dist, L, make_run):
             "iterations": iters, "wall_s": dt,
             "note": "dpmm_dp_parallel from host float64 points: upload, init, all iterations and label "
                     "download in the timed region"}
+
+
+def screen_summary(flag, st):
+    """counters of the learned split/merge screen over the whole run (burn-in included)"""
+    if flag != "on":
+        return {"enabled": False}
+    keys = ("split_candidates", "split_exact", "merge_candidates", "merge_exact", "sweeps", "sweep_accepts",
+            "sweep_hits", "disabled_at")
+    d = {k: int(v) for k, v in zip(keys, st)}
+    d["enabled"] = True
+    d["top"], d["sweep_every"], d["split_min_candidates"] = 16, 10, 256
+    d["sweep_recall"] = d["sweep_hits"] / d["sweep_accepts"] if d["sweep_accepts"] else None
+    return d
 
 
 def _nmi(a, b):

@@ -62,6 +62,10 @@ class ModelInfo:
         self.nmi_score_history = np.zeros(0)
         self.likelihood_history = np.zeros(0)
         self.cluster_count_history = np.zeros(0, np.int32)
+        # learned split/merge screen (no counterpart in the reference): counters and the log of
+        # DPMM_SCREEN_LOG runs (features (rows, 32), exact log ratios, kinds 0 split / 1 merge, iterations)
+        self.screen_stats = {}
+        self.screen_log = None
 
     @staticmethod
     def _from_handle(h) -> "ModelInfo":
@@ -80,6 +84,18 @@ class ModelInfo:
             p = L.dpmm_model_info_nmi_history(h)
             if p:
                 mi.nmi_score_history = np.ctypeslib.as_array(p, shape=(it,)).copy()
+        st = np.zeros(8, np.int64)
+        check(L.dpmm_model_info_screen_stats(h, st.ctypes.data_as(ctypes.POINTER(c_int64))))
+        keys = ("split_candidates", "split_exact", "merge_candidates", "merge_exact", "sweeps", "sweep_accepts",
+                "sweep_hits", "disabled_at")
+        mi.screen_stats = {k: int(v) for k, v in zip(keys, st)}
+        rows = L.dpmm_model_info_screen_log_rows(h)
+        if rows:
+            mi.screen_log = (
+                np.ctypeslib.as_array(L.dpmm_model_info_screen_log_features(h), shape=(rows, capi.SCREEN_FEATURES)).copy(),
+                np.ctypeslib.as_array(L.dpmm_model_info_screen_log_hr(h), shape=(rows,)).copy(),
+                np.ctypeslib.as_array(L.dpmm_model_info_screen_log_kind(h), shape=(rows,)).copy(),
+                np.ctypeslib.as_array(L.dpmm_model_info_screen_log_iter(h), shape=(rows,)).copy())
         return mi
 
 
@@ -110,9 +126,20 @@ class dp_parallel_sampling_class:
     dp_parallel_sampling_class(modelDataFileName (.npy, N x D), modelParamsFileName (JSON), priorType)."""
 
     def __init__(self, a, b, c=None, d=None, *, loglik_mode: int = capi.LL_AUTO, rng_kind: int = capi.RNG_PHILOX,
-                 k_max: int = 0, device: int = 0):
+                 k_max: int = 0, device: int = 0, screen_mode: int = capi.SCREEN_OFF, screen_params=None,
+                 screen_top: int = 16, screen_sweep_every: int = 10, screen_min_recall: float = 0.5,
+                 screen_split_min: int = 256):
+        """screen_*: the learned split/merge screen (no counterpart in the reference); screen_params
+        defaults to the trained parameters shipped with the package when screen_mode is SCREEN_ON."""
         self._from_file = isinstance(a, str)
         self.loglik_mode, self.rng_kind, self.k_max, self.device = loglik_mode, rng_kind, k_max, device
+        self.screen_mode, self.screen_top = screen_mode, screen_top
+        self.screen_sweep_every, self.screen_min_recall = screen_sweep_every, screen_min_recall
+        self.screen_split_min = screen_split_min
+        if screen_mode == capi.SCREEN_ON and screen_params is None:
+            from .screen import load_params
+            screen_params = load_params()
+        self.screen_params = None if screen_params is None else np.ascontiguousarray(screen_params, np.float32)
         if self._from_file:
             self.model_path, self.params_path = a, b
             self.prior = prior_type(c if c is not None else prior_type.Gaussian)
@@ -143,6 +170,7 @@ class dp_parallel_sampling_class:
         rd.rng_kind = self.rng_kind
         rd.k_max = self.k_max
         rd.device = self.device
+        self._put_screen(rd)
         keep = []
 
         def put(h, prefix):
@@ -173,6 +201,17 @@ class dp_parallel_sampling_class:
         finally:
             lib().dpmm_model_info_free(h)
 
+    def _put_screen(self, rd):
+        rd.screen_mode = self.screen_mode
+        rd.screen_top = self.screen_top
+        rd.screen_sweep_every = self.screen_sweep_every
+        rd.screen_min_recall = self.screen_min_recall
+        rd.screen_split_min = self.screen_split_min
+        if self.screen_params is not None:
+            if self.screen_params.size != capi.SCREEN_PARAMS:
+                raise ValueError(f"screen_params must hold {capi.SCREEN_PARAMS} values")
+            rd.screen_params = _fptr(self.screen_params)
+
     def dp_parallel_from_file(self, result_path: Optional[str] = None) -> ModelInfo:
         if not self._from_file:
             raise RuntimeError("dp_parallel_from_file needs the (npy, params, prior) constructor")
@@ -181,6 +220,7 @@ class dp_parallel_sampling_class:
         rd.rng_kind = self.rng_kind
         rd.k_max = self.k_max
         rd.device = self.device
+        self._put_screen(rd)
         h = c_void_p()
         check(lib().dpmm_dp_parallel_from_file(self.model_path.encode(), self.params_path.encode(), int(self.prior),
                                                byref(rd), byref(h)))
@@ -397,6 +437,47 @@ class CudaKernel:
         hr = np.empty(K * K)
         check(lib().dpmm_merge_hastings(self.ctx, K, alpha, _dptr(hr)))
         return hr.reshape(K, K)
+
+    # -------------------------------------------------------------- learned screen (no reference counterpart)
+    def screen_set_params(self, params):
+        p = np.ascontiguousarray(params, np.float32)
+        if p.size != capi.SCREEN_PARAMS:
+            raise ValueError(f"params must hold {capi.SCREEN_PARAMS} values")
+        check(lib().dpmm_screen_set_params(self.ctx, _fptr(p)))
+
+    @staticmethod
+    def _rows(K, kind):
+        return K * (K - 1) // 2 if kind == capi.SCREEN_MERGE else K
+
+    def screen_features(self, K: int, kind: int, alpha: float):
+        """-> features (rows, 32) float32, proxy log ratios (rows,)"""
+        rows = self._rows(K, kind)
+        f = np.empty((rows, capi.SCREEN_FEATURES), np.float32)
+        p = np.empty(rows)
+        check(lib().dpmm_screen_features(self.ctx, K, kind, alpha, _fptr(f), _dptr(p)))
+        return f, p
+
+    def screen_select(self, K: int, kind: int, alpha: float, eligible, top: int = 16):
+        """-> selected rows (ascending), scores of every row"""
+        e = np.ascontiguousarray(eligible, np.uint8)
+        sel = np.empty(capi.SCREEN_MAX_TOP, np.int32)
+        n = c_int32()
+        sc = np.empty(self._rows(K, kind), np.float32)
+        check(lib().dpmm_screen_select(self.ctx, K, kind, alpha, e.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), top,
+                                       _iptr(sel), byref(n), _fptr(sc)))
+        return sel[:n.value].copy(), sc
+
+    def split_hastings_list(self, K: int, alpha: float, clusters):
+        c = np.ascontiguousarray(clusters, np.int32)
+        out = np.empty(c.size)
+        check(lib().dpmm_split_hastings_list(self.ctx, K, alpha, c.size, _iptr(c), _dptr(out)))
+        return out
+
+    def merge_hastings_list(self, K: int, alpha: float, pairs):
+        pr = np.ascontiguousarray(pairs, np.int32).reshape(-1, 2)
+        out = np.empty(pr.shape[0])
+        check(lib().dpmm_merge_hastings_list(self.ctx, K, alpha, pr.shape[0], _iptr(pr), _dptr(out)))
+        return out
 
     def synchronize(self):
         check(lib().dpmm_synchronize(self.ctx))

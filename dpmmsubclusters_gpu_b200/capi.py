@@ -7,7 +7,8 @@ from __future__ import annotations
 
 import ctypes
 import os
-from ctypes import POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int32, c_int64, c_uint32, c_uint64, c_void_p
+from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int, c_int8, c_int32, c_int64, c_uint8,
+                    c_uint32, c_uint64, c_void_p)
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libdpmm_b200.so")
@@ -20,6 +21,9 @@ STATUS_NAMES = {0: "DPMM_OK", 1: "DPMM_ERR_INVALID_ARG", 2: "DPMM_ERR_OOM", 3: "
 PRIOR_GAUSSIAN, PRIOR_MULTINOMIAL = 0, 1
 RNG_PHILOX, RNG_CURAND_XORWOW = 0, 1
 LL_FP32, LL_TC_BF16X3, LL_AUTO = 0, 1, 2
+SCREEN_OFF, SCREEN_ON, SCREEN_LOG = 0, 1, 2
+SCREEN_SPLIT, SCREEN_MERGE = 0, 1
+SCREEN_FEATURES, SCREEN_HIDDEN, SCREEN_PARAMS, SCREEN_MAX_TOP = 32, 64, 6337, 256
 
 
 class DpmmError(RuntimeError):
@@ -44,7 +48,10 @@ class dpmm_run_desc(Structure):
                 ("loglik_mode", c_int32), ("rng_kind", c_int32), ("k_max", c_int32),
                 ("niw_k", c_double), ("niw_v", c_double), ("niw_m", _PD), ("niw_psi", _PD), ("mult_alpha", _PD),
                 ("out_niw_k", c_double), ("out_niw_v", c_double), ("out_niw_m", _PD), ("out_niw_psi", _PD),
-                ("out_mult_alpha", _PD), ("gt", POINTER(c_int32)), ("device", c_int32), ("reserved", c_int32 * 7)]
+                ("out_mult_alpha", _PD), ("gt", POINTER(c_int32)), ("device", c_int32),
+                ("screen_mode", c_int32), ("screen_top", c_int32), ("screen_sweep_every", c_int32),
+                ("screen_min_recall", c_float), ("screen_params", POINTER(c_float)), ("screen_split_min", c_int32),
+                ("reserved", c_int32 * 3)]
 
 
 # every symbol include/dpmm_capi.h declares, with its ctypes signature
@@ -112,6 +119,20 @@ SIGNATURES = {
     "dpmm_phase_times": (c_int, [_CTX, c_int, _PD, _PI64]),
     "dpmm_merge_hastings_static": (c_int, [c_int32, c_int32, c_int32, c_double, c_double, c_double, c_void_p,
                                            c_void_p, c_void_p, c_void_p]),
+    "dpmm_screen_set_params": (c_int, [_CTX, _PF]),
+    "dpmm_screen_features": (c_int, [_CTX, c_int, c_int, c_double, _PF, _PD]),
+    "dpmm_screen_select": (c_int, [_CTX, c_int, c_int, c_double, POINTER(c_uint8), c_int, _PI32, _PI32, _PF]),
+    "dpmm_split_hastings_list": (c_int, [_CTX, c_int, c_double, c_int, _PI32, _PD]),
+    "dpmm_merge_hastings_list": (c_int, [_CTX, c_int, c_double, c_int, _PI32, _PD]),
+    "dpmm_screen_forward": (c_int, [_PF, c_int64, _PF, _PF, c_int32]),
+    "dpmm_screen_loss_grad": (c_int, [_PF, _PF, c_int32, _PF, _PF, _PF, c_int32]),
+    "dpmm_screen_train": (c_int, [_PF, _PF, c_int64, c_int32, c_int32, c_float, c_uint64, _PF, _PF, c_int32]),
+    "dpmm_model_info_screen_stats": (c_int, [c_void_p, _PI64]),
+    "dpmm_model_info_screen_log_rows": (c_int64, [c_void_p]),
+    "dpmm_model_info_screen_log_features": (_PF, [c_void_p]),
+    "dpmm_model_info_screen_log_hr": (_PD, [c_void_p]),
+    "dpmm_model_info_screen_log_kind": (POINTER(c_int8), [c_void_p]),
+    "dpmm_model_info_screen_log_iter": (_PI32, [c_void_p]),
 }
 
 _lib = None

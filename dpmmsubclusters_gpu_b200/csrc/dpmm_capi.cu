@@ -148,7 +148,9 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_mu, c->d_perm, c->d_blk_hist, c->d_seg, c->d_chunk, c->d_nchunks, c->d_part, c->d_stats,
                     c->d_u, c->d_bits, c->d_remap, c->d_aux, c->d_r64, c->d_dbl_scratch, c->d_prior, c->d_lml,
                     c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc, c->d_rbuf,
-                    c->d_rpart, c->d_Bsub};
+                    c->d_rpart, c->d_Bsub, c->d_scr_rec, c->d_scr_vec, c->d_scr_linv, c->d_scr_feat,
+                    c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
+                    c->d_scr_list, c->d_scr_slots, c->d_scr_hr};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -262,6 +264,22 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     chk(dev_alloc(&c->d_split_hr, (size_t)KM));
     chk(dev_alloc(&c->d_merge_hr, (size_t)KM * KM));
     chk(dev_alloc(&c->d_post_logdet, (size_t)3 * KM));
+    {
+        const size_t rows = std::max<size_t>((size_t)KM, (size_t)KM * (KM - 1) / 2);
+        chk(dev_alloc(&c->d_scr_rec, (size_t)3 * KM * kScrRec));
+        chk(dev_alloc(&c->d_scr_vec, (size_t)3 * KM * 2 * c->D));
+        if (gauss) chk(dev_alloc(&c->d_scr_linv, (size_t)KM * c->D * c->D));
+        chk(dev_alloc(&c->d_scr_feat, rows * kScrF));
+        chk(dev_alloc(&c->d_scr_prox, rows));
+        chk(dev_alloc(&c->d_scr_score, rows));
+        chk(dev_alloc(&c->d_scr_w, (size_t)kScrParams));
+        chk(dev_alloc(&c->d_scr_wdep, (size_t)kScrParams));
+        chk(dev_alloc(&c->d_scr_elig, (size_t)KM));
+        chk(dev_alloc(&c->d_scr_sel, (size_t)kScrMaxTop + 1));
+        chk(dev_alloc(&c->d_scr_list, (size_t)2 * kScrMaxTop));
+        chk(dev_alloc(&c->d_scr_slots, (size_t)3 * kScrMaxTop));
+        chk(dev_alloc(&c->d_scr_hr, (size_t)kScrMaxTop));
+    }
     if (c->rng_kind == DPMM_RNG_CURAND_XORWOW) chk(dev_alloc(&c->d_curand, (size_t)N));
     if (st == DPMM_OK) {
         c->h_pinned_bytes = std::max({sizeof(double) * 3 * KM * (size_t)c->stat_len, sizeof(double) * (size_t)KM * KM,
@@ -878,6 +896,12 @@ extern "C" dpmm_status dpmm_set_prior_niw(dpmm_ctx* c, double k, const double* m
     std::vector<double> L;
     if (!la::cholesky(psi, D, L)) return fail(DPMM_ERR_NOT_PD, "prior psi is not positive definite");
     c->prior_logdet = la::logdet_from_chol(L, D);
+    c->prior_identity = true;
+    for (int j = 0; j < D && c->prior_identity; ++j) {
+        if (m[j] != 0.0) c->prior_identity = false;
+        for (int i = 0; i < D; ++i)
+            if (psi[(size_t)j * D + i] != (i == j ? 1.0 : 0.0)) c->prior_identity = false;
+    }
     c->prior_k = k;
     c->prior_v = v;
     std::vector<double> h((size_t)D + D * D);

@@ -24,6 +24,23 @@ constexpr int kMaxMultDim = 4096;
 constexpr int kChunkUnit = 1024;
 constexpr int kChunkMax = 4096;
 
+// Learned split/merge screen (dpmm_screen.cu): 32 features per candidate, a 32 -> 64 -> 64 -> 1 MLP
+// whose parameters are one FP32 vector W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3.
+constexpr int kScrF = 32;
+constexpr int kScrH = 64;
+constexpr int kScrOffW1 = 0;
+constexpr int kScrOffB1 = kScrOffW1 + kScrH * kScrF;
+constexpr int kScrOffW2 = kScrOffB1 + kScrH;
+constexpr int kScrOffB2 = kScrOffW2 + kScrH * kScrH;
+constexpr int kScrOffW3 = kScrOffB2 + kScrH;
+constexpr int kScrOffB3 = kScrOffW3 + kScrH;
+constexpr int kScrParams = kScrOffB3 + 1;
+constexpr int kScrRec = 10;         // FP64 values per statistics slot
+constexpr int kScrMaxTop = 256;     // largest candidate list of one selection / exact-ratio call
+static_assert(kScrParams == DPMM_SCREEN_PARAMS, "screen parameter count");
+static_assert(kScrF == DPMM_SCREEN_FEATURES, "screen feature count");
+static_assert(kScrMaxTop == DPMM_SCREEN_MAX_TOP, "screen list capacity");
+
 int padded_dim(int d);  // 4, 8, 16, 32, 64, 128 (Gaussian); d rounded up to 32 (multinomial)
 
 // Thread-local error message for dpmm_last_error().
@@ -144,11 +161,27 @@ struct dpmm_ctx {
     bool prior_set = false;
     double prior_k = 0, prior_v = 0;
     double prior_logdet = 0;       // log det psi0 (NIW)
+    bool prior_identity = false;   // NIW prior with m0 = 0 and psi0 = I
     double* d_prior = nullptr;     // NIW: m[D], psi[D*D]; multinomial: alpha[D]
     double* d_lml = nullptr;       // [3*k_max]
     double* d_split_hr = nullptr;  // [k_max]
     double* d_merge_hr = nullptr;  // [k_max*k_max]
     double* d_post_logdet = nullptr; // [3*k_max]
+    // learned split/merge screen (dpmm_screen.cu)
+    double* d_scr_rec = nullptr;   // [3*k_max][kScrRec] per-slot posterior quantities
+    double* d_scr_vec = nullptr;   // [3*k_max][2][D]: NIW m', diag(psi'); Dirichlet a'/sum a', a'
+    float* d_scr_linv = nullptr;   // [k_max][D][D] inverse Cholesky factor of each cluster's psi' (NIW)
+    float* d_scr_feat = nullptr;   // [rows][kScrF], rows = max(k_max, k_max (k_max - 1) / 2)
+    double* d_scr_prox = nullptr;  // [rows] proxy log Hastings ratio (feature 2 before scaling)
+    float* d_scr_score = nullptr;  // [rows] MLP scores
+    float* d_scr_w = nullptr;      // [kScrParams] FP32 parameters
+    float* d_scr_wdep = nullptr;   // [kScrParams] deployed: weights rounded to BF16, biases FP32
+    uint8_t* d_scr_elig = nullptr; // [k_max] eligible clusters
+    int32_t* d_scr_sel = nullptr;  // [kScrMaxTop + 1] selected rows, then their count
+    int32_t* d_scr_list = nullptr; // [2 * kScrMaxTop] clusters / pairs of an exact-ratio list
+    int32_t* d_scr_slots = nullptr;// [3 * kScrMaxTop] slots whose lml the list needs
+    double* d_scr_hr = nullptr;    // [kScrMaxTop] exact ratios of the list
+    bool scr_params_set = false;
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
 
@@ -229,6 +262,9 @@ dpmm_status launch_sample_log_cat_sub(dpmm_ctx* c, int m, const double* d_r, con
 // Hastings (dpmm_hastings.cu)
 dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha);
 dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha);
+// learned screen (dpmm_screen.cu)
+dpmm_status launch_screen_features(dpmm_ctx* c, int K, int kind, double alpha);
+dpmm_status launch_screen_select(dpmm_ctx* c, int K, int kind, double alpha, int top);
 // tensor-core label kernel (dpmm_tc.cu); returns DPMM_ERR_INVALID_ARG when the shape is unsupported
 bool tc_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);

@@ -75,6 +75,20 @@ struct Config {
     Hyper hyper, outlier_hyper;
     std::vector<int32_t> gt;
     int loglik_mode = DPMM_LL_AUTO, rng_kind = DPMM_RNG_PHILOX, k_max = 0, device = 0;
+    // learned split/merge screen (no counterpart in the reference)
+    int screen_mode = DPMM_SCREEN_OFF, screen_top = 16, screen_sweep = 10, screen_split_min = 256;
+    double screen_min_recall = 0.5;
+    std::vector<float> screen_params;
+};
+
+// screen counters and the DPMM_SCREEN_LOG record of a run
+struct ScreenRecord {
+    int64_t split_cand = 0, split_exact = 0, merge_cand = 0, merge_exact = 0;
+    int64_t sweeps = 0, sweep_accepts = 0, sweep_hits = 0, disabled_at = 0;
+    std::vector<float> log_features;
+    std::vector<double> log_hr;
+    std::vector<int8_t> log_kind;
+    std::vector<int32_t> log_iter;
 };
 
 class Sampler {
@@ -89,6 +103,7 @@ public:
     dpmm_status step(int n, dpmm_model_info* mi);
     dpmm_status finish(dpmm_model_info* mi);
     int num_clusters() const { return (int)clusters_.size(); }
+    const ScreenRecord& screen_record() const { return scr_; }
     int iteration() const { return iter_; }
 
 private:
@@ -300,6 +315,21 @@ private:
     std::vector<Splittable> clusters_;
     std::vector<double> weights_;
 
+    // ----------------------------------------------------------------- learned screen
+    enum ScreenUse { USE_FULL, USE_SCREEN, USE_SWEEP };
+    ScreenRecord scr_;
+    bool scr_disabled_ = false;
+    bool scr_swept_ = false;     // a full sweep ran in this iteration
+    // min_cand: fewer candidates than this are all evaluated exactly (the screen would cost more)
+    ScreenUse screen_use(int64_t ncand, int64_t min_cand = 0) const
+    {
+        if (cfg_.screen_mode != DPMM_SCREEN_ON || scr_disabled_) return USE_FULL;
+        if (cfg_.screen_sweep > 0 && iter_ % cfg_.screen_sweep == 0) return USE_SWEEP;
+        return ncand > cfg_.screen_top && ncand >= min_cand ? USE_SCREEN : USE_FULL;
+    }
+    dpmm_status screen_log(int K, int kind, const std::vector<uint8_t>& row_ok, const double* hr_of_row);
+    void screen_judge();
+
 };
 
 }  // namespace host
@@ -310,6 +340,7 @@ struct dpmm_model_info {
     std::vector<int32_t> labels;
     std::vector<double> weights, iter_count, likelihood_history, nmi_history;
     std::vector<int32_t> cluster_count_history;
+    dpmm::host::ScreenRecord screen;
 };
 
 namespace dpmm {
@@ -467,7 +498,8 @@ dpmm_status Sampler::reset_bad_clusters()
 }
 
 // local_clusters_actions::check_and_split + should_split_local + split_cluster_local
-// (local_clusters_actions.cpp:183-194, 215-285), split ratios from one device launch
+// (local_clusters_actions.cpp:183-194, 215-285), split ratios from one device launch.  With the
+// learned screen on, only the screen's top candidates are proposed (and evaluated exactly).
 dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indices)
 {
     const int K = (int)clusters_.size();
@@ -478,15 +510,47 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
         if (clusters_[i].splittable && clusters_[i].c.stats.N > 1 && !(cfg_.outlier_mod > 0 && i == 1))
             any_candidate = true;
     if (!any_candidate || final_) return DPMM_OK;
-    std::vector<double> hr(K);
-    DPMM_TRY(dpmm_split_hastings(ctx_, K, cfg_.alpha, nullptr, hr.data()));
+    // candidates whose ratio the device computes (the outlier cluster's is computed on the host)
+    std::vector<uint8_t> elig(K, 0);
+    int64_t ncand = 0;
+    for (int i = 0; i < K; ++i) {
+        const Splittable& sc = clusters_[i];
+        if (sc.splittable && sc.c.stats.N > 1 && sc.l.stats.N > 0 && sc.r.stats.N > 0 && !(cfg_.outlier_mod > 0 && i <= 1)) {
+            elig[i] = 1;
+            ++ncand;
+        }
+    }
+    std::vector<double> hr(K, NAN);
+    std::vector<uint8_t> in_sel(K, 0);
+    const ScreenUse use = screen_use(ncand, cfg_.screen_split_min);
+    if (use != USE_FULL && ncand > 0) {
+        std::vector<int32_t> sel(kScrMaxTop);
+        int32_t nsel = 0;
+        DPMM_TRY(dpmm_screen_select(ctx_, K, DPMM_SCREEN_SPLIT, cfg_.alpha, elig.data(), cfg_.screen_top, sel.data(),
+                                    &nsel, nullptr));
+        for (int t = 0; t < nsel; ++t) in_sel[sel[t]] = 1;
+        if (use == USE_SCREEN) {
+            std::vector<double> out(nsel);
+            DPMM_TRY(dpmm_split_hastings_list(ctx_, K, cfg_.alpha, nsel, sel.data(), out.data()));
+            for (int t = 0; t < nsel; ++t) hr[sel[t]] = out[t];
+            scr_.split_exact += nsel;
+        }
+    }
+    if (use != USE_SCREEN) {
+        DPMM_TRY(dpmm_split_hastings(ctx_, K, cfg_.alpha, nullptr, hr.data()));
+        scr_.split_exact += ncand;
+        if (cfg_.screen_mode == DPMM_SCREEN_LOG) DPMM_TRY(screen_log(K, DPMM_SCREEN_SPLIT, elig, hr.data()));
+    }
+    scr_.split_cand += ncand;
     for (int i = 0; i < K; ++i) {
         if (cfg_.outlier_mod > 0 && i == 1) continue;
         Splittable& sc = clusters_[i];
         if (!(sc.splittable && sc.c.stats.N > 1)) continue;
         if (sc.l.stats.N == 0 || sc.r.stats.N == 0) continue;
+        const bool outlier0 = cfg_.outlier_mod > 0 && i == 0;
+        if (use == USE_SCREEN && !outlier0 && !in_sel[i]) continue;   // not proposed this iteration
         double log_hr = hr[i];
-        if (cfg_.outlier_mod > 0 && i == 0) {
+        if (outlier0) {
             // the outlier cluster has its own prior: evaluate its ratio on the host
             Hyper p = posterior(sc.c.prior, sc.c.stats), pl = posterior(sc.c.prior, sc.l.stats),
                   pr = posterior(sc.c.prior, sc.r.stats);
@@ -495,7 +559,13 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
                      (std::lgamma((double)sc.c.stats.N) + lml(sc.c.prior, p, sc.c.stats));
         }
         const double u = uniform();
-        if (log_hr > std::log(u)) split[i] = 1;
+        if (log_hr > std::log(u)) {
+            split[i] = 1;
+            if (use == USE_SWEEP && elig[i]) {
+                ++scr_.sweep_accepts;
+                scr_.sweep_hits += in_sel[i];
+            }
+        }
     }
     int n_split = std::accumulate(split.begin(), split.end(), 0);
     // capacity guard: the device tables hold k_max clusters
@@ -542,45 +612,139 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
 
 // local_clusters_actions::check_and_merge + shared_actions::should_merge + merge_clusters
 // (local_clusters_actions.cpp:204-213, 287-321; shared_actions.cpp:72-111); all pair ratios
-// from one device launch, accepted greedily in (i, j) order
+// from one device launch, accepted greedily in (i, j) order.  With the learned screen on, only the
+// screen's top pairs are proposed (and evaluated exactly), still greedily in (i, j) order.
 dpmm_status Sampler::check_and_merge(bool final_)
 {
     const int K = (int)clusters_.size();
     int n_split = 0;
     for (auto& c : clusters_) n_split += c.splittable && c.c.stats.N > 0;
     if (n_split < 2) return DPMM_OK;
-    std::vector<double> hr((size_t)K * K);
-    DPMM_TRY(dpmm_merge_hastings(ctx_, K, cfg_.alpha, hr.data()));
-    std::vector<int32_t> idx, nidx;
+    std::vector<uint8_t> elig(K, 0);
+    int64_t m = 0;
     for (int i = 0; i < K; ++i) {
-        if (cfg_.outlier_mod > 0 && i == 0) continue;
-        for (int j = i + 1; j < K; ++j) {
-            Splittable& a = clusters_[i];
-            Splittable& b = clusters_[j];
-            if (!(a.splittable && b.splittable && a.c.stats.N > 0 && b.c.stats.N > 0)) continue;
-            const double log_hr = hr[(size_t)i * K + j];
-            const double u = uniform();
-            if (!((log_hr > std::log(u)) || (final_ && log_hr > std::log(0.1)))) continue;
-            // merge_clusters_to_splittable(a, b.c) then local bookkeeping
-            a.c.stats = aggregate(a.c.stats, b.c.stats);
-            a.c.post = posterior(a.c.prior, a.c.stats);
-            std::vector<double> w = dirichlet({(double)a.c.stats.N + cfg_.alpha / 2, (double)b.c.stats.N + cfg_.alpha / 2});
-            a.lrw[0] = w[0];
-            a.lrw[1] = w[1];
-            a.l = a.c;
-            a.r = b.c;
-            a.splittable = false;
-            a.hist = fresh_hist();
-            a.points_count += b.points_count;
-            b.points_count = 0;
-            b.c.stats.N = 0;
-            b.splittable = false;
-            idx.push_back(i);
-            nidx.push_back(j);
+        const Splittable& a = clusters_[i];
+        elig[i] = !(cfg_.outlier_mod > 0 && i == 0) && a.splittable && a.c.stats.N > 0;
+        m += elig[i];
+    }
+    const int64_t ncand = m * (m - 1) / 2;
+    const ScreenUse use = screen_use(ncand);
+    // proposals in (i, j) order with their ratios
+    struct Prop {
+        int i, j;
+        double hr;
+        bool sel;
+    };
+    std::vector<Prop> props;
+    std::vector<uint8_t> in_sel;
+    std::vector<int32_t> sel_pairs;
+    if (use != USE_FULL && ncand > 0) {
+        std::vector<int32_t> sel(kScrMaxTop);
+        int32_t nsel = 0;
+        DPMM_TRY(dpmm_screen_select(ctx_, K, DPMM_SCREEN_MERGE, cfg_.alpha, elig.data(), cfg_.screen_top, sel.data(),
+                                    &nsel, nullptr));
+        in_sel.assign((size_t)K * K, 0);
+        for (int t = 0; t < nsel; ++t) {
+            int64_t b = sel[t];
+            int i = 0, rowlen = K - 1;
+            while (b >= rowlen) {
+                b -= rowlen;
+                ++i;
+                --rowlen;
+            }
+            const int j = i + 1 + (int)b;
+            in_sel[(size_t)i * K + j] = 1;
+            sel_pairs.push_back(i);
+            sel_pairs.push_back(j);
         }
+        if (use == USE_SCREEN) {
+            std::vector<double> out(nsel);
+            DPMM_TRY(dpmm_merge_hastings_list(ctx_, K, cfg_.alpha, nsel, sel_pairs.data(), out.data()));
+            for (int t = 0; t < nsel; ++t) props.push_back({sel_pairs[2 * t], sel_pairs[2 * t + 1], out[t], true});
+            scr_.merge_exact += nsel;
+        }
+    }
+    if (use != USE_SCREEN) {
+        std::vector<double> hr((size_t)K * K);
+        DPMM_TRY(dpmm_merge_hastings(ctx_, K, cfg_.alpha, hr.data()));
+        scr_.merge_exact += ncand;
+        if (cfg_.screen_mode == DPMM_SCREEN_LOG) {
+            std::vector<uint8_t> row_ok;
+            std::vector<double> hr_rows;
+            for (int i = 0; i < K; ++i)
+                for (int j = i + 1; j < K; ++j) {
+                    row_ok.push_back(elig[i] && elig[j]);
+                    hr_rows.push_back(hr[(size_t)i * K + j]);
+                }
+            DPMM_TRY(screen_log(K, DPMM_SCREEN_MERGE, row_ok, hr_rows.data()));
+        }
+        for (int i = 0; i < K; ++i)
+            for (int j = i + 1; j < K; ++j)
+                props.push_back({i, j, hr[(size_t)i * K + j], !in_sel.empty() && in_sel[(size_t)i * K + j]});
+    }
+    scr_.merge_cand += ncand;
+    std::vector<int32_t> idx, nidx;
+    for (const Prop& pr : props) {
+        const int i = pr.i, j = pr.j;
+        if (cfg_.outlier_mod > 0 && i == 0) continue;
+        Splittable& a = clusters_[i];
+        Splittable& b = clusters_[j];
+        if (!(a.splittable && b.splittable && a.c.stats.N > 0 && b.c.stats.N > 0)) continue;
+        const double log_hr = pr.hr;
+        const double u = uniform();
+        if (!((log_hr > std::log(u)) || (final_ && log_hr > std::log(0.1)))) continue;
+        if (use == USE_SWEEP) {
+            ++scr_.sweep_accepts;
+            scr_.sweep_hits += pr.sel;
+        }
+        // merge_clusters_to_splittable(a, b.c) then local bookkeeping
+        a.c.stats = aggregate(a.c.stats, b.c.stats);
+        a.c.post = posterior(a.c.prior, a.c.stats);
+        std::vector<double> w = dirichlet({(double)a.c.stats.N + cfg_.alpha / 2, (double)b.c.stats.N + cfg_.alpha / 2});
+        a.lrw[0] = w[0];
+        a.lrw[1] = w[1];
+        a.l = a.c;
+        a.r = b.c;
+        a.splittable = false;
+        a.hist = fresh_hist();
+        a.points_count += b.points_count;
+        b.points_count = 0;
+        b.c.stats.N = 0;
+        b.splittable = false;
+        idx.push_back(i);
+        nidx.push_back(j);
     }
     if (idx.empty()) return DPMM_OK;
     return dpmm_merge_clusters(ctx_, (int)idx.size(), idx.data(), nidx.data());
+}
+
+// features + exact ratio of every loggable candidate row (DPMM_SCREEN_LOG)
+dpmm_status Sampler::screen_log(int K, int kind, const std::vector<uint8_t>& row_ok, const double* hr_of_row)
+{
+    const size_t rows = row_ok.size();
+    if (rows == 0) return DPMM_OK;
+    std::vector<float> f(rows * kScrF);
+    DPMM_TRY(dpmm_screen_features(ctx_, K, kind, cfg_.alpha, f.data(), nullptr));
+    for (size_t r = 0; r < rows; ++r) {
+        if (!row_ok[r] || !std::isfinite(hr_of_row[r])) continue;
+        scr_.log_features.insert(scr_.log_features.end(), &f[r * kScrF], &f[r * kScrF] + kScrF);
+        scr_.log_hr.push_back(hr_of_row[r]);
+        scr_.log_kind.push_back((int8_t)kind);
+        scr_.log_iter.push_back(iter_);
+    }
+    return DPMM_OK;
+}
+
+// after an iteration with a full sweep: switch the screen off when its recall is too low
+void Sampler::screen_judge()
+{
+    if (!scr_swept_) return;
+    scr_swept_ = false;
+    ++scr_.sweeps;
+    if (scr_.sweep_accepts >= 8 && (double)scr_.sweep_hits < cfg_.screen_min_recall * (double)scr_.sweep_accepts) {
+        scr_disabled_ = true;
+        scr_.disabled_at = iter_;
+    }
 }
 
 // local_clusters_actions::remove_empty_clusters (local_clusters_actions.cpp:384-419)
@@ -618,9 +782,11 @@ dpmm_status Sampler::group_step(bool no_more_splits, bool final_)
     DPMM_TRY(reset_bad_clusters());
     if (!no_more_splits) {
         std::vector<int32_t> idx;
+        scr_swept_ = screen_use(0) == USE_SWEEP;
         DPMM_TRY(check_and_split(final_, idx));
         DPMM_TRY(update_suff_stats_posterior(idx));
         DPMM_TRY(check_and_merge(final_));
+        screen_judge();
     }
     return remove_empty_clusters();
 }
@@ -755,6 +921,7 @@ dpmm_status Sampler::finish(dpmm_model_info* mi)
     mi->labels.resize(N_);
     DPMM_TRY(dpmm_get_labels(ctx_, mi->labels.data()));
     mi->weights = weights_;
+    mi->screen = scr_;
     return DPMM_OK;
 }
 
@@ -816,6 +983,10 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
     DPMM_TRY(finish(cfg.outlier_hyper));
     if (cfg.burnout < 1) return fail(DPMM_ERR_INVALID_ARG, "burnout must be >= 1");
     if (cfg.initial_clusters < 1) return fail(DPMM_ERR_INVALID_ARG, "initial_clusters must be >= 1");
+    if (cfg.screen_mode < DPMM_SCREEN_OFF || cfg.screen_mode > DPMM_SCREEN_LOG)
+        return fail(DPMM_ERR_INVALID_ARG, "unknown screen_mode");
+    if (cfg.screen_top < 1 || cfg.screen_top > kScrMaxTop)
+        return fail(DPMM_ERR_INVALID_ARG, "screen_top must be in [1, 256]");
     if (!(cfg.alpha > 0)) return fail(DPMM_ERR_INVALID_ARG, "alpha must be positive");
     dpmm_desc desc{};
     desc.n_points = N;
@@ -834,6 +1005,11 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
         DPMM_TRY(dpmm_set_prior_niw(h->ctx, cfg.hyper.k, cfg.hyper.m.data(), cfg.hyper.v, cfg.hyper.psi.data()));
     else
         DPMM_TRY(dpmm_set_prior_multinomial(h->ctx, cfg.hyper.alpha.data()));
+    if (cfg.screen_mode == DPMM_SCREEN_ON) {
+        if ((int)cfg.screen_params.size() != kScrParams)
+            return fail(DPMM_ERR_INVALID_ARG, "screen_mode DPMM_SCREEN_ON needs screen_params");
+        DPMM_TRY(dpmm_screen_set_params(h->ctx, cfg.screen_params.data()));
+    }
     h->sampler = std::make_unique<Sampler>(cfg, h->ctx, N, D);
     DPMM_TRY(h->sampler->init());
     out = std::move(h);
@@ -899,6 +1075,16 @@ static Hyper hyper_from_json(int prior, int D, const io::Json& j)
 
 using namespace dpmm;
 
+static void screen_from_run(const dpmm_run_desc* run, host::Config& cfg)
+{
+    cfg.screen_mode = run->screen_mode;
+    cfg.screen_top = run->screen_top > 0 ? run->screen_top : 16;
+    cfg.screen_sweep = run->screen_sweep_every > 0 ? run->screen_sweep_every : 10;
+    cfg.screen_min_recall = run->screen_min_recall > 0 ? run->screen_min_recall : 0.5;
+    cfg.screen_split_min = run->screen_split_min > 0 ? run->screen_split_min : 256;
+    if (run->screen_params) cfg.screen_params.assign(run->screen_params, run->screen_params + kScrParams);
+}
+
 static host::Config config_from_run(const dpmm_run_desc* run, int64_t n, int32_t d)
 {
     host::Config cfg;
@@ -919,6 +1105,7 @@ static host::Config config_from_run(const dpmm_run_desc* run, int64_t n, int32_t
     cfg.outlier_hyper = host::hyper_from_run(cfg.prior, d, run->out_niw_k, run->out_niw_v, run->out_niw_m,
                                              run->out_niw_psi, run->out_mult_alpha);
     if (run->gt) cfg.gt.assign(run->gt, run->gt + n);
+    screen_from_run(run, cfg);
     return cfg;
 }
 
@@ -1018,6 +1205,7 @@ extern "C" dpmm_status dpmm_dp_parallel_from_file(const char* npy_path, const ch
         cfg.k_max = ov->k_max;
         cfg.device = ov->device;
         if (ov->seed) cfg.seed = ov->seed;
+        screen_from_run(ov, cfg);
     }
     return host::run_sampler(cfg, rows, D, pts.data(), false, out);
 }
@@ -1061,6 +1249,37 @@ extern "C" dpmm_status dpmm_model_info_write_json(const dpmm_model_info* mi, con
     }
     f << "]}\n";
     return f ? DPMM_OK : fail(DPMM_ERR_IO, "write failed");
+}
+
+extern "C" dpmm_status dpmm_model_info_screen_stats(const dpmm_model_info* mi, int64_t* out)
+{
+    if (!mi || !out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    const host::ScreenRecord& r = mi->screen;
+    const int64_t v[8] = {r.split_cand, r.split_exact, r.merge_cand, r.merge_exact,
+                          r.sweeps,     r.sweep_accepts, r.sweep_hits, r.disabled_at};
+    std::memcpy(out, v, sizeof(v));
+    return DPMM_OK;
+}
+extern "C" int64_t dpmm_model_info_screen_log_rows(const dpmm_model_info* mi)
+{
+    return mi ? (int64_t)mi->screen.log_hr.size() : 0;
+}
+extern "C" const float* dpmm_model_info_screen_log_features(const dpmm_model_info* mi)
+{
+    return (mi && !mi->screen.log_features.empty()) ? mi->screen.log_features.data() : nullptr;
+}
+extern "C" const double* dpmm_model_info_screen_log_hr(const dpmm_model_info* mi)
+{
+    return (mi && !mi->screen.log_hr.empty()) ? mi->screen.log_hr.data() : nullptr;
+}
+extern "C" const int8_t* dpmm_model_info_screen_log_kind(const dpmm_model_info* mi)
+{
+    return (mi && !mi->screen.log_kind.empty()) ? mi->screen.log_kind.data() : nullptr;
+}
+
+extern "C" const int32_t* dpmm_model_info_screen_log_iter(const dpmm_model_info* mi)
+{
+    return (mi && !mi->screen.log_iter.empty()) ? mi->screen.log_iter.data() : nullptr;
 }
 
 extern "C" void dpmm_model_info_free(dpmm_model_info* mi) { delete mi; }

@@ -244,6 +244,51 @@ dpmm_status dpmm_merge_hastings_static(int32_t prior_type, int32_t D, int32_t K,
                                        const double* prior, const double* stats, double* merge_log_hr,
                                        void* stream);
 
+/* ---- learned split/merge screen (no counterpart in the reference) ----------------------------
+ * The reference computes the exact ratio of every split candidate and every cluster pair each
+ * iteration (local_clusters_actions.cpp:244-321).  The screen ranks the candidates with a small MLP
+ * over 32 features derived from the statistics on the device, so the exact FP64 ratio
+ * (dpmm_split_hastings_list / dpmm_merge_hastings_list, the same arithmetic as dpmm_split_hastings /
+ * dpmm_merge_hastings) is needed for the best-ranked few only; the accept test stays exact.
+ * Candidate rows: split row k = cluster k (K rows); merge row = pair i < j, row-major over the
+ * strict upper triangle (K(K-1)/2 rows). */
+#define DPMM_SCREEN_FEATURES 32
+#define DPMM_SCREEN_HIDDEN 64
+/* parameters, one FP32 vector: W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3 */
+#define DPMM_SCREEN_PARAMS 6337
+#define DPMM_SCREEN_MAX_TOP 256
+typedef enum dpmm_screen_kind { DPMM_SCREEN_SPLIT = 0, DPMM_SCREEN_MERGE = 1 } dpmm_screen_kind;
+
+/* MLP parameters of the context's screen (inference rounds the weights to BF16, biases stay FP32) */
+dpmm_status dpmm_screen_set_params(dpmm_ctx* ctx, const float* params);
+/* features (rows x 32, nullable) and proxy log ratios (rows, nullable) of every candidate of `kind`
+ * for the K clusters whose statistics are on the device; rows with an empty slot are zero */
+dpmm_status dpmm_screen_features(dpmm_ctx* ctx, int K, int kind, double alpha, float* features, double* proxy);
+/* features + MLP scores + selection: the `top` (<= DPMM_SCREEN_MAX_TOP) best-scored candidate rows
+ * whose clusters are all eligible (eligible[K], nonzero = eligible), in ascending row order, into
+ * selected[n_selected]; scores (rows, nullable) receives every row's score */
+dpmm_status dpmm_screen_select(dpmm_ctx* ctx, int K, int kind, double alpha, const uint8_t* eligible, int top,
+                               int32_t* selected, int32_t* n_selected, float* scores);
+/* exact split ratios of n (<= DPMM_SCREEN_MAX_TOP) listed clusters / merge ratios of n listed pairs
+ * (pairs[2t], pairs[2t+1]); values equal those of dpmm_split_hastings / dpmm_merge_hastings */
+dpmm_status dpmm_split_hastings_list(dpmm_ctx* ctx, int K, double alpha, int n, const int32_t* clusters,
+                                     double* split_log_hr);
+dpmm_status dpmm_merge_hastings_list(dpmm_ctx* ctx, int K, double alpha, int n, const int32_t* pairs,
+                                     double* merge_log_hr);
+/* MLP on the device without a context (host arrays in and out):
+ *   forward: scores[rows] of features[rows x 32] with the deployed (BF16-weight) parameters;
+ *   loss_grad: mean squared error (1/rows) sum (z - t)^2 of the FP32 parameters and its gradient;
+ *   train: `epochs` passes of shuffled minibatches (the last partial batch of an epoch is dropped),
+ *          Adam (beta 0.9 / 0.999, eps 1e-8) at rate lr from the given parameters, updated in place;
+ *          epoch_loss[epochs] (nullable) = mean minibatch loss of each epoch. */
+dpmm_status dpmm_screen_forward(const float* features, int64_t rows, const float* params, float* scores,
+                                int32_t device);
+dpmm_status dpmm_screen_loss_grad(const float* features, const float* targets, int32_t rows, const float* params,
+                                  float* loss, float* grad, int32_t device);
+dpmm_status dpmm_screen_train(const float* features, const float* targets, int64_t rows, int32_t epochs,
+                              int32_t batch, float lr, uint64_t seed, float* params, float* epoch_loss,
+                              int32_t device);
+
 /* Synchronise the context's stream; returns any pending device error. */
 dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
@@ -286,8 +331,23 @@ typedef struct dpmm_run_desc {
     const double* out_mult_alpha;
     const int32_t* gt;           /* ground-truth labels for NMI (nullable) */
     int32_t device;
-    int32_t reserved[7];
+    /* learned split/merge screen (no counterpart in the reference; 0 = every candidate exact) */
+    int32_t screen_mode;         /* dpmm_screen_mode */
+    int32_t screen_top;          /* candidates of each kind sent to the exact ratio (0 -> 16) */
+    int32_t screen_sweep_every;  /* every this many iterations all candidates are exact (0 -> 10) */
+    float screen_min_recall;     /* the screen is switched off for the rest of the run when the full
+                                    sweeps' recall of accepted moves falls below this (0 -> 0.5) */
+    const float* screen_params;  /* DPMM_SCREEN_PARAMS floats; required by DPMM_SCREEN_ON */
+    int32_t screen_split_min;    /* split candidates are screened only above this many (0 -> 256): the
+                                    exact split ratios of K clusters cost one launch of 3K blocks */
+    int32_t reserved[3];
 } dpmm_run_desc;
+
+typedef enum dpmm_screen_mode {
+    DPMM_SCREEN_OFF = 0,         /* every candidate exact (the reference's behaviour) */
+    DPMM_SCREEN_ON = 1,          /* exact ratio for the screen's top candidates only */
+    DPMM_SCREEN_LOG = 2          /* every candidate exact, and its features + exact ratio logged */
+} dpmm_screen_mode;
 
 typedef struct dpmm_model_info dpmm_model_info;
 
@@ -330,6 +390,19 @@ const double* dpmm_model_info_iter_count(const dpmm_model_info* mi);
 const double* dpmm_model_info_likelihood_history(const dpmm_model_info* mi);
 const double* dpmm_model_info_nmi_history(const dpmm_model_info* mi);  /* NULL without gt */
 const int32_t* dpmm_model_info_cluster_count_history(const dpmm_model_info* mi);
+/* screen counters of the run (all 0 with the screen off): out[0] split candidates, out[1] split
+ * candidates evaluated exactly, out[2] merge candidates (pairs), out[3] pairs evaluated exactly,
+ * out[4] full sweeps run, out[5] moves accepted in them, out[6] of those, moves the screen's
+ * selection of the same iteration held, out[7] iteration at which the screen was switched off (0:
+ * never) */
+dpmm_status dpmm_model_info_screen_stats(const dpmm_model_info* mi, int64_t* out);
+/* the DPMM_SCREEN_LOG record: rows of (features[32], exact log ratio, kind 0 split / 1 merge,
+ * iteration) */
+int64_t dpmm_model_info_screen_log_rows(const dpmm_model_info* mi);
+const float* dpmm_model_info_screen_log_features(const dpmm_model_info* mi);
+const double* dpmm_model_info_screen_log_hr(const dpmm_model_info* mi);
+const int8_t* dpmm_model_info_screen_log_kind(const dpmm_model_info* mi);
+const int32_t* dpmm_model_info_screen_log_iter(const dpmm_model_info* mi);
 /* write {"labels": [...], "weights": [...], "iter_count": [...]} as main.cpp:72-87 does */
 dpmm_status dpmm_model_info_write_json(const dpmm_model_info* mi, const char* path);
 void dpmm_model_info_free(dpmm_model_info* mi);
