@@ -250,6 +250,8 @@ def main():
     ap.add_argument("--d", type=int, default=64)
     ap.add_argument("--k-true", type=int, default=100)
     ap.add_argument("--mode", default="auto", choices=["auto", "fp32", "tc"])
+    ap.add_argument("--host-draws", action="store_true",
+                    help="draw the cluster parameters on the host instead of the device")
     ap.add_argument("--screen", default="on", choices=["on", "off"],
                     help="learned split/merge screen (exact ratios for the top 16 candidates of each kind)")
     ap.add_argument("--no-e2e", action="store_true")
@@ -304,6 +306,7 @@ def main():
         rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
         rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        rd.host_param_draws = int(args.host_draws)
         if screen_params is not None:
             rd.screen_mode = capi.SCREEN_ON
             rd.screen_params = screen_params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
@@ -393,6 +396,7 @@ def main():
                        "clusters_in_timed_steps": ks, "loglik_mode": args.mode,
                        "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
                        "nmi_vs_generating_labels": nmi,
+                       "parameter_draws": "host" if args.host_draws else "device",
                        "screen": screen_summary(args.screen, scr)},
             "gpu_launches": int(launches),
             "roofline": roofline,

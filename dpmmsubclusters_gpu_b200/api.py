@@ -128,7 +128,7 @@ class dp_parallel_sampling_class:
     def __init__(self, a, b, c=None, d=None, *, loglik_mode: int = capi.LL_AUTO, rng_kind: int = capi.RNG_PHILOX,
                  k_max: int = 0, device: int = 0, screen_mode: int = capi.SCREEN_OFF, screen_params=None,
                  screen_top: int = 16, screen_sweep_every: int = 10, screen_min_recall: float = 0.5,
-                 screen_split_min: int = 256):
+                 screen_split_min: int = 256, host_param_draws: bool = False):
         """screen_*: the learned split/merge screen (no counterpart in the reference); screen_params
         defaults to the trained parameters shipped with the package when screen_mode is SCREEN_ON."""
         self._from_file = isinstance(a, str)
@@ -136,6 +136,7 @@ class dp_parallel_sampling_class:
         self.screen_mode, self.screen_top = screen_mode, screen_top
         self.screen_sweep_every, self.screen_min_recall = screen_sweep_every, screen_min_recall
         self.screen_split_min = screen_split_min
+        self.host_param_draws = host_param_draws
         if screen_mode == capi.SCREEN_ON and screen_params is None:
             from .screen import load_params
             screen_params = load_params()
@@ -207,6 +208,7 @@ class dp_parallel_sampling_class:
         rd.screen_sweep_every = self.screen_sweep_every
         rd.screen_min_recall = self.screen_min_recall
         rd.screen_split_min = self.screen_split_min
+        rd.host_param_draws = int(self.host_param_draws)
         if self.screen_params is not None:
             if self.screen_params.size != capi.SCREEN_PARAMS:
                 raise ValueError(f"screen_params must hold {capi.SCREEN_PARAMS} values")
@@ -478,6 +480,44 @@ class CudaKernel:
         out = np.empty(pr.shape[0])
         check(lib().dpmm_merge_hastings_list(self.ctx, K, alpha, pr.shape[0], _iptr(pr), _dptr(out)))
         return out
+
+    # -------------------------------------------------------------- device parameter draws
+    def sample_gaussian_params(self, K: int, seed: int, draw: int, weights, lr_weights):
+        """NIW draws of every slot on the device (into the label-phase parameters); -> lml (K, 3)"""
+        w = np.ascontiguousarray(weights, np.float64)
+        lw = np.ascontiguousarray(lr_weights, np.float64).reshape(-1)
+        lml = np.empty(3 * K)
+        check(lib().dpmm_sample_gaussian_params(self.ctx, K, seed, draw, _dptr(w), _dptr(lw), _dptr(lml)))
+        return lml.reshape(K, 3)
+
+    def merge_statistics(self, index, new_index):
+        i = np.atleast_1d(np.asarray(index, np.int32))
+        j = np.atleast_1d(np.asarray(new_index, np.int32))
+        check(lib().dpmm_merge_statistics(self.ctx, i.size, _iptr(i), _iptr(j)))
+
+    def compact_statistics(self, keep):
+        k = np.ascontiguousarray(keep, np.int32)
+        check(lib().dpmm_compact_statistics(self.ctx, k.size, _iptr(k)))
+
+    def statistics_counts(self, indices):
+        idx = np.ascontiguousarray(indices, np.int32)
+        out = np.empty(3 * idx.size, np.int64)
+        check(lib().dpmm_statistics_counts(self.ctx, idx.size, _iptr(idx), out.ctypes.data_as(ctypes.POINTER(c_int64))))
+        return out.reshape(-1, 3)
+
+    def gaussian_params(self, K: int):
+        """-> W (3K, D, D), b (3K, D), c (3K,), mu - shift (3K, D) as packed on the device"""
+        Dp = 4
+        while Dp < self.D:
+            Dp *= 2
+        S = 3 * K
+        wt = np.empty((S, Dp, Dp), np.float32)
+        b = np.empty((S, Dp), np.float32)
+        c = np.empty(S, np.float32)
+        mu = np.empty((S, Dp), np.float32)
+        check(lib().dpmm_get_gaussian_params(self.ctx, K, _fptr(wt), _fptr(b), _fptr(c), _fptr(mu)))
+        D = self.D
+        return np.swapaxes(wt, 1, 2)[:, :D, :D].copy(), b[:, :D].copy(), c, mu[:, :D].copy()
 
     def synchronize(self):
         check(lib().dpmm_synchronize(self.ctx))

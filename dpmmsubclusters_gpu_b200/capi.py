@@ -51,7 +51,7 @@ class dpmm_run_desc(Structure):
                 ("out_mult_alpha", _PD), ("gt", POINTER(c_int32)), ("device", c_int32),
                 ("screen_mode", c_int32), ("screen_top", c_int32), ("screen_sweep_every", c_int32),
                 ("screen_min_recall", c_float), ("screen_params", POINTER(c_float)), ("screen_split_min", c_int32),
-                ("reserved", c_int32 * 3)]
+                ("host_param_draws", c_int32), ("reserved", c_int32 * 2)]
 
 
 # every symbol include/dpmm_capi.h declares, with its ctypes signature
@@ -133,6 +133,11 @@ SIGNATURES = {
     "dpmm_model_info_screen_log_hr": (_PD, [c_void_p]),
     "dpmm_model_info_screen_log_kind": (POINTER(c_int8), [c_void_p]),
     "dpmm_model_info_screen_log_iter": (_PI32, [c_void_p]),
+    "dpmm_sample_gaussian_params": (c_int, [_CTX, c_int, c_uint64, c_uint64, _PD, _PD, _PD]),
+    "dpmm_merge_statistics": (c_int, [_CTX, c_int, _PI32, _PI32]),
+    "dpmm_compact_statistics": (c_int, [_CTX, c_int, _PI32]),
+    "dpmm_statistics_counts": (c_int, [_CTX, c_int, _PI32, _PI64]),
+    "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
 }
 
 _lib = None

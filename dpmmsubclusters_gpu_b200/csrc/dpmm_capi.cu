@@ -150,7 +150,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc, c->d_rbuf,
                     c->d_rpart, c->d_Bsub, c->d_scr_rec, c->d_scr_vec, c->d_scr_linv, c->d_scr_feat,
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
-                    c->d_scr_list, c->d_scr_slots, c->d_scr_hr};
+                    c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -254,6 +254,8 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     chk(dev_alloc(&c->d_nchunks, (size_t)1));
     chk(dev_alloc(&c->d_part, (size_t)c->max_chunks * 2 * SL));
     chk(dev_alloc(&c->d_stats, (size_t)3 * KM * c->stat_len));
+    chk(dev_alloc(&c->d_stats_tmp, (size_t)3 * KM * c->stat_len));
+    chk(dev_alloc(&c->d_logw, (size_t)KM));
     chk(dev_alloc(&c->d_remap, (size_t)KM + 2));
     chk(dev_alloc(&c->d_mask, (size_t)KM));
     c->stats_ok.assign(KM, 0);

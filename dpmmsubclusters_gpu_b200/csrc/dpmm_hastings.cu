@@ -72,6 +72,16 @@ static dpmm_status launch_slot_lml(dpmm_ctx* c, int K)
     return DPMM_OK;
 }
 
+dpmm_status slot_lml_as_is(dpmm_ctx* c, int K, double* lml)
+{
+    if (!c->prior_set) return fail(DPMM_ERR_STATE, "prior hyper-parameters not set");
+    DPMM_TRY(launch_slot_lml(c, K));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(lml, c->d_lml, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    g_d2h_bytes.fetch_add(sizeof(double) * 3 * K, std::memory_order_relaxed);
+    return DPMM_OK;
+}
+
 dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha)
 {
     if (!c->prior_set) return fail(DPMM_ERR_STATE, "prior hyper-parameters not set");

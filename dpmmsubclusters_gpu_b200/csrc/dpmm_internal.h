@@ -144,6 +144,8 @@ struct dpmm_ctx {
     // statistics: chunk partials (FP64) and per-slot results in original coordinates
     double* d_part = nullptr;      // [max_chunks][2][stat_len]
     double* d_stats = nullptr;     // [3*k_max][stat_len]: count, sum[D], S[D*D] (col-major)
+    double* d_stats_tmp = nullptr; // same size: the target of a compaction (then swapped)
+    double* d_logw = nullptr;      // [k_max] log mixture weights of the device parameter draw
     int stat_len = 0;              // 1 + D + D*D (Gaussian) / 1 + D (multinomial)
     int stats_K = -1;              // clusters 0..stats_K-1 have statistics on the device ...
     std::vector<uint8_t> stats_ok; // ... and stats_ok[k] says whether they are still current
@@ -262,6 +264,9 @@ dpmm_status launch_sample_log_cat_sub(dpmm_ctx* c, int m, const double* d_r, con
 // Hastings (dpmm_hastings.cu)
 dpmm_status launch_split_hastings(dpmm_ctx* c, int K, double alpha);
 dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha);
+// log marginal likelihood of the 3K slots of the statistics as they are on the device (no
+// recompute from the labels), copied to lml[3K]
+dpmm_status slot_lml_as_is(dpmm_ctx* c, int K, double* lml);
 // learned screen (dpmm_screen.cu)
 dpmm_status launch_screen_features(dpmm_ctx* c, int K, int kind, double alpha);
 dpmm_status launch_screen_select(dpmm_ctx* c, int K, int kind, double alpha, int top);

@@ -154,20 +154,24 @@ __device__ double reg_chol_logdet(double (&a)[RegChol<DP>::EP], int D, double* s
 // D <= DP.  sh: RegChol<DP>::SMEM doubles of shared memory (mp[DP] at 2 DP).  The posterior scale psi'
 // (upper triangle mirrored, as selfadjointView<Upper>) is built in registers and factored by
 // reg_chol_logdet.  Lout (nullable) receives its lower Cholesky factor.  Valid in every thread.
+// With allow_empty, an empty slot (n = 0) is factored too (its posterior is the prior; the
+// parameter draw needs the factor) and its statistics are read as zero; otherwise it returns 0.
 template <int DP>
 __device__ double niw_lml_reg(int D, double n, const double* sum, const double* S, const double* sum2, const double* S2,
                               double k0, double v0, const double* m0, const double* psi0, double ld0, double* sh,
-                              NiwExtras* ex = nullptr, double* Lout = nullptr)
+                              NiwExtras* ex = nullptr, double* Lout = nullptr, bool allow_empty = false)
 {
     using RC = RegChol<DP>;
-    if (n == 0) return 0.0;      // posterior == prior (niw.cpp:27-30): every term cancels
+    if (n == 0 && !allow_empty) return 0.0;   // posterior == prior (niw.cpp:27-30): every term cancels
+    const bool has = n > 0;
     double* mp = sh + 2 * DP;
     double* red = sh + 3 * DP;
     const int t = threadIdx.x;
     const int i = t % DP, c = t / DP;
     const bool act = c < RC::C && i < D;
     const double kp = k0 + n, vp = v0 + n;
-    for (int d = t; d < D; d += blockDim.x) mp[d] = (m0[d] * k0 + (sum2 ? sum[d] + sum2[d] : sum[d])) / kp;
+    for (int d = t; d < D; d += blockDim.x)
+        mp[d] = (m0[d] * k0 + (has ? (sum2 ? sum[d] + sum2[d] : sum[d]) : 0.0)) / kp;
     __syncthreads();
     double a[RC::EP];
     double h = 0, tr = 0;
@@ -178,7 +182,7 @@ __device__ double niw_lml_reg(int D, double n, const double* sum, const double* 
         if (act && k <= i) {
             const size_t ki = (size_t)i * D + k;   // upper-triangle source: row k <= column i
             const double tm = v0 * psi0[ki] + k0 * m0[k] * m0[i];
-            const double sv = S2 ? S[ki] + S2[ki] : S[ki];
+            const double sv = has ? (S2 ? S[ki] + S2[ki] : S[ki]) : 0.0;
             a[q] = (tm - kp * mp[k] * mp[i] + sv) / vp;
             if (k == i) {
                 h += log(a[q]);

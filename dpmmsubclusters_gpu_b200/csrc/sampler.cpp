@@ -79,6 +79,7 @@ struct Config {
     int screen_mode = DPMM_SCREEN_OFF, screen_top = 16, screen_sweep = 10, screen_split_min = 256;
     double screen_min_recall = 0.5;
     std::vector<float> screen_params;
+    bool host_param_draws = false;   // draw the NIW parameters on the host even where the device can
 };
 
 // screen counters and the DPMM_SCREEN_LOG record of a run
@@ -96,6 +97,9 @@ public:
     Sampler(const Config& cfg, dpmm_ctx* ctx, int64_t N, int D)
         : cfg_(cfg), ctx_(ctx), N_(N), D_(D), gen_((unsigned long)cfg.seed)
     {
+        // device-resident parameters: the NIW draws run on the device from the device statistics,
+        // the host keeps counts only (the outlier cluster's own prior stays on the host path)
+        dev_ = cfg.prior == DPMM_PRIOR_GAUSSIAN && !(cfg.outlier_mod > 0) && !cfg.host_param_draws && D <= 64;
     }
 
     // init_model + init_first_clusters, then iterations first..first+n-1 of run_model
@@ -296,14 +300,16 @@ private:
     dpmm_status upload_params(const std::vector<double>& weights);
     dpmm_status update_suff_stats_posterior(const std::vector<int32_t>& indices);
     void sample_cluster_params_all();
-    void sample_clusters();
+    dpmm_status sample_clusters();
+    dpmm_status sample_clusters_device();
+    void mixture_weights();
     dpmm_status reset_bad_clusters();
     dpmm_status check_and_split(bool final_, std::vector<int32_t>& all_indices);
     dpmm_status check_and_merge(bool final_);
     dpmm_status remove_empty_clusters();
     dpmm_status group_step(bool no_more_splits, bool final_);
     dpmm_status init_first_clusters();
-    double calculate_posterior() const;
+    dpmm_status calculate_posterior(double* out);
     double nmi(const std::vector<int32_t>& labels) const;
     Config cfg_;
     dpmm_ctx* ctx_;
@@ -317,6 +323,7 @@ private:
 
     // ----------------------------------------------------------------- learned screen
     enum ScreenUse { USE_FULL, USE_SCREEN, USE_SWEEP };
+    bool dev_ = false;            // parameters drawn on the device (see the constructor)
     ScreenRecord scr_;
     bool scr_disabled_ = false;
     bool scr_swept_ = false;     // a full sweep ran in this iteration
@@ -389,6 +396,18 @@ dpmm_status Sampler::update_suff_stats_posterior(const std::vector<int32_t>& ind
 {
     const int n = (int)indices.size();
     if (n == 0) return DPMM_OK;
+    if (dev_) {   // the statistics stay on the device; the host bookkeeping needs the counts
+        std::vector<int64_t> cnt(3 * (size_t)n);
+        DPMM_TRY(dpmm_statistics_counts(ctx_, n, indices.data(), cnt.data()));
+        for (int q = 0; q < n; ++q) {
+            Splittable& sc = clusters_[indices[q]];
+            sc.c.stats.N = cnt[3 * (size_t)q];
+            sc.l.stats.N = cnt[3 * (size_t)q + 1];
+            sc.r.stats.N = cnt[3 * (size_t)q + 2];
+            sc.points_count = sc.c.stats.N;
+        }
+        return DPMM_OK;
+    }
     const int D = D_;
     const bool gauss = cfg_.prior == DPMM_PRIOR_GAUSSIAN;
     std::vector<int64_t> cnt(3 * (size_t)n);
@@ -463,9 +482,17 @@ void Sampler::sample_cluster_params_all()
 }
 
 // local_clusters_actions::sample_clusters (local_clusters_actions.cpp:341-371)
-void Sampler::sample_clusters()
+dpmm_status Sampler::sample_clusters()
 {
+    if (dev_) return sample_clusters_device();
     sample_cluster_params_all();
+    mixture_weights();
+    return DPMM_OK;
+}
+
+// the cluster weights: Dir(N_1 .. N_K, alpha) without its last entry (local_clusters_actions.cpp:341-371)
+void Sampler::mixture_weights()
+{
     std::vector<double> pc;
     for (size_t i = 0; i < clusters_.size(); ++i) {
         if (cfg_.outlier_mod > 0 && i == 1) continue;
@@ -478,6 +505,44 @@ void Sampler::sample_clusters()
     weights_.clear();
     for (size_t i = 0; i + 1 < d.size(); ++i) weights_.push_back(d[i] * (1 - cfg_.outlier_mod));
     if (cfg_.outlier_mod > 0) weights_.insert(weights_.begin(), cfg_.outlier_mod);
+}
+
+// sample_clusters with the NIW draws on the device: the host draws the Dirichlet weights (same
+// generator order as the host path: sub-cluster weights cluster by cluster, then the mixture
+// weights), the device draws every slot's parameters into the label-phase buffers and returns each
+// slot's log marginal likelihood for the splittable history (shared_actions.cpp:30-54)
+dpmm_status Sampler::sample_clusters_device()
+{
+    const int K = (int)clusters_.size();
+    std::vector<double> lrw(2 * (size_t)K);
+    for (int i = 0; i < K; ++i) {
+        Splittable& sc = clusters_[i];
+        std::vector<double> w = dirichlet({(double)sc.l.stats.N + cfg_.alpha / 2, (double)sc.r.stats.N + cfg_.alpha / 2});
+        sc.lrw[0] = w[0];
+        sc.lrw[1] = w[1];
+        lrw[2 * i] = w[0];
+        lrw[2 * i + 1] = w[1];
+    }
+    mixture_weights();
+    std::vector<double> w(K, 0.0), lml(3 * (size_t)K);
+    for (int k = 0; k < K && k < (int)weights_.size(); ++k) w[k] = weights_[k];
+    DPMM_TRY(dpmm_sample_gaussian_params(ctx_, K, cfg_.seed, draw_ctr_, w.data(), lrw.data(), lml.data()));
+    draw_ctr_ += 3 * (uint64_t)K;
+    const int B = cfg_.burnout;
+    for (int i = 0; i < K; ++i) {
+        Splittable& sc = clusters_[i];
+        for (int q = 0; q < B - 1; ++q) sc.hist[q] = sc.hist[q + 1];
+        sc.hist[B - 1] = std::make_pair(true, lml[3 * (size_t)i + 1] + lml[3 * (size_t)i + 2]);
+        double now = 0.0;
+        bool ready = true;
+        for (int q = 0; q < B; ++q) {
+            if (sc.hist[q].first) now += sc.hist[q].second * (1 / (B - 0.1));
+            else ready = false;
+        }
+        if (ready && now - sc.hist[B - 1].second < 1e-2) sc.splittable = true;
+        sc.points_count = sc.c.stats.N;
+    }
+    return DPMM_OK;
 }
 
 // local_clusters_actions::reset_bad_clusters (local_clusters_actions.cpp:429-447)
@@ -587,9 +652,11 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
         auto make = [&](const ClusterParams& p, Splittable& out) {   // create_splittable_from_params
             out.l = p;
             out.r = p;
-            std::mt19937_64 g1 = draw_gen(draw_ctr_++), g2 = draw_gen(draw_ctr_++);
-            out.l.dist = sample(p.post, g1);
-            out.r.dist = sample(p.post, g2);
+            if (!dev_) {   // (device mode: every slot is drawn on the device before the next label phase)
+                std::mt19937_64 g1 = draw_gen(draw_ctr_++), g2 = draw_gen(draw_ctr_++);
+                out.l.dist = sample(p.post, g1);
+                out.r.dist = sample(p.post, g2);
+            }
             std::vector<double> w = dirichlet({cfg_.alpha / 2, cfg_.alpha / 2});
             out.lrw[0] = w[0];
             out.lrw[1] = w[1];
@@ -699,7 +766,7 @@ dpmm_status Sampler::check_and_merge(bool final_)
         }
         // merge_clusters_to_splittable(a, b.c) then local bookkeeping
         a.c.stats = aggregate(a.c.stats, b.c.stats);
-        a.c.post = posterior(a.c.prior, a.c.stats);
+        if (!dev_) a.c.post = posterior(a.c.prior, a.c.stats);
         std::vector<double> w = dirichlet({(double)a.c.stats.N + cfg_.alpha / 2, (double)b.c.stats.N + cfg_.alpha / 2});
         a.lrw[0] = w[0];
         a.lrw[1] = w[1];
@@ -715,7 +782,9 @@ dpmm_status Sampler::check_and_merge(bool final_)
         nidx.push_back(j);
     }
     if (idx.empty()) return DPMM_OK;
-    return dpmm_merge_clusters(ctx_, (int)idx.size(), idx.data(), nidx.data());
+    DPMM_TRY(dpmm_merge_clusters(ctx_, (int)idx.size(), idx.data(), nidx.data()));
+    if (dev_) DPMM_TRY(dpmm_merge_statistics(ctx_, (int)idx.size(), idx.data(), nidx.data()));
+    return DPMM_OK;
 }
 
 // features + exact ratio of every loggable candidate row (DPMM_SCREEN_LOG)
@@ -751,7 +820,7 @@ void Sampler::screen_judge()
 dpmm_status Sampler::remove_empty_clusters()
 {
     std::vector<Splittable> keep;
-    std::vector<int32_t> limits;
+    std::vector<int32_t> limits, kept;
     int removed = 0;
     const size_t K = clusters_.size();
     for (size_t i = 0; i < K; ++i) {
@@ -760,19 +829,23 @@ dpmm_status Sampler::remove_empty_clusters()
             limits.push_back((int32_t)(i - removed + 1));
             ++removed;
         }
-        if (pc > 0 || (cfg_.outlier_mod > 0 && i == 0) || (cfg_.outlier_mod > 0 && i == 1 && K == 2))
+        if (pc > 0 || (cfg_.outlier_mod > 0 && i == 0) || (cfg_.outlier_mod > 0 && i == 1 && K == 2)) {
             keep.push_back(std::move(clusters_[i]));
+            kept.push_back((int32_t)i);
+        }
     }
     clusters_ = std::move(keep);
     if (limits.empty()) return DPMM_OK;
-    return dpmm_remove_empty_clusters(ctx_, (int)limits.size(), limits.data());
+    DPMM_TRY(dpmm_remove_empty_clusters(ctx_, (int)limits.size(), limits.data()));
+    if (dev_) DPMM_TRY(dpmm_compact_statistics(ctx_, (int)kept.size(), kept.data()));
+    return DPMM_OK;
 }
 
 // local_clusters_actions::group_step (local_clusters_actions.cpp:460-490)
 dpmm_status Sampler::group_step(bool no_more_splits, bool final_)
 {
-    sample_clusters();
-    DPMM_TRY(upload_params(weights_));
+    DPMM_TRY(sample_clusters());
+    if (!dev_) DPMM_TRY(upload_params(weights_));
     const int K = (int)clusters_.size();
     DPMM_TRY(dpmm_create_clusters_labels(ctx_, K, final_ ? 1 : 0, nullptr, nullptr));
     DPMM_TRY(dpmm_create_subclusters_labels(ctx_, K, nullptr, nullptr));
@@ -840,20 +913,27 @@ dpmm_status Sampler::init_first_clusters()
     std::vector<int32_t> all(clusters_.size());
     std::iota(all.begin(), all.end(), 0);
     DPMM_TRY(update_suff_stats_posterior(all));
-    sample_clusters();
-    return DPMM_OK;
+    return sample_clusters();
 }
 
-// dp_parallel_sampling_class::calculate_posterior (dp_parallel_sampling.cpp:218-236)
-double Sampler::calculate_posterior() const
+// dp_parallel_sampling_class::calculate_posterior (dp_parallel_sampling.cpp:218-236); with device
+// draws the clusters' marginal likelihoods come from the device statistics
+dpmm_status Sampler::calculate_posterior(double* out)
 {
     double lp = std::lgamma(cfg_.alpha) - std::lgamma((double)N_ + cfg_.alpha);
-    for (const Splittable& sc : clusters_) {
+    std::vector<double> dl;
+    if (dev_ && !clusters_.empty()) {
+        dl.resize(3 * clusters_.size());
+        DPMM_TRY(slot_lml_as_is(ctx_, (int)clusters_.size(), dl.data()));
+    }
+    for (size_t k = 0; k < clusters_.size(); ++k) {
+        const Splittable& sc = clusters_[k];
         if (sc.c.stats.N == 0) continue;
-        lp += lml(sc.c.prior, sc.c.post, sc.c.stats);
+        lp += dev_ ? dl[3 * k] : lml(sc.c.prior, sc.c.post, sc.c.stats);
         lp += std::log(cfg_.alpha) + std::lgamma((double)sc.c.stats.N);
     }
-    return lp;
+    *out = lp;
+    return DPMM_OK;
 }
 
 // NMI = 2 I(X;Y) / (H(X) + H(Y)) (dp_parallel_sampling.cpp:171-179)
@@ -899,7 +979,9 @@ dpmm_status Sampler::step(int n, dpmm_model_info* mi)
         mi->iter_count.push_back(std::chrono::duration<double>(t1 - t0).count());
         mi->cluster_count_history.push_back((int32_t)clusters_.size());
         if (cfg_.verbose) {
-            mi->likelihood_history.push_back(calculate_posterior());
+            double lp = 0;
+            DPMM_TRY(calculate_posterior(&lp));
+            mi->likelihood_history.push_back(lp);
             if (!cfg_.gt.empty()) {
                 std::vector<int32_t> lab(N_);
                 DPMM_TRY(dpmm_get_labels(ctx_, lab.data()));
@@ -1082,6 +1164,7 @@ static void screen_from_run(const dpmm_run_desc* run, host::Config& cfg)
     cfg.screen_sweep = run->screen_sweep_every > 0 ? run->screen_sweep_every : 10;
     cfg.screen_min_recall = run->screen_min_recall > 0 ? run->screen_min_recall : 0.5;
     cfg.screen_split_min = run->screen_split_min > 0 ? run->screen_split_min : 256;
+    cfg.host_param_draws = run->host_param_draws != 0;
     if (run->screen_params) cfg.screen_params.assign(run->screen_params, run->screen_params + kScrParams);
 }
 

@@ -289,6 +289,32 @@ dpmm_status dpmm_screen_train(const float* features, const float* targets, int64
                               int32_t batch, float lr, uint64_t seed, float* params, float* epoch_loss,
                               int32_t device);
 
+/* ---- cluster parameter draws on the device (NIW prior, D <= 64) -------------------------------
+ * shared_actions::sample_cluster_params (shared_actions.cpp:9-55) with niw::sample_distribution
+ * (niw.cpp:82-107) for the cluster and both sub-clusters of each of the K clusters, from the
+ * statistics on the device (as the statistics phase, dpmm_merge_statistics and
+ * dpmm_compact_statistics leave them); the draws become the label / sub-label parameters directly
+ * (what dpmm_set_gaussian_factors would upload).  weights[K]: mixture weights; lr_weights[2K]: the
+ * sub-cluster weights; (seed, draw): the Philox stream of this draw; lml (nullable, 3K): each slot's
+ * log marginal likelihood (niw.cpp:122-138).  A posterior that is not positive definite gives
+ * DPMM_ERR_NOT_PD. */
+dpmm_status dpmm_sample_gaussian_params(dpmm_ctx* ctx, int K, uint64_t seed, uint64_t draw, const double* weights,
+                                        const double* lr_weights, double* lml);
+/* merge_clusters_to_splittable (shared_actions.cpp:72-86) applied to the device statistics for each
+ * (disjoint) pair: cluster index[t] and its l sub-cluster take c_i + c_j, its r sub-cluster c_j. */
+dpmm_status dpmm_merge_statistics(dpmm_ctx* ctx, int n, const int32_t* index, const int32_t* new_index);
+/* the slot compaction of remove_empty_clusters (local_clusters_actions.cpp:384-419): cluster k takes
+ * the statistics of cluster keep[k] (increasing indices) */
+dpmm_status dpmm_compact_statistics(dpmm_ctx* ctx, int n_keep, const int32_t* keep);
+/* counts of the listed clusters' three slots (as dpmm_create_sufficient_statistics, counts only) */
+dpmm_status dpmm_statistics_counts(dpmm_ctx* ctx, int n, const int32_t* indices, int64_t* count);
+/* Test seam (no counterpart in the reference): the label-phase parameters of the 3K slots as they are
+ * on the device, FP32, with the padded dimension Dp (the next power of two >= max(D, 4)):
+ * wt[3K][Dp][Dp] (wt[s][j][i] = W(i, j)), b[3K][Dp] = W^T (mu - shift), c[3K] = -log det Sigma / 2
+ * (+ log w for cluster slots), mu[3K][Dp] = mu - shift, where shift is the data mean the points are
+ * stored relative to.  Any output may be NULL. */
+dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, float* c, float* mu);
+
 /* Synchronise the context's stream; returns any pending device error. */
 dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
@@ -340,7 +366,9 @@ typedef struct dpmm_run_desc {
     const float* screen_params;  /* DPMM_SCREEN_PARAMS floats; required by DPMM_SCREEN_ON */
     int32_t screen_split_min;    /* split candidates are screened only above this many (0 -> 256): the
                                     exact split ratios of K clusters cost one launch of 3K blocks */
-    int32_t reserved[3];
+    int32_t host_param_draws;    /* nonzero: draw the cluster parameters on the host (FP64, OpenMP) even
+                                    where the device draws them (NIW prior, D <= 64, no outlier cluster) */
+    int32_t reserved[2];
 } dpmm_run_desc;
 
 typedef enum dpmm_screen_mode {
