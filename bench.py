@@ -257,6 +257,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-points-per-core", type=int, default=600)
+    ap.add_argument("--workload", default="c5", choices=["c5", "c4"],
+                    help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time")
+    ap.add_argument("--c4-sets", type=int, default=256)
+    ap.add_argument("--c4-seq-sets", type=int, default=32, help="data sets timed one at a time (a subset)")
     args = ap.parse_args()
     assert args.warmup >= 0 and args.steps >= 1
 
@@ -265,6 +269,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.workload == "c4":
+        return run_c4(args, rank, world, local)
 
     import numpy as np
     import torch
@@ -458,6 +464,77 @@ def run_e2e(args, cfg, rank, local, world, dist, L, make_run):
             "iterations": iters, "wall_s": dt,
             "note": "dpmm_dp_parallel from host float64 points: upload, init, all iterations and label "
                     "download in the timed region"}
+
+
+def c4_data(n_sets, seed):
+    """Seeded synthetic data sets of the batched-uneven shape: N ~ logUniform[1e3, 2e5], D from
+    {2, 8, 16, 64}, true K ~ Uniform{2..30}, means U(-10, 10)^D, covariances A A^T / D + 0.5 I."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_sets):
+        N = int(round(math.exp(rng.uniform(math.log(1e3), math.log(2e5)))))
+        D = int(rng.choice([2, 8, 16, 64]))
+        K = int(rng.integers(2, 31))
+        mus = rng.uniform(-10, 10, size=(K, D))
+        z = rng.integers(0, K, size=N)
+        x = np.empty((N, D))
+        for c in range(K):
+            idx = np.flatnonzero(z == c)
+            A = rng.normal(size=(D, D))
+            L = np.linalg.cholesky(A @ A.T / D + 0.5 * np.eye(D))
+            x[idx] = mus[c] + rng.normal(size=(idx.size, D)) @ L.T
+        out.append((x.astype(np.float32).astype(np.float64).T.copy(), z))
+    return out
+
+
+def run_c4(args, rank, world, local):
+    """Batched uneven data sets: all data sets advanced together by BatchSampler (one label launch per
+    padded dimension per iteration, CUDA-graph replayed) vs a subset of the same data sets run one at a
+    time through dp_parallel; throughput = sum of N x iterations / wall time of the sampler loop."""
+    import numpy as np
+    import torch
+    from dpmmsubclusters_gpu_b200 import BatchSampler, capi, niw_hyperparams, prior_type
+    from dpmmsubclusters_gpu_b200.api import dp_parallel_sampling_class
+    torch.cuda.set_device(local)
+    iters = 100
+    data = c4_data(args.c4_sets, 1004 + rank)
+    hyp = [niw_hyperparams(1.0, np.zeros(x.shape[0]), x.shape[0] + 3.0, np.eye(x.shape[0])) for x, _ in data]
+    npts = np.array([x.shape[1] for x, _ in data], dtype=np.float64)
+    b = BatchSampler([x for x, _ in data], hyp, 5.0, iters=iters, init_clusters=1, burnout=15, k_max=64,
+                     device=local)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(iters)
+    torch.cuda.synchronize()
+    t_batch = time.perf_counter() - t0
+    info = b.info()
+    nmis = [_nmi(b.model_info(i).labels, z) for i, (_, z) in enumerate(data)]
+    b.close()
+    m = min(args.c4_seq_sets, len(data))
+    t0 = time.perf_counter()
+    for i in range(m):
+        x = data[i][0]
+        s = dp_parallel_sampling_class(x.shape[1], x, 1 + i, prior_type.Gaussian, loglik_mode=capi.LL_FP32,
+                                       k_max=64, device=local)
+        s.dp_parallel(hyp[i], 5.0, iters=iters, init_clusters=1, verbose=False, burnout=15)
+    torch.cuda.synchronize()
+    t_seq = time.perf_counter() - t0
+    line = {"metric": "batched uneven data sets: points*iters/sec (all data sets advanced together)",
+            "value": float(npts.sum() * iters / t_batch), "unit": UNIT, "n_gpus": world, "steps": iters,
+            "warmup": 0, "ms_per_step": t_batch / iters * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded, host)",
+            "config": {"workload": "C4: %d data sets, N ~ logU[1e3, 2e5], D in {2, 8, 16, 64}, K* ~ U{2..30}, "
+                                   "NIW k=1 m=0 nu=D+3 Psi=I, alpha=5, %d iterations" % (len(data), iters),
+                       "total_points": int(npts.sum()), "batch_info": info,
+                       "nmi_mean": float(np.mean(nmis)), "nmi_min": float(np.min(nmis)),
+                       "timing": "wall clock around the sampler loop (setup and data upload excluded)"},
+            "one_at_a_time": {"data_sets": m, "value": float(npts[:m].sum() * iters / t_seq), "unit": UNIT,
+                              "wall_s": t_seq},
+            "batch_wall_s": t_batch}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
 
 
 def screen_summary(flag, st):

@@ -7,11 +7,11 @@ reference's iteration semantics.  This package mirrors the reference's API
 (dp_parallel_sampling_class, niw_hyperparams, multinomial_hyper, ModelInfo, prior_type) and
 exposes the device back-end (CudaKernel) for kernel-level use.
 """
-from .api import (DBL_MAX, CudaKernel, ModelInfo, dp_parallel_sampling_class, multinomial_hyper,  # noqa: F401
-                  niw_hyperparams, prior_type)
+from .api import (DBL_MAX, BatchSampler, CudaKernel, ModelInfo, dp_parallel_sampling_class,  # noqa: F401
+                  multinomial_hyper, niw_hyperparams, prior_type)
 from .capi import (LL_AUTO, LL_FP32, LL_TC_BF16X3, RNG_CURAND_XORWOW, RNG_PHILOX, DpmmError,  # noqa: F401
                    lib)
 
-__all__ = ["CudaKernel", "ModelInfo", "dp_parallel_sampling_class", "multinomial_hyper", "niw_hyperparams",
+__all__ = ["BatchSampler", "CudaKernel", "ModelInfo", "dp_parallel_sampling_class", "multinomial_hyper", "niw_hyperparams",
            "prior_type", "DpmmError", "lib", "LL_AUTO", "LL_FP32", "LL_TC_BF16X3", "RNG_PHILOX",
            "RNG_CURAND_XORWOW", "DBL_MAX"]

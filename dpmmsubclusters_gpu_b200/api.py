@@ -521,3 +521,67 @@ class CudaKernel:
 
     def synchronize(self):
         check(lib().dpmm_synchronize(self.ctx))
+
+
+class BatchSampler:
+    """Many independent samplers advanced together (dpmm_batch_* of the C ABI; no counterpart in the
+    reference, which runs one sampler per process).  datasets: list of D x N matrices (reference
+    layout); hypers: one niw_hyperparams per data set (or one for all); every data set runs `iters`
+    iterations with the same alpha / init_clusters / burnout; seeds: per data set (default 1 + index)."""
+
+    def __init__(self, datasets, hypers, alpha: float, iters: int = 100, init_clusters: int = 1, burnout: int = 15,
+                 seeds=None, k_max: int = 64, device: int = 0):
+        B = len(datasets)
+        self._keep = []
+        runs = (capi.dpmm_run_desc * B)()
+        pts = (ctypes.POINTER(c_double) * B)()
+        n = np.empty(B, np.int64)
+        d = np.empty(B, np.int32)
+        for i, x in enumerate(datasets):
+            xp = _points_major(x)
+            h = hypers[i] if isinstance(hypers, (list, tuple)) else hypers
+            m, psi = np.ascontiguousarray(h.m), np.ascontiguousarray(h.psi.T)
+            self._keep += [xp, m, psi]
+            r = runs[i]
+            r.prior_type = capi.PRIOR_GAUSSIAN
+            r.iterations, r.initial_clusters, r.burnout = iters, init_clusters, burnout
+            r.alpha = alpha
+            r.seed = int(seeds[i]) if seeds is not None else 1 + i
+            r.loglik_mode, r.rng_kind, r.k_max, r.device = capi.LL_FP32, capi.RNG_PHILOX, k_max, device
+            r.niw_k, r.niw_v, r.niw_m, r.niw_psi = h.k, h.v, _dptr(m), _dptr(psi)
+            pts[i] = _dptr(xp)
+            n[i], d[i] = xp.shape
+        self._n = n
+        self.h = c_void_p()
+        check(lib().dpmm_batch_create(B, runs, n.ctypes.data_as(ctypes.POINTER(c_int64)),
+                                      d.ctypes.data_as(ctypes.POINTER(c_int32)), pts, byref(self.h)))
+        self.count = B
+
+    def step(self, n_iters: int):
+        check(lib().dpmm_batch_step(self.h, n_iters))
+
+    def info(self) -> dict:
+        out = np.zeros(10, np.int64)
+        check(lib().dpmm_batch_info(self.h, out.ctypes.data_as(ctypes.POINTER(c_int64))))
+        return {"data_sets": int(out[0]), "groups": int(out[1]), "batched_label_launches": int(out[2]),
+                "graph_launches": int(out[3]),
+                "block_size_by_padded_dim": {dp: int(v) for dp, v in zip((4, 8, 16, 32, 64, 128), out[4:]) if v}}
+
+    def model_info(self, i: int) -> ModelInfo:
+        h = c_void_p()
+        check(lib().dpmm_batch_model_info(self.h, i, byref(h)))
+        try:
+            return ModelInfo._from_handle(h)
+        finally:
+            lib().dpmm_model_info_free(h)
+
+    def close(self):
+        if self.h:
+            lib().dpmm_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

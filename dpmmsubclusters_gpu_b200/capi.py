@@ -138,6 +138,11 @@ SIGNATURES = {
     "dpmm_compact_statistics": (c_int, [_CTX, c_int, _PI32]),
     "dpmm_statistics_counts": (c_int, [_CTX, c_int, _PI32, _PI64]),
     "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
+    "dpmm_batch_create": (c_int, [c_int32, POINTER(dpmm_run_desc), _PI64, _PI32, POINTER(_PD), POINTER(c_void_p)]),
+    "dpmm_batch_step": (c_int, [c_void_p, c_int32]),
+    "dpmm_batch_info": (c_int, [c_void_p, _PI64]),
+    "dpmm_batch_model_info": (c_int, [c_void_p, c_int32, POINTER(c_void_p)]),
+    "dpmm_batch_destroy": (c_int, [c_void_p]),
 }
 
 _lib = None

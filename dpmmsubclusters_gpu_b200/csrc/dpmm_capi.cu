@@ -610,6 +610,28 @@ static dpmm_status check_ready(dpmm_ctx* c, int K)
     return DPMM_OK;
 }
 
+namespace dpmm {
+// The label phase of one context as a job of a batched launch (launch_labels_batched): the same
+// checks and random stream as dpmm_create_clusters_labels with device uniforms, SIMT FP32 form.
+dpmm_status make_label_job(dpmm_ctx* c, int K, int final_, LabelJob* job)
+{
+    DPMM_TRY(check_ready(c, K));
+    if (c->prior != DPMM_PRIOR_GAUSSIAN) return fail(DPMM_ERR_INVALID_ARG, "batched label phase: NIW prior only");
+    job->x = c->d_x;
+    job->N = c->N;
+    job->Wt = c->d_Wt;
+    job->b = c->d_b;
+    job->c = c->d_c;
+    job->K = K;
+    job->final_ = final_;
+    job->rng = rng_args(c, nullptr);
+    job->labels = c->d_labels;
+    c->perm_K = -1;
+    invalidate_stats(c);
+    return DPMM_OK;
+}
+}  // namespace dpmm
+
 extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final_, const float* u, float* loglik_out)
 {
     DPMM_TRY(check_ready(c, K));

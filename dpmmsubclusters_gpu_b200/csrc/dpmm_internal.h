@@ -240,7 +240,27 @@ struct KernelTimer {
 }  // namespace dpmm
 
 namespace dpmm {
+// One data set's share of a batched label phase (see launch_labels_batched)
+struct LabelJob {
+    const float* x;
+    int64_t N;
+    const float* Wt;
+    const float* b;
+    const float* c;
+    int K;
+    int final_;
+    RngArgs rng;
+    int32_t* labels;
+};
+
 // kernel launchers (dpmm_kernels.cu)
+// label phase of several Gaussian data sets of padded dimension Dp in one launch: nitems blocks of
+// P points, item (job, block); kmax: the largest K of the jobs
+dpmm_status launch_labels_batched(int Dp, int P, const LabelJob* d_jobs, const int2* d_items, int nitems, int kmax,
+                                  cudaStream_t st);
+size_t gauss_label_smem_bytes(int DP, int P, int K);
+// a context's label phase as a batch job (dpmm_capi.cu)
+dpmm_status make_label_job(dpmm_ctx* c, int K, int final_, LabelJob* job);
 dpmm_status launch_init_curand(dpmm_ctx* c);
 dpmm_status launch_labels_init(dpmm_ctx* c, int initial_clusters, double outlier_mod, const float* d_u);
 dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u);

@@ -114,20 +114,20 @@ __device__ __forceinline__ int draw_from_r(float* sr, int p, int K, int final_, 
 // Gaussian label phase, FP32 SIMT: one thread per point, x in registers, each cluster's
 // precision factor (transposed) broadcast from shared memory.
 //   z_j = sum_i W(i,j) x_i - b_j,   r_k = c_k - 0.5 * sum_j z_j^2
+// one block of P points starting at pt0 (the body of k_gauss_labels_simt and of its batched form)
 template <int DP, int P>
-__global__ void __launch_bounds__(P) k_gauss_labels_simt(
-    const float* __restrict__ x, int64_t N, const float* __restrict__ Wt, const float* __restrict__ bvec,
-    const float* __restrict__ cvec, int K, int final_, RngArgs rng, int32_t* __restrict__ labels,
-    float* __restrict__ r_out)
+__device__ __forceinline__ void gauss_labels_tile(const float* __restrict__ x, int64_t N,
+                                                  const float* __restrict__ Wt, const float* __restrict__ bvec,
+                                                  const float* __restrict__ cvec, int K, int final_,
+                                                  const RngArgs& rng, int32_t* __restrict__ labels,
+                                                  float* __restrict__ r_out, int64_t pt0, unsigned char* smem)
 {
-    extern __shared__ __align__(16) unsigned char smem[];
     float* sW = reinterpret_cast<float*>(smem);          // DP*DP
     float* sbv = sW + DP * DP;                            // DP
     float* sx = sbv + DP;                                 // P*(DP+1)
     float* sr = sx + P * (DP + 1);                        // K*P
 
     const int p = threadIdx.x;
-    const int64_t pt0 = (int64_t)blockIdx.x * P;
     const int64_t pt = pt0 + p;
     const bool valid = pt < N;
 
@@ -179,6 +179,73 @@ __global__ void __launch_bounds__(P) k_gauss_labels_simt(
     }
     if (!valid) return;
     labels[pt] = draw_from_r<P>(sr, p, K, final_, rng, pt);
+}
+
+template <int DP, int P>
+__global__ void __launch_bounds__(P) k_gauss_labels_simt(
+    const float* __restrict__ x, int64_t N, const float* __restrict__ Wt, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, int K, int final_, RngArgs rng, int32_t* __restrict__ labels,
+    float* __restrict__ r_out)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    gauss_labels_tile<DP, P>(x, N, Wt, bvec, cvec, K, final_, rng, labels, r_out, (int64_t)blockIdx.x * P, smem);
+}
+
+// Batched form: one launch for many data sets of the same padded dimension.  Block b works on
+// item items[b] = (data set, block of P points of it); the data set's buffers, K, mode and random
+// stream come from its descriptor.  Shared memory is sized for the largest K of the batch.
+template <int DP, int P>
+__global__ void __launch_bounds__(P) k_gauss_labels_batched(const LabelJob* __restrict__ jobs,
+                                                            const int2* __restrict__ items)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int2 it = items[blockIdx.x];
+    const LabelJob& j = jobs[it.x];
+    gauss_labels_tile<DP, P>(j.x, j.N, j.Wt, j.b, j.c, j.K, j.final_, j.rng, j.labels, nullptr, (int64_t)it.y * P,
+                             smem);
+}
+
+size_t gauss_label_smem_bytes(int DP, int P, int K)
+{
+    return sizeof(float) * (DP * DP + DP + P * (DP + 1) + (size_t)K * P);
+}
+
+template <int DP, int P>
+static dpmm_status launch_labels_batched_t(const LabelJob* d_jobs, const int2* d_items, int nitems, int kmax,
+                                           cudaStream_t st)
+{
+    const size_t sm = gauss_label_smem_bytes(DP, P, kmax);
+    if (sm > 220 * 1024) return fail(DPMM_ERR_INVALID_ARG, "too many clusters for the batched label kernel");
+    auto kern = k_gauss_labels_batched<DP, P>;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<nitems, P, sm, st>>>(d_jobs, d_items);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+template <int DP>
+static dpmm_status launch_labels_batched_dp(int P, const LabelJob* d_jobs, const int2* d_items, int nitems, int kmax,
+                                            cudaStream_t st)
+{
+    switch (P) {
+        case 32: return launch_labels_batched_t<DP, 32>(d_jobs, d_items, nitems, kmax, st);
+        case 64: return launch_labels_batched_t<DP, 64>(d_jobs, d_items, nitems, kmax, st);
+        default: return launch_labels_batched_t<DP, 128>(d_jobs, d_items, nitems, kmax, st);
+    }
+}
+
+dpmm_status launch_labels_batched(int Dp, int P, const LabelJob* d_jobs, const int2* d_items, int nitems, int kmax,
+                                  cudaStream_t st)
+{
+    switch (Dp) {
+        case 4: return launch_labels_batched_dp<4>(P, d_jobs, d_items, nitems, kmax, st);
+        case 8: return launch_labels_batched_dp<8>(P, d_jobs, d_items, nitems, kmax, st);
+        case 16: return launch_labels_batched_dp<16>(P, d_jobs, d_items, nitems, kmax, st);
+        case 32: return launch_labels_batched_dp<32>(P, d_jobs, d_items, nitems, kmax, st);
+        case 64: return launch_labels_batched_dp<64>(P, d_jobs, d_items, nitems, kmax, st);
+        case 128: return launch_labels_batched_dp<128>(P, d_jobs, d_items, nitems, kmax, st);
+        default: return fail(DPMM_ERR_INVALID_ARG, "unsupported padded dimension");
+    }
 }
 
 // Multinomial label phase, FP32 SIMT: tiled dot products r[p][k] = sum_d x[p][d] * logtheta[k][d]

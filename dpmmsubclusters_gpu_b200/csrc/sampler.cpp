@@ -107,6 +107,19 @@ public:
     dpmm_status step(int n, dpmm_model_info* mi);
     dpmm_status finish(dpmm_model_info* mi);
     int num_clusters() const { return (int)clusters_.size(); }
+    bool running() const { return iter_ < cfg_.iterations; }
+    dpmm_ctx* context() const { return ctx_; }
+
+    // one iteration in stages, for drivers that run the label phase of many samplers together
+    struct IterState {
+        int i = 0;
+        bool final_ = false, no_more_splits = false;
+        std::chrono::steady_clock::time_point t0;
+    };
+    IterState begin_iteration();
+    dpmm_status stage_params();
+    dpmm_status stage_rest(bool no_more_splits, bool final_);
+    dpmm_status end_iteration(const IterState& st, dpmm_model_info* mi);
     const ScreenRecord& screen_record() const { return scr_; }
     int iteration() const { return iter_; }
 
@@ -844,10 +857,23 @@ dpmm_status Sampler::remove_empty_clusters()
 // local_clusters_actions::group_step (local_clusters_actions.cpp:460-490)
 dpmm_status Sampler::group_step(bool no_more_splits, bool final_)
 {
+    DPMM_TRY(stage_params());
+    DPMM_TRY(dpmm_create_clusters_labels(ctx_, (int)clusters_.size(), final_ ? 1 : 0, nullptr, nullptr));
+    return stage_rest(no_more_splits, final_);
+}
+
+// the stages of group_step: parameters for the label phase ...
+dpmm_status Sampler::stage_params()
+{
     DPMM_TRY(sample_clusters());
     if (!dev_) DPMM_TRY(upload_params(weights_));
+    return DPMM_OK;
+}
+
+// ... and everything after it (sub-labels, statistics, reset, split, merge, compaction)
+dpmm_status Sampler::stage_rest(bool no_more_splits, bool final_)
+{
     const int K = (int)clusters_.size();
-    DPMM_TRY(dpmm_create_clusters_labels(ctx_, K, final_ ? 1 : 0, nullptr, nullptr));
     DPMM_TRY(dpmm_create_subclusters_labels(ctx_, K, nullptr, nullptr));
     std::vector<int32_t> all(K);
     std::iota(all.begin(), all.end(), 0);
@@ -969,14 +995,32 @@ dpmm_status Sampler::step(int n, dpmm_model_info* mi)
 {
     mi->n = N_;
     for (int q = 0; q < n && iter_ < cfg_.iterations; ++q) {
-        const int i = ++iter_;
-        const bool final_ = i >= cfg_.iterations - cfg_.argmax_sample_stop;
-        const bool no_more_splits =
-            i >= cfg_.iterations - cfg_.split_stop || (double)clusters_.size() >= cfg_.max_clusters;
-        auto t0 = std::chrono::steady_clock::now();
-        DPMM_TRY(group_step(no_more_splits, final_));
+        IterState st = begin_iteration();
+        DPMM_TRY(group_step(st.no_more_splits, st.final_));
+        DPMM_TRY(end_iteration(st, mi));
+    }
+    return DPMM_OK;
+}
+
+// the loop head of run_model (dp_parallel_sampling.cpp:139-150)
+Sampler::IterState Sampler::begin_iteration()
+{
+    IterState st;
+    st.i = ++iter_;
+    st.final_ = st.i >= cfg_.iterations - cfg_.argmax_sample_stop;
+    st.no_more_splits = st.i >= cfg_.iterations - cfg_.split_stop || (double)clusters_.size() >= cfg_.max_clusters;
+    st.t0 = std::chrono::steady_clock::now();
+    return st;
+}
+
+// the loop tail: iteration time, histories, verbose line (dp_parallel_sampling.cpp:151-200)
+dpmm_status Sampler::end_iteration(const IterState& st, dpmm_model_info* mi)
+{
+    mi->n = N_;
+    const int i = st.i;
+    {
         auto t1 = std::chrono::steady_clock::now();
-        mi->iter_count.push_back(std::chrono::duration<double>(t1 - t0).count());
+        mi->iter_count.push_back(std::chrono::duration<double>(t1 - st.t0).count());
         mi->cluster_count_history.push_back((int32_t)clusters_.size());
         if (cfg_.verbose) {
             double lp = 0;
@@ -1366,3 +1410,285 @@ extern "C" const int32_t* dpmm_model_info_screen_log_iter(const dpmm_model_info*
 }
 
 extern "C" void dpmm_model_info_free(dpmm_model_info* mi) { delete mi; }
+
+// ============================================================================== batches of samplers
+// Many independent samplers (data sets of uneven N, D and K) advanced together, one iteration at a
+// time: the host stages of all samplers run on a thread pool, and the label phase of every NIW data
+// set of a padded dimension is ONE launch over a work list of (data set, block of points) items,
+// replayed from a CUDA graph; the points per block are chosen per padded dimension by timing the
+// candidates on the first iteration.  The reference can run one sampler per process only (its init
+// calls cudaDeviceReset, cudaKernel.cu:615).
+struct dpmm_batch {
+    struct Group {
+        int Dp = 0, kcap = 0, P = 0;
+        std::vector<int> members;          // sampler indices
+        std::vector<int> graph_members;    // the members the captured graph covers
+        LabelJob* h_jobs = nullptr;        // pinned
+        LabelJob* d_jobs = nullptr;
+        int2* d_items = nullptr;
+        int nitems = 0;
+        cudaStream_t st = nullptr;
+        cudaEvent_t done = nullptr;
+        cudaGraphExec_t graph = nullptr;
+        float tune_ms[3] = {0, 0, 0};
+    };
+    std::vector<std::unique_ptr<dpmm::host::SamplerHandle>> s;
+    std::vector<Group> groups;
+    std::vector<int> group_of;
+    std::vector<cudaEvent_t> ready;
+    int device = 0;
+    int64_t batched_launches = 0, graph_launches = 0;
+    ~dpmm_batch()
+    {
+        cudaSetDevice(device);
+        for (Group& g : groups) {
+            if (g.st) cudaStreamSynchronize(g.st);
+            if (g.graph) cudaGraphExecDestroy(g.graph);
+            if (g.h_jobs) cudaFreeHost(g.h_jobs);
+            if (g.d_jobs) cudaFree(g.d_jobs);
+            if (g.d_items) cudaFree(g.d_items);
+            if (g.done) cudaEventDestroy(g.done);
+            if (g.st) cudaStreamDestroy(g.st);
+        }
+        for (cudaEvent_t e : ready)
+            if (e) cudaEventDestroy(e);
+        s.clear();
+    }
+};
+
+namespace dpmm {
+namespace host {
+
+static const int kBatchP[3] = {32, 64, 128};
+
+// work list of a group for P points per block: one item per (job j, block) of the members in order
+static dpmm_status batch_items(dpmm_batch& b, dpmm_batch::Group& g, const std::vector<int>& mem, int P)
+{
+    std::vector<int2> items;
+    for (size_t j = 0; j < mem.size(); ++j) {
+        const int64_t N = b.s[mem[j]]->sampler->context()->N;
+        for (int64_t blk = 0; blk * P < N; ++blk) items.push_back(make_int2((int)j, (int)blk));
+    }
+    if (g.d_items) cudaFree(g.d_items);
+    g.d_items = nullptr;
+    DPMM_CUDA_TRY(cudaMalloc(&g.d_items, sizeof(int2) * std::max<size_t>(items.size(), 1)));
+    DPMM_CUDA_TRY(cudaMemcpy(g.d_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice));
+    g.nitems = (int)items.size();
+    return DPMM_OK;
+}
+
+// the label phase of one group; its members' parameters are ready (g.st waits on their events)
+static dpmm_status batch_labels(dpmm_batch& b, dpmm_batch::Group& g, const std::vector<int>& mem,
+                                const std::vector<Sampler::IterState>& st)
+{
+    for (size_t j = 0; j < mem.size(); ++j) {
+        Sampler& sm = *b.s[mem[j]]->sampler;
+        DPMM_TRY(make_label_job(sm.context(), sm.num_clusters(), st[mem[j]].final_ ? 1 : 0, &g.h_jobs[j]));
+    }
+    const size_t jb = sizeof(LabelJob) * mem.size();
+    if (g.P == 0) {
+        // first iteration: time every block size on the live jobs (each run draws the same labels:
+        // a point's log-likelihoods and uniforms do not depend on the block size), keep the fastest
+        cudaEvent_t e0, e1;
+        DPMM_CUDA_TRY(cudaEventCreate(&e0));
+        DPMM_CUDA_TRY(cudaEventCreate(&e1));
+        DPMM_CUDA_TRY(cudaMemcpyAsync(g.d_jobs, g.h_jobs, jb, cudaMemcpyHostToDevice, g.st));
+        int best = 0;
+        for (int q = 0; q < 3; ++q) {
+            DPMM_TRY(batch_items(b, g, mem, kBatchP[q]));
+            DPMM_CUDA_TRY(cudaEventRecord(e0, g.st));
+            DPMM_TRY(launch_labels_batched(g.Dp, kBatchP[q], g.d_jobs, g.d_items, g.nitems, g.kcap, g.st));
+            DPMM_CUDA_TRY(cudaEventRecord(e1, g.st));
+            DPMM_CUDA_TRY(cudaEventSynchronize(e1));
+            DPMM_CUDA_TRY(cudaEventElapsedTime(&g.tune_ms[q], e0, e1));
+            if (g.tune_ms[q] < g.tune_ms[best]) best = q;
+            ++b.batched_launches;
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        g.P = kBatchP[best];
+        DPMM_TRY(batch_items(b, g, mem, g.P));
+        return DPMM_OK;
+    }
+    if (!g.graph || g.graph_members != mem) {
+        // (re)capture: jobs upload + the batched launch
+        if (g.graph) {
+            cudaGraphExecDestroy(g.graph);
+            g.graph = nullptr;
+        }
+        DPMM_TRY(batch_items(b, g, mem, g.P));
+        cudaGraph_t graph;
+        DPMM_CUDA_TRY(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeRelaxed));
+        cudaMemcpyAsync(g.d_jobs, g.h_jobs, jb, cudaMemcpyHostToDevice, g.st);
+        dpmm_status ls = launch_labels_batched(g.Dp, g.P, g.d_jobs, g.d_items, g.nitems, g.kcap, g.st);
+        cudaError_t ce = cudaStreamEndCapture(g.st, &graph);
+        DPMM_TRY(ls);
+        DPMM_CUDA_TRY(ce);
+        ce = cudaGraphInstantiate(&g.graph, graph, 0);
+        cudaGraphDestroy(graph);
+        DPMM_CUDA_TRY(ce);
+        g.graph_members = mem;
+    }
+    DPMM_CUDA_TRY(cudaGraphLaunch(g.graph, g.st));
+    ++b.graph_launches;
+    ++b.batched_launches;
+    return DPMM_OK;
+}
+
+static dpmm_status batch_iteration(dpmm_batch& b)
+{
+    const int n = (int)b.s.size();
+    std::vector<Sampler::IterState> st(n);
+    std::vector<uint8_t> act(n, 0);
+    for (int i = 0; i < n; ++i) act[i] = b.s[i]->sampler->running();
+    std::vector<dpmm_status> err(n, DPMM_OK);
+    std::vector<std::string> msg(n);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < n; ++i) {
+        if (!act[i]) continue;
+        Sampler& sm = *b.s[i]->sampler;
+        st[i] = sm.begin_iteration();
+        dpmm_status e = sm.stage_params();
+        if (e == DPMM_OK && b.group_of[i] < 0)   // not batched: the context's own label phase
+            e = dpmm_create_clusters_labels(sm.context(), sm.num_clusters(), st[i].final_ ? 1 : 0, nullptr, nullptr);
+        if (e == DPMM_OK && b.group_of[i] >= 0) {
+            cudaError_t ce = cudaEventRecord(b.ready[i], sm.context()->stream);
+            if (ce != cudaSuccess) e = cuda_status(ce, "cudaEventRecord");
+        }
+        if (e != DPMM_OK) {
+            err[i] = e;
+            msg[i] = dpmm_last_error();
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (err[i] != DPMM_OK) return fail(err[i], "data set " + std::to_string(i) + ": " + msg[i]);
+    for (dpmm_batch::Group& g : b.groups) {
+        std::vector<int> mem;
+        for (int m : g.members)
+            if (act[m]) mem.push_back(m);
+        if (mem.empty()) continue;
+        for (int m : mem) DPMM_CUDA_TRY(cudaStreamWaitEvent(g.st, b.ready[m], 0));
+        DPMM_TRY(batch_labels(b, g, mem, st));
+        DPMM_CUDA_TRY(cudaEventRecord(g.done, g.st));
+        for (int m : mem) DPMM_CUDA_TRY(cudaStreamWaitEvent(b.s[m]->sampler->context()->stream, g.done, 0));
+    }
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < n; ++i) {
+        if (!act[i]) continue;
+        Sampler& sm = *b.s[i]->sampler;
+        dpmm_status e = sm.stage_rest(st[i].no_more_splits, st[i].final_);
+        if (e == DPMM_OK) e = sm.end_iteration(st[i], &b.s[i]->mi);
+        if (e != DPMM_OK) {
+            err[i] = e;
+            msg[i] = dpmm_last_error();
+        }
+    }
+    for (int i = 0; i < n; ++i)
+        if (err[i] != DPMM_OK) return fail(err[i], "data set " + std::to_string(i) + ": " + msg[i]);
+    return DPMM_OK;
+}
+
+}  // namespace host
+}  // namespace dpmm
+
+extern "C" dpmm_status dpmm_batch_create(int32_t count, const dpmm_run_desc* runs, const int64_t* n, const int32_t* d,
+                                         const double* const* points, dpmm_batch** out)
+{
+    if (count < 1 || !runs || !n || !d || !points || !out) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    *out = nullptr;
+    auto b = std::make_unique<dpmm_batch>();
+    b->device = runs[0].device;
+    for (int i = 0; i < count; ++i)
+        if (runs[i].device != b->device) return fail(DPMM_ERR_INVALID_ARG, "all data sets of a batch share one device");
+    b->s.resize(count);
+    std::vector<dpmm_status> err(count, DPMM_OK);
+    std::vector<std::string> msg(count);
+#pragma omp parallel for schedule(dynamic)
+    for (int i = 0; i < count; ++i) {
+        if (n[i] <= 0 || d[i] <= 0 || !points[i]) {
+            err[i] = DPMM_ERR_INVALID_ARG;
+            msg[i] = "invalid data set";
+            continue;
+        }
+        host::Config cfg = config_from_run(&runs[i], n[i], d[i]);
+        if (cfg.prior == DPMM_PRIOR_GAUSSIAN) cfg.loglik_mode = DPMM_LL_FP32;   // the batched SIMT label kernel
+        if (cudaSetDevice(b->device) != cudaSuccess) {
+            err[i] = DPMM_ERR_NO_DEVICE;
+            continue;
+        }
+        dpmm_status e = host::make_sampler(cfg, n[i], d[i], points[i], false, b->s[i]);
+        if (e != DPMM_OK) {
+            err[i] = e;
+            msg[i] = dpmm_last_error();
+        }
+    }
+    for (int i = 0; i < count; ++i)
+        if (err[i] != DPMM_OK) return fail(err[i], "data set " + std::to_string(i) + ": " + msg[i]);
+    DPMM_CUDA_TRY(cudaSetDevice(b->device));
+    b->group_of.assign(count, -1);
+    b->ready.assign(count, nullptr);
+    for (int i = 0; i < count; ++i) {
+        dpmm_ctx* c = b->s[i]->sampler->context();
+        if (c->prior != DPMM_PRIOR_GAUSSIAN) continue;
+        int gi = -1;
+        for (size_t q = 0; q < b->groups.size(); ++q)
+            if (b->groups[q].Dp == c->Dp) gi = (int)q;
+        if (gi < 0) {
+            b->groups.emplace_back();
+            gi = (int)b->groups.size() - 1;
+            b->groups[gi].Dp = c->Dp;
+        }
+        b->groups[gi].members.push_back(i);
+        b->groups[gi].kcap = std::max(b->groups[gi].kcap, c->k_max);
+        b->group_of[i] = gi;
+        DPMM_CUDA_TRY(cudaEventCreateWithFlags(&b->ready[i], cudaEventDisableTiming));
+    }
+    for (dpmm_batch::Group& g : b->groups) {
+        DPMM_CUDA_TRY(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+        DPMM_CUDA_TRY(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+        DPMM_CUDA_TRY(cudaMallocHost(&g.h_jobs, sizeof(LabelJob) * g.members.size()));
+        DPMM_CUDA_TRY(cudaMalloc(&g.d_jobs, sizeof(LabelJob) * g.members.size()));
+        if (gauss_label_smem_bytes(g.Dp, 128, g.kcap) > 220 * 1024)
+            return fail(DPMM_ERR_INVALID_ARG, "k_max too large for the batched label kernel at this dimension");
+    }
+    *out = b.release();
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_batch_step(dpmm_batch* b, int32_t n_iters)
+{
+    if (!b || n_iters < 0) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    DPMM_CUDA_TRY(cudaSetDevice(b->device));
+    for (int q = 0; q < n_iters; ++q) DPMM_TRY(host::batch_iteration(*b));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_batch_info(const dpmm_batch* b, int64_t* out)
+{
+    if (!b || !out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    out[0] = (int64_t)b->s.size();
+    out[1] = (int64_t)b->groups.size();
+    out[2] = b->batched_launches;
+    out[3] = b->graph_launches;
+    const int dps[6] = {4, 8, 16, 32, 64, 128};
+    for (int q = 0; q < 6; ++q) {
+        out[4 + q] = 0;
+        for (const auto& g : b->groups)
+            if (g.Dp == dps[q]) out[4 + q] = g.P;
+    }
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_batch_model_info(dpmm_batch* b, int32_t index, dpmm_model_info** out)
+{
+    if (!b || !out || index < 0 || index >= (int)b->s.size()) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    DPMM_TRY(b->s[index]->sampler->finish(&b->s[index]->mi));
+    *out = new dpmm_model_info(b->s[index]->mi);
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_batch_destroy(dpmm_batch* b)
+{
+    delete b;
+    return DPMM_OK;
+}

@@ -408,6 +408,25 @@ dpmm_status dpmm_dp_parallel(const dpmm_run_desc* run, int64_t n, int32_t d, con
 dpmm_status dpmm_dp_parallel_from_file(const char* npy_path, const char* params_path, int32_t prior_type,
                                        const dpmm_run_desc* overrides /* nullable */,
                                        dpmm_model_info** out);
+/* ---- batches of samplers (no counterpart in the reference, which runs one sampler per process:
+ * its init calls cudaDeviceReset, cudaKernel.cu:615) ------------------------------------------------
+ * count independent data sets (uneven N, D, K; runs[i], n[i] points of d[i] dimensions at
+ * points[i], host FP64 point-major, all on runs[0].device) advanced together one iteration at a
+ * time: the host stages of all samplers on a thread pool; the label phase of all NIW data sets of one
+ * padded dimension as ONE launch (work list of (data set, block of points) items, replayed from a
+ * CUDA graph; the points per block chosen by timing 32 / 64 / 128 on the first iteration).  NIW data
+ * sets use the FP32 SIMT label kernel.  Each data set's result is what dpmm_dp_parallel returns. */
+typedef struct dpmm_batch dpmm_batch;
+dpmm_status dpmm_batch_create(int32_t count, const dpmm_run_desc* runs, const int64_t* n, const int32_t* d,
+                              const double* const* points, dpmm_batch** out);
+dpmm_status dpmm_batch_step(dpmm_batch* b, int32_t n_iters);
+/* out[0] data sets, out[1] padded-dimension groups, out[2] batched label launches, out[3] of them
+ * replayed from a CUDA graph, out[4..9] block size chosen for padded dimension 4, 8, 16, 32, 64, 128
+ * (0: no such group / not tuned yet) */
+dpmm_status dpmm_batch_info(const dpmm_batch* b, int64_t* out);
+dpmm_status dpmm_batch_model_info(dpmm_batch* b, int32_t index, dpmm_model_info** out);
+dpmm_status dpmm_batch_destroy(dpmm_batch* b);
+
 /* ModelInfo accessors (modelInfo.h:45-56).  Arrays stay valid until dpmm_model_info_free. */
 int64_t dpmm_model_info_n(const dpmm_model_info* mi);
 const int32_t* dpmm_model_info_labels(const dpmm_model_info* mi);
