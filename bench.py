@@ -354,6 +354,8 @@ def main():
     ph_ms = (ctypes.c_double * 8)()
     ph_calls = (ctypes.c_int64 * 8)()
     check(L.dpmm_phase_times(ctx, 0, ph_ms, ph_calls))
+    prune = (ctypes.c_double * 4)()
+    check(L.dpmm_label_pruning_stats(ctx, prune))
     h2d1, d2h1 = ctypes.c_uint64(), ctypes.c_uint64()
     L.dpmm_transfer_bytes(ctypes.byref(h2d1), ctypes.byref(d2h1))
     if dist:
@@ -403,6 +405,8 @@ def main():
                        "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
                        "nmi_vs_generating_labels": nmi,
                        "parameter_draws": "host" if args.host_draws else "device",
+                       "label_pruning": {"attempts": int(prune[0]), "pruned_phases": int(prune[1]),
+                                         "kept_other_clusters_per_point": prune[2], "margin_nats": prune[3]},
                        "screen": screen_summary(args.screen, scr)},
             "gpu_launches": int(launches),
             "roofline": roofline,

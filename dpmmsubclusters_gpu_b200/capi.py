@@ -51,7 +51,7 @@ class dpmm_run_desc(Structure):
                 ("out_mult_alpha", _PD), ("gt", POINTER(c_int32)), ("device", c_int32),
                 ("screen_mode", c_int32), ("screen_top", c_int32), ("screen_sweep_every", c_int32),
                 ("screen_min_recall", c_float), ("screen_params", POINTER(c_float)), ("screen_split_min", c_int32),
-                ("host_param_draws", c_int32), ("reserved", c_int32 * 2)]
+                ("host_param_draws", c_int32), ("label_prune_margin", c_float), ("reserved", c_int32 * 1)]
 
 
 # every symbol include/dpmm_capi.h declares, with its ctypes signature
@@ -138,6 +138,8 @@ SIGNATURES = {
     "dpmm_compact_statistics": (c_int, [_CTX, c_int, _PI32]),
     "dpmm_statistics_counts": (c_int, [_CTX, c_int, _PI32, _PI64]),
     "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
+    "dpmm_set_label_pruning": (c_int, [_CTX, c_double]),
+    "dpmm_label_pruning_stats": (c_int, [_CTX, _PD]),
     "dpmm_batch_create": (c_int, [c_int32, POINTER(dpmm_run_desc), _PI64, _PI32, POINTER(_PD), POINTER(c_void_p)]),
     "dpmm_batch_step": (c_int, [c_void_p, c_int32]),
     "dpmm_batch_info": (c_int, [c_void_p, _PI64]),

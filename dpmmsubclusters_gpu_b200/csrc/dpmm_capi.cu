@@ -150,7 +150,9 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_split_hr, c->d_merge_hr, c->d_post_logdet, c->d_mask, c->d_Btc, c->d_Atc, c->d_rbuf,
                     c->d_rpart, c->d_Bsub, c->d_scr_rec, c->d_scr_vec, c->d_scr_linv, c->d_scr_feat,
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
-                    c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw};
+                    c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
+                    c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
+                    c->d_prune_beta};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -281,6 +283,18 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
         chk(dev_alloc(&c->d_scr_list, (size_t)2 * kScrMaxTop));
         chk(dev_alloc(&c->d_scr_slots, (size_t)3 * kScrMaxTop));
         chk(dev_alloc(&c->d_scr_hr, (size_t)kScrMaxTop));
+    }
+    if (gauss && Dp <= 64) {
+        chk(dev_alloc(&c->d_prune_rh, (size_t)N));
+        chk(dev_alloc(&c->d_prune_cand, (size_t)c->max_chunks * 17));
+        const size_t KP = (size_t)std::min(KM, 256);   // the pruned phase takes K <= 256
+        chk(dev_alloc(&c->d_prune_lam, KP));
+        chk(dev_alloc(&c->d_prune_M, KP * KP));
+        chk(dev_alloc(&c->d_prune_V, KP * KP * Dp));
+        chk(dev_alloc(&c->d_prune_beta, KP * KP));
+        chk(dev_alloc(&c->d_prune_cnt, (size_t)2));
+    } else {
+        c->prune_margin = 0.f;
     }
     if (c->rng_kind == DPMM_RNG_CURAND_XORWOW) chk(dev_alloc(&c->d_curand, (size_t)N));
     if (st == DPMM_OK) {
@@ -642,7 +656,11 @@ extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final
     dpmm_status s;
     const bool use_tc = c->ll_mode != DPMM_LL_FP32 && tc_supported(c, K);
     PhaseTimer pt(c, PH_LABELS);
-    if (c->ll_mode == DPMM_LL_TC_BF16X3 && !use_tc) {
+    bool pruned = false;
+    s = DPMM_OK;
+    if (!d_rout) s = launch_cluster_labels_pruned(c, K, final_, du, &pruned);
+    if (s != DPMM_OK || pruned) {
+    } else if (c->ll_mode == DPMM_LL_TC_BF16X3 && !use_tc) {
         s = fail(DPMM_ERR_INVALID_ARG, "tensor-core log-likelihood not available for this shape");
     } else {
         s = use_tc ? launch_cluster_labels_tc(c, K, final_, du, d_rout) : launch_cluster_labels(c, K, final_, du, d_rout);
@@ -1061,3 +1079,25 @@ dpmm_status ensure_stats(dpmm_ctx* c, int K)
 }
 
 }  // namespace dpmm
+
+extern "C" dpmm_status dpmm_set_label_pruning(dpmm_ctx* c, double margin)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (!c->d_prune_rh) {
+        if (margin > 0) return fail(DPMM_ERR_INVALID_ARG, "the pruned label phase needs the NIW prior and D <= 64");
+        return DPMM_OK;
+    }
+    c->prune_margin = margin > 0 ? (float)margin : 0.f;
+    c->prune_wait = 0;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* c, double* out)
+{
+    if (!c || !out) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    out[0] = (double)c->prune_tries;
+    out[1] = (double)c->prune_used;
+    out[2] = c->prune_used ? c->prune_extra / (double)c->prune_used : 0.0;
+    out[3] = c->prune_margin;
+    return DPMM_OK;
+}

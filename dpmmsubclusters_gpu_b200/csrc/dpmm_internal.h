@@ -184,6 +184,19 @@ struct dpmm_ctx {
     int32_t* d_scr_slots = nullptr;// [3 * kScrMaxTop] slots whose lml the list needs
     double* d_scr_hr = nullptr;    // [kScrMaxTop] exact ratios of the list
     bool scr_params_set = false;
+
+    // pruned label phase (dpmm_kernels.cu: k_prune_*): NIW prior, padded dimension <= 64
+    float prune_margin = 30.f;     // nats; <= 0 switches the pruned phase off
+    int prune_wait = 0;            // label phases to run dense before the next attempt
+    int64_t prune_tries = 0, prune_used = 0;
+    double prune_extra = 0;        // sum over used phases of kept other clusters per point
+    float* d_prune_rh = nullptr;   // [N] r of each point's current cluster, permutation order
+    int32_t* d_prune_cand = nullptr; // [max_chunks][17] kept clusters per chunk
+    float* d_prune_lam = nullptr;  // [KP], KP = min(k_max, 256) (the pruned phase takes K <= 256)
+    float* d_prune_M = nullptr;    // [KP][KP]
+    float* d_prune_V = nullptr;    // [KP][KP][Dp] point-bound directions
+    float* d_prune_beta = nullptr; // [KP][KP]
+    unsigned long long* d_prune_cnt = nullptr;   // [2]
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
 
@@ -265,6 +278,8 @@ dpmm_status launch_init_curand(dpmm_ctx* c);
 dpmm_status launch_labels_init(dpmm_ctx* c, int initial_clusters, double outlier_mod, const float* d_u);
 dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u);
 dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
+// the pruned label phase; *used = false when it declined (the caller then runs the dense phase)
+dpmm_status launch_cluster_labels_pruned(dpmm_ctx* c, int K, int final_, const float* d_u, bool* used);
 dpmm_status build_permutation(dpmm_ctx* c, int K);
 dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, float* d_rout, bool draw,
                                         const uint8_t* d_mask = nullptr);

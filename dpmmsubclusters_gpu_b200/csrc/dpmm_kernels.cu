@@ -114,6 +114,39 @@ __device__ __forceinline__ int draw_from_r(float* sr, int p, int K, int final_, 
 // Gaussian label phase, FP32 SIMT: one thread per point, x in registers, each cluster's
 // precision factor (transposed) broadcast from shared memory.
 //   z_j = sum_i W(i,j) x_i - b_j,   r_k = c_k - 0.5 * sum_j z_j^2
+// r = c - 0.5 |W^T x - b|^2 for one point (x in registers) and one cluster whose transposed factor
+// (Wt[j][i] = W(i, j)) and b are staged in shared memory
+template <int DP>
+__device__ __forceinline__ float gauss_r_point(const float* __restrict__ sW, const float* __restrict__ sbv,
+                                               const float (&xr)[DP], float c)
+{
+    float q = 0.f;
+#pragma unroll 2
+    for (int j = 0; j < DP; j += 2) {
+        const float4* w0 = reinterpret_cast<const float4*>(sW + j * DP);
+        const float4* w1 = reinterpret_cast<const float4*>(sW + (j + 1) * DP);
+        float z0 = -sbv[j], z1 = -sbv[j + 1];
+        float z0b = 0.f, z1b = 0.f;
+#pragma unroll
+        for (int i4 = 0; i4 < DP / 4; ++i4) {
+            float4 a = w0[i4], b = w1[i4];
+            z0 = fmaf(a.x, xr[4 * i4 + 0], z0);
+            z1 = fmaf(b.x, xr[4 * i4 + 0], z1);
+            z0b = fmaf(a.y, xr[4 * i4 + 1], z0b);
+            z1b = fmaf(b.y, xr[4 * i4 + 1], z1b);
+            z0 = fmaf(a.z, xr[4 * i4 + 2], z0);
+            z1 = fmaf(b.z, xr[4 * i4 + 2], z1);
+            z0b = fmaf(a.w, xr[4 * i4 + 3], z0b);
+            z1b = fmaf(b.w, xr[4 * i4 + 3], z1b);
+        }
+        z0 += z0b;
+        z1 += z1b;
+        q = fmaf(z0, z0, q);
+        q = fmaf(z1, z1, q);
+    }
+    return c - 0.5f * q;
+}
+
 // one block of P points starting at pt0 (the body of k_gauss_labels_simt and of its batched form)
 template <int DP, int P>
 __device__ __forceinline__ void gauss_labels_tile(const float* __restrict__ x, int64_t N,
@@ -149,31 +182,7 @@ __device__ __forceinline__ void gauss_labels_tile(const float* __restrict__ x, i
         for (int e = p; e < DP * DP / 4; e += P) dst[e] = src[e];
         for (int e = p; e < DP; e += P) sbv[e] = bvec[(size_t)3 * k * DP + e];
         __syncthreads();
-        float q = 0.f;
-#pragma unroll 2
-        for (int j = 0; j < DP; j += 2) {
-            const float4* w0 = reinterpret_cast<const float4*>(sW + j * DP);
-            const float4* w1 = reinterpret_cast<const float4*>(sW + (j + 1) * DP);
-            float z0 = -sbv[j], z1 = -sbv[j + 1];
-            float z0b = 0.f, z1b = 0.f;
-#pragma unroll
-            for (int i4 = 0; i4 < DP / 4; ++i4) {
-                float4 a = w0[i4], b = w1[i4];
-                z0 = fmaf(a.x, xr[4 * i4 + 0], z0);
-                z1 = fmaf(b.x, xr[4 * i4 + 0], z1);
-                z0b = fmaf(a.y, xr[4 * i4 + 1], z0b);
-                z1b = fmaf(b.y, xr[4 * i4 + 1], z1b);
-                z0 = fmaf(a.z, xr[4 * i4 + 2], z0);
-                z1 = fmaf(b.z, xr[4 * i4 + 2], z1);
-                z0b = fmaf(a.w, xr[4 * i4 + 3], z0b);
-                z1b = fmaf(b.w, xr[4 * i4 + 3], z1b);
-            }
-            z0 += z0b;
-            z1 += z1b;
-            q = fmaf(z0, z0, q);
-            q = fmaf(z1, z1, q);
-        }
-        const float r = cvec[3 * k] - 0.5f * q;
+        const float r = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
         sr[k * P + p] = r;
         if (r_out && valid) r_out[pt * K + k] = r;
     }
@@ -362,6 +371,336 @@ dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d
                                                                        c->d_labels, d_rout);
     DPMM_LAUNCHED();
     return DPMM_OK;
+}
+
+// ----------------------------------------------------------------------------- pruned label phase
+// The points are taken in chunks of one current cluster h (the label-ordered permutation).  For a
+// chunk, r_h is computed exactly for every point; another cluster k is kept only if some point of the
+// chunk could have r_k within `margin` nats of its r_h, by two bounds (r_k = c_k - 0.5 |W_k^T (x - mu_k)|^2):
+//   chunk bound: |W_k^T (x - mu_k)| >= M_hk - sigma_max(W_k) |x - mu_h|, with M_hk = |W_k^T (mu_h - mu_k)|,
+//                sigma_max(W_k)^2 <= max_i sum_j |Lambda_k(i,j)| (Gershgorin), |x - mu_h| <= R;
+//   point bound: |W_k^T (x - mu_k)| >= |u^T W_k^T (x - mu_k)| = |v_hk^T x - beta_hk| for the unit vector
+//                u = W_k^T (mu_h - mu_k) / M_hk, v_hk = W_k u, beta_hk = v_hk^T mu_k.
+// A left-out cluster has r_k(x) < r_h(x) - margin <= max_k' r_k'(x) - margin at every point of the chunk,
+// so it carries less than K e^-margin of the point's probability; the draw runs over all K columns with
+// it at probability 0, which gives the dense draw's label unless a uniform falls inside that mass.  A
+// chunk left with its own cluster only takes it as every point's label.
+constexpr int kPrTh = 128;       // threads per block
+constexpr int kMaxKForPrune = 256;
+constexpr int kPrMaxCand = 16;   // other clusters a chunk may keep (more: the dense phase runs)
+
+// one block per cluster k: lam[k] = sqrt of the Gershgorin bound of lambda_max(W_k W_k^T) (inflated);
+// for every h: M[h][k] (deflated), v[h][k][DP] and beta[h][k]
+template <int DP>
+__global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ Wt, const float* __restrict__ mu,
+                                                      int K, float* __restrict__ lam, float* __restrict__ M,
+                                                      float* __restrict__ V, float* __restrict__ beta)
+{
+    constexpr int NW = kPrTh / 32;
+    __shared__ float sW[DP * DP];
+    __shared__ double red[NW];
+    __shared__ double zs[NW][DP];
+    const int k = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    for (int e = t; e < DP * DP; e += blockDim.x) sW[e] = Wt[(size_t)3 * k * DP * DP + e];
+    __syncthreads();
+    double rmax = 0;
+    for (int i = t; i < DP; i += blockDim.x) {
+        double srow = 0;
+        for (int j = 0; j < DP; ++j) {
+            double l = 0;
+            for (int cc = 0; cc < DP; ++cc) l += (double)sW[cc * DP + i] * (double)sW[cc * DP + j];
+            srow += fabs(l);
+        }
+        rmax = fmax(rmax, srow);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+    if (lane == 0) red[warp] = rmax;
+    __syncthreads();
+    if (t == 0) {
+        double m = 0;
+        for (int w = 0; w < NW; ++w) m = fmax(m, red[w]);
+        lam[k] = (float)(sqrt(m) * (1.0 + 1e-5));
+    }
+    const float* mk = mu + (size_t)3 * k * DP;
+    for (int h = warp; h < K; h += NW) {
+        const float* mh = mu + (size_t)3 * h * DP;
+        double q = 0;
+        for (int j = lane; j < DP; j += 32) {   // z = W_k^T (mu_h - mu_k)
+            double z = 0;
+            for (int i = 0; i < DP; ++i) z += (double)sW[j * DP + i] * ((double)mh[i] - (double)mk[i]);
+            zs[warp][j] = z;
+            q += z * z;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+        __syncwarp();
+        const double nz = sqrt(q);
+        const double inv = nz > 0 ? 1.0 / nz : 0.0;
+        float* vh = V + ((size_t)h * K + k) * DP;
+        double bsum = 0;
+        for (int i = lane; i < DP; i += 32) {    // v = W_k u, u = z / |z|
+            double v = 0;
+            for (int j = 0; j < DP; ++j) v += (double)sW[j * DP + i] * zs[warp][j];
+            v *= inv;
+            vh[i] = (float)v;
+            bsum += (double)(float)v * (double)mk[i];
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) bsum += __shfl_xor_sync(0xffffffffu, bsum, o);
+        if (lane == 0) {
+            M[(size_t)h * K + k] = (float)(nz * (1.0 - 1e-5));
+            beta[(size_t)h * K + k] = (float)bsum;
+        }
+        __syncwarp();
+    }
+}
+
+template <int DP>
+__device__ __forceinline__ void load_row(const float* __restrict__ x, int64_t pt, float (&xr)[DP])
+{
+    const float4* src = reinterpret_cast<const float4*>(x + pt * DP);
+#pragma unroll
+    for (int q = 0; q < DP / 4; ++q) {
+        const float4 v = src[q];
+        xr[4 * q] = v.x;
+        xr[4 * q + 1] = v.y;
+        xr[4 * q + 2] = v.z;
+        xr[4 * q + 3] = v.w;
+    }
+}
+
+// pass 1, one block per chunk (chunk length <= kChunkMax): r_h of every point (into rh, permutation
+// order), the clusters the bounds cannot leave out (cand[q] = count, then up to kPrMaxCand indices),
+// and the totals cnt[0] += count * chunk length, cnt[1] += (count > capacity).
+// Dynamic shared memory: kChunkMax + K * (DP + 3) floats + K ints.
+template <int DP>
+__global__ void __launch_bounds__(kPrTh) k_prune_scan(const float* __restrict__ x, const int32_t* __restrict__ perm,
+                                                      const int32_t* __restrict__ chunk,
+                                                      const int32_t* __restrict__ nchunks, const float* __restrict__ Wt,
+                                                      const float* __restrict__ bvec, const float* __restrict__ cvec,
+                                                      const float* __restrict__ mu, const float* __restrict__ lam,
+                                                      const float* __restrict__ M, const float* __restrict__ V,
+                                                      const float* __restrict__ beta, int K, float margin,
+                                                      float* __restrict__ rh, int32_t* __restrict__ cand,
+                                                      unsigned long long* __restrict__ cnt)
+{
+    __shared__ __align__(16) float sW[DP * DP];
+    __shared__ float sbv[DP], smu[DP];
+    __shared__ float rmin_w[kPrTh / 32], r2_w[kPrTh / 32];
+    __shared__ int n_test;
+    __shared__ unsigned int keep[(kMaxKForPrune + 31) / 32];
+    extern __shared__ __align__(16) float dsm[];
+    float* srh = dsm;                          // kChunkMax
+    float* sv = srh + kChunkMax;               // n_test * DP
+    float* sbeta = sv + (size_t)K * DP;        // n_test
+    float* sck = sbeta + K;                    // n_test
+    int* sk = reinterpret_cast<int*>(sck + K); // n_test
+    const int q = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (q >= *nchunks) return;
+    const int h = chunk[3 * q], start = chunk[3 * q + 1], L = chunk[3 * q + 2];
+    {
+        const float4* src = reinterpret_cast<const float4*>(Wt + (size_t)3 * h * DP * DP);
+        float4* dst = reinterpret_cast<float4*>(sW);
+        for (int e = t; e < DP * DP / 4; e += blockDim.x) dst[e] = src[e];
+        for (int e = t; e < DP; e += blockDim.x) {
+            sbv[e] = bvec[(size_t)3 * h * DP + e];
+            smu[e] = mu[(size_t)3 * h * DP + e];
+        }
+        for (int e = t; e < (K + 31) / 32; e += blockDim.x) keep[e] = 0u;
+        if (t == 0) n_test = 0;
+    }
+    __syncthreads();
+    const float ch = cvec[3 * h];
+    float tmin = INFINITY, tr2 = 0.f;
+    for (int i = start + t; i < start + L; i += blockDim.x) {
+        float xr[DP];
+        load_row<DP>(x, perm[i], xr);
+        const float r = gauss_r_point<DP>(sW, sbv, xr, ch);
+        rh[i] = r;
+        srh[i - start] = r;
+        tmin = fminf(tmin, r);
+        float d2 = 0.f;
+#pragma unroll
+        for (int e = 0; e < DP; ++e) d2 = fmaf(xr[e] - smu[e], xr[e] - smu[e], d2);
+        tr2 = fmaxf(tr2, d2);
+    }
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+        tr2 = fmaxf(tr2, __shfl_xor_sync(0xffffffffu, tr2, o));
+    }
+    if (lane == 0) {
+        rmin_w[warp] = tmin;
+        r2_w[warp] = tr2;
+    }
+    __syncthreads();
+    float rmin = rmin_w[0], r2 = r2_w[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+        rmin = fminf(rmin, rmin_w[w]);
+        r2 = fmaxf(r2, r2_w[w]);
+    }
+    const float R = sqrtf(r2) * 1.0001f + 1e-4f;
+    // chunk bound: clusters it cannot leave out go to the point test
+    for (int k = t; k < K; k += blockDim.x) {
+        if (k == h) continue;
+        const float d = M[(size_t)h * K + k] - lam[k] * R;
+        const float ub = cvec[3 * k] - 0.5f * (d > 0.f ? d * d : 0.f);
+        if (!(ub < rmin - margin)) sk[atomicAdd(&n_test, 1)] = k;
+    }
+    __syncthreads();
+    const int nt = n_test;
+    for (int e = t; e < nt * DP; e += blockDim.x) {
+        const int a = e / DP, i = e % DP;
+        sv[e] = V[((size_t)h * K + sk[a]) * DP + i];
+    }
+    for (int a = t; a < nt; a += blockDim.x) {
+        sbeta[a] = beta[(size_t)h * K + sk[a]];
+        sck[a] = cvec[3 * sk[a]];
+    }
+    __syncthreads();
+    // point bound
+    if (nt > 0) {
+        for (int i = start + t; i < start + L; i += blockDim.x) {
+            float xr[DP];
+            load_row<DP>(x, perm[i], xr);
+            const float lim = srh[i - start] - margin;
+            for (int a = 0; a < nt; ++a) {
+                const float* va = sv + (size_t)a * DP;
+                float p0 = -sbeta[a], p1 = 0.f;
+#pragma unroll
+                for (int e = 0; e < DP; e += 2) {
+                    p0 = fmaf(va[e], xr[e], p0);
+                    p1 = fmaf(va[e + 1], xr[e + 1], p1);
+                }
+                const float pr = p0 + p1;
+                const float ub = sck[a] - 0.5f * pr * pr;
+                if (!(ub < lim)) atomicOr(&keep[sk[a] >> 5], 1u << (sk[a] & 31));
+            }
+        }
+    }
+    __syncthreads();
+    if (t == 0) {
+        int n = 0;
+        int32_t* cq = cand + (size_t)q * (kPrMaxCand + 1);
+        for (int k = 0; k < K; ++k)
+            if ((keep[k >> 5] >> (k & 31)) & 1u) {
+                if (n < kPrMaxCand) cq[1 + n] = k;
+                ++n;
+            }
+        cq[0] = n;
+        atomicAdd(&cnt[0], (unsigned long long)n * (unsigned long long)L);
+        if (n > kPrMaxCand) atomicAdd(&cnt[1], 1ull);
+    }
+}
+
+// pass 2, one block per chunk: labels.  A chunk without other clusters takes h + 1; otherwise, per
+// tile of kPrTh points, r of the kept clusters (r_h from pass 1), the others at -inf, and the draw
+// (or argmax) of the dense label phase over all K columns.  Shared memory: DP*DP + DP + K*kPrTh floats.
+template <int DP>
+__global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ x, const int32_t* __restrict__ perm,
+                                                      const int32_t* __restrict__ chunk,
+                                                      const int32_t* __restrict__ nchunks, const float* __restrict__ Wt,
+                                                      const float* __restrict__ bvec, const float* __restrict__ cvec,
+                                                      int K, int final_, RngArgs rng, const float* __restrict__ rh,
+                                                      const int32_t* __restrict__ cand, int32_t* __restrict__ labels)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* sW = reinterpret_cast<float*>(smem);
+    float* sbv = sW + DP * DP;
+    float* sr = sbv + DP;
+    const int q = blockIdx.x, t = threadIdx.x;
+    if (q >= *nchunks) return;
+    const int h = chunk[3 * q], start = chunk[3 * q + 1], L = chunk[3 * q + 2];
+    const int32_t* cq = cand + (size_t)q * (kPrMaxCand + 1);
+    const int n = cq[0];
+    if (n == 0) {
+        for (int i = start + t; i < start + L; i += blockDim.x) labels[perm[i]] = h + 1;
+        return;
+    }
+    for (int base = start; base < start + L; base += blockDim.x) {
+        const int i = base + t;
+        const bool valid = i < start + L;
+        const int64_t pt = valid ? perm[i] : 0;
+        float xr[DP];
+        if (valid) load_row<DP>(x, pt, xr);
+        else
+#pragma unroll
+            for (int e = 0; e < DP; ++e) xr[e] = 0.f;
+        for (int k = 0; k < K; ++k) sr[k * kPrTh + t] = -INFINITY;
+        sr[h * kPrTh + t] = valid ? rh[i] : 0.f;
+        for (int a = 0; a < n; ++a) {
+            const int k = cq[1 + a];
+            __syncthreads();
+            const float4* src = reinterpret_cast<const float4*>(Wt + (size_t)3 * k * DP * DP);
+            float4* dst = reinterpret_cast<float4*>(sW);
+            for (int e = t; e < DP * DP / 4; e += blockDim.x) dst[e] = src[e];
+            for (int e = t; e < DP; e += blockDim.x) sbv[e] = bvec[(size_t)3 * k * DP + e];
+            __syncthreads();
+            sr[k * kPrTh + t] = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
+        }
+        if (valid) labels[pt] = draw_from_r<kPrTh>(sr, t, K, final_, rng, pt);
+    }
+}
+
+static size_t prune_draw_smem(int DP, int K) { return sizeof(float) * ((size_t)DP * DP + DP + (size_t)K * kPrTh); }
+
+template <int DP>
+static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float* d_u, bool* used)
+{
+    DPMM_TRY(build_permutation(c, K));
+    k_prune_prep<DP><<<K, kPrTh, 0, c->stream>>>(c->d_Wt, c->d_mu, K, c->d_prune_lam, c->d_prune_M, c->d_prune_V,
+                                                 c->d_prune_beta);
+    DPMM_LAUNCHED();
+    DPMM_CUDA_TRY(cudaMemsetAsync(c->d_prune_cnt, 0, 2 * sizeof(unsigned long long), c->stream));
+    const size_t ssm = sizeof(float) * ((size_t)kChunkMax + (size_t)K * (DP + 3));
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_scan<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
+    k_prune_scan<DP><<<c->max_chunks, kPrTh, ssm, c->stream>>>(
+        c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c, c->d_mu, c->d_prune_lam, c->d_prune_M,
+        c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand, c->d_prune_cnt);
+    DPMM_LAUNCHED();
+    unsigned long long* h = reinterpret_cast<unsigned long long*>(c->h_pinned);
+    int32_t* outside = reinterpret_cast<int32_t*>(h + 2);   // points whose label has no chunk
+    DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_prune_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                  c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(outside, c->d_aux + 8 + K, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->prune_tries += 1;
+    const double extra = (double)h[0] / (double)c->N;
+    if (h[1] > 0 || extra > 0.5 || *outside != 0) {   // the bound keeps too much: the dense phase, and wait
+        c->prune_wait = 8;
+        return DPMM_OK;
+    }
+    const RngArgs r = rng_args(c, d_u);
+    const size_t sm = prune_draw_smem(DP, K);
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_draw<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_prune_draw<DP><<<c->max_chunks, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
+                                                             c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
+                                                             c->d_prune_cand, c->d_labels);
+    DPMM_LAUNCHED();
+    c->prune_used += 1;
+    c->prune_extra += extra;
+    *used = true;
+    return DPMM_OK;
+}
+
+dpmm_status launch_cluster_labels_pruned(dpmm_ctx* c, int K, int final_, const float* d_u, bool* used)
+{
+    *used = false;
+    if (c->prior != DPMM_PRIOR_GAUSSIAN || c->Dp > 64 || c->prune_margin <= 0 || K < 2 || K > kMaxKForPrune)
+        return DPMM_OK;
+    if (prune_draw_smem(c->Dp, K) > 220 * 1024) return DPMM_OK;
+    if (c->prune_wait > 0) {
+        --c->prune_wait;
+        return DPMM_OK;
+    }
+    switch (c->Dp) {
+        case 4: return launch_pruned_dp<4>(c, K, final_, d_u, used);
+        case 8: return launch_pruned_dp<8>(c, K, final_, d_u, used);
+        case 16: return launch_pruned_dp<16>(c, K, final_, d_u, used);
+        case 32: return launch_pruned_dp<32>(c, K, final_, d_u, used);
+        default: return launch_pruned_dp<64>(c, K, final_, d_u, used);
+    }
 }
 
 // ----------------------------------------------------------------------------- permutation

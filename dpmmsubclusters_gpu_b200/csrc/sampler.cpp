@@ -80,6 +80,7 @@ struct Config {
     double screen_min_recall = 0.5;
     std::vector<float> screen_params;
     bool host_param_draws = false;   // draw the NIW parameters on the host even where the device can
+    double label_prune_margin = 30.0;  // pruned label phase margin (<= 0: off)
 };
 
 // screen counters and the DPMM_SCREEN_LOG record of a run
@@ -1131,6 +1132,7 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
         DPMM_TRY(dpmm_set_prior_niw(h->ctx, cfg.hyper.k, cfg.hyper.m.data(), cfg.hyper.v, cfg.hyper.psi.data()));
     else
         DPMM_TRY(dpmm_set_prior_multinomial(h->ctx, cfg.hyper.alpha.data()));
+    if (h->ctx->d_prune_rh) DPMM_TRY(dpmm_set_label_pruning(h->ctx, cfg.label_prune_margin));
     if (cfg.screen_mode == DPMM_SCREEN_ON) {
         if ((int)cfg.screen_params.size() != kScrParams)
             return fail(DPMM_ERR_INVALID_ARG, "screen_mode DPMM_SCREEN_ON needs screen_params");
@@ -1209,6 +1211,7 @@ static void screen_from_run(const dpmm_run_desc* run, host::Config& cfg)
     cfg.screen_min_recall = run->screen_min_recall > 0 ? run->screen_min_recall : 0.5;
     cfg.screen_split_min = run->screen_split_min > 0 ? run->screen_split_min : 256;
     cfg.host_param_draws = run->host_param_draws != 0;
+    cfg.label_prune_margin = run->label_prune_margin == 0 ? 30.0 : (double)run->label_prune_margin;
     if (run->screen_params) cfg.screen_params.assign(run->screen_params, run->screen_params + kScrParams);
 }
 

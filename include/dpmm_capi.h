@@ -315,6 +315,17 @@ dpmm_status dpmm_statistics_counts(dpmm_ctx* ctx, int n, const int32_t* indices,
  * stored relative to.  Any output may be NULL. */
 dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, float* c, float* mu);
 
+/* ---- pruned label phase (NIW prior, D <= 64; no counterpart in the reference) -----------------
+ * dpmm_create_clusters_labels (without loglik_out) evaluates, for each chunk of points of one current
+ * cluster, only the clusters that an upper bound cannot put more than `margin` nats below the chunk's
+ * own cluster; the left-out clusters carry less than K e^-margin of each point's probability and get
+ * probability 0 in the same draw.  When the bound keeps too much (early iterations) the dense phase
+ * runs and the next 8 label phases stay dense.  margin <= 0 switches it off (default 30).
+ * stats: out[0] attempts, out[1] label phases run pruned, out[2] mean kept other clusters per point
+ * in those, out[3] the margin. */
+dpmm_status dpmm_set_label_pruning(dpmm_ctx* ctx, double margin);
+dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* ctx, double* out);
+
 /* Synchronise the context's stream; returns any pending device error. */
 dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
@@ -368,7 +379,8 @@ typedef struct dpmm_run_desc {
                                     exact split ratios of K clusters cost one launch of 3K blocks */
     int32_t host_param_draws;    /* nonzero: draw the cluster parameters on the host (FP64, OpenMP) even
                                     where the device draws them (NIW prior, D <= 64, no outlier cluster) */
-    int32_t reserved[2];
+    float label_prune_margin;    /* pruned label phase margin in nats (0 -> 30; negative -> off) */
+    int32_t reserved[1];
 } dpmm_run_desc;
 
 typedef enum dpmm_screen_mode {

@@ -1,0 +1,78 @@
+"""The pruned label phase (dpmm_set_label_pruning; csrc/dpmm_kernels.cu k_prune_*) against the dense
+phase with the same parameters and caller uniforms.  Left-out clusters are provably more than the
+margin (30 nats) below each point's own cluster, so both draw the same label unless a uniform falls
+inside < K e^-30 of probability: the labels must be identical.  A state the bound cannot prune (random
+current labels) falls back to the dense phase."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import uniforms
+from dpmmsubclusters_gpu_b200 import CudaKernel, LL_FP32, prior_type
+from dpmmsubclusters_gpu_b200.capi import check, lib
+
+pytestmark = pytest.mark.gpu
+
+
+def _mixture(seed, N, D, K, spread):
+    rng = np.random.default_rng(seed)
+    mus = rng.normal(size=(K, D)) * spread
+    covs = []
+    z = rng.integers(0, K, size=N)
+    x = np.empty((N, D))
+    for c in range(K):
+        A = rng.normal(size=(D, D))
+        C = A @ A.T / D + 0.5 * np.eye(D)
+        covs.append(C)
+        idx = np.flatnonzero(z == c)
+        x[idx] = rng.multivariate_normal(mus[c], C, size=idx.size)
+    return x, z, mus, np.array(covs), rng
+
+
+def _stats(kern):
+    out = (ctypes.c_double * 4)()
+    check(lib().dpmm_label_pruning_stats(kern.ctx, out))
+    return list(out)
+
+
+@pytest.mark.parametrize("D,mode", [(16, None), (64, None), (32, LL_FP32)])
+def test_pruned_labels_equal_dense_labels(D, mode):
+    K, N = 10, 60000
+    x, z, mus, covs, rng = _mixture(D, N, D, K, 6.0)
+    kern = CudaKernel(prior_type.Gaussian, k_max=16, loglik_mode=mode).init(N, x.T, seed=1)
+    mu = mus + 0.05 * rng.normal(size=mus.shape)
+    inv = np.array([np.linalg.inv(c) for c in covs])
+    ld = np.array([np.linalg.slogdet(c)[1] for c in covs])
+    w = rng.dirichlet(np.ones(K) * 3)
+    kern.set_gaussian_params(mu, inv, ld, w)
+    u = uniforms(2 * N, 5)
+    res = {}
+    for margin in (30.0, 0.0):
+        check(lib().dpmm_set_label_pruning(kern.ctx, margin))
+        for final in (False, True):
+            kern.set_labels((z + 1).astype(np.int32))
+            kern.create_clusters_labels(K, final, None if final else u)
+            res[(margin, final)] = kern.get_labels()
+    st = _stats(kern)
+    assert st[1] == 2, st          # both pruned phases ran pruned
+    for final in (False, True):
+        np.testing.assert_array_equal(res[(30.0, final)], res[(0.0, final)])
+
+
+def test_unprunable_state_falls_back_to_dense():
+    K, N, D = 6, 30000, 8
+    x, z, mus, covs, rng = _mixture(3, N, D, K, 0.5)    # overlapping clusters
+    kern = CudaKernel(prior_type.Gaussian, k_max=16).init(N, x.T, seed=1)
+    kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
+                             np.array([np.linalg.slogdet(c)[1] for c in covs]), np.full(K, 1.0 / K))
+    u = uniforms(2 * N, 7)
+    lab = {}
+    for margin in (30.0, 0.0):
+        check(lib().dpmm_set_label_pruning(kern.ctx, margin))
+        kern.set_labels(rng.integers(1, K + 1, size=N).astype(np.int32))
+        kern.create_clusters_labels(K, False, u)
+        lab[margin] = kern.get_labels()
+    st = _stats(kern)
+    assert st[0] == 1 and st[1] == 0, st
+    np.testing.assert_array_equal(lab[30.0], lab[0.0])
