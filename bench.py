@@ -75,6 +75,46 @@ def label_kernel_traffic(N, K):
     return vals["dram_bytes_per_launch"] * model(N, K) / model(vals["capture_N"], vals["capture_K"])
 
 
+def padded(d):
+    p = 4
+    while p < d:
+        p *= 2
+    return p
+
+
+def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src):
+    """Per timed kernel (CUDA events around each launch on its stream): algorithmic work per launch,
+    achieved rate and the fraction of the measured peak of its bound."""
+    Dp = padded(D)
+    hbm = pk.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+    bf16 = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
+    out = {}
+
+    def add(name, slot, bound, work, unit, peak, peak_key, note, traffic=None):
+        if ph_calls[slot] == 0:
+            return
+        ms = ph_ms[slot] / ph_calls[slot]
+        scale = 1e12 if unit == "TFLOP/s" else 1e9
+        ach = work / (ms / 1e3) / scale if ms > 0 else None
+        out[name] = {"bound": bound, "achieved": ach, "peak": peak, "unit": unit,
+                     "frac": ach / peak if ach else None, "traffic": traffic, "launch_ms": ms,
+                     "launches": int(ph_calls[slot]), "total_ms": ph_ms[slot],
+                     "peak_source": f"{peak_key} of {pk_src}", "algorithmic": note}
+
+    add("k_gauss_labels_tc", 7, "tensor", 2.0 * N * k_mean * D * D, "TFLOP/s", bf16, "bf16_tflops",
+        f"2*N*K*D^2 FLOP per launch (one product; the split form issues 3), K mean {k_mean:.1f}",
+        label_kernel_traffic(N, k_mean))
+    add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
+        "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
+        "bound), its permutation index and r written; FP32 SIMT work 2*N*Dp^2 FLOP + the bounds")
+    add("k_prune_draw", 9, "hbm", N * 12.0 + kept * N * Dp * 4, "GB/s", hbm, "hbm_gbs",
+        "N*12 B (permutation, r, label) + the points of chunks that keep other clusters")
+    add("k_gauss_slot_stats", 10, "hbm", N * (2.0 * Dp * 4 + 12), "GB/s", hbm, "hbm_gbs",
+        "N*(2*Dp*4 + 12) B per launch: every point read once per sub-cluster pass, permutation, "
+        "sub-label; FP32 products N*Dp*(Dp+1)")
+    return out
+
+
 def c5_config(args):
     return dict(N=args.n, D=args.d, K_true=args.k_true, alpha=10.0, nu=args.d + 3.0, kappa=1.0, iterations=300,
                 mean_sd=5.0, dirichlet=2.0)
@@ -257,6 +297,8 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-points-per-core", type=int, default=600)
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
     ap.add_argument("--workload", default="c5", choices=["c5", "c4"],
                     help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time")
     ap.add_argument("--c4-sets", type=int, default=256)
@@ -339,6 +381,8 @@ def main():
         torch.cuda.synchronize()
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
+        if args.profile_region:
+            torch.cuda.profiler.start()
         e0.record(stream)
         for _ in range(args.steps):
             check(L.dpmm_sampler_step(h, 1))
@@ -347,14 +391,16 @@ def main():
             ks.append(kk.value)
         e1.record(stream)
         torch.cuda.synchronize()
+        if args.profile_region:
+            torch.cuda.profiler.stop()
         if dist:
             dist.barrier()
     elapsed_ms = e0.elapsed_time(e1)
     launches = L.dpmm_kernel_launch_count() - launches0
-    ph_ms = (ctypes.c_double * 8)()
-    ph_calls = (ctypes.c_int64 * 8)()
+    ph_ms = (ctypes.c_double * 11)()
+    ph_calls = (ctypes.c_int64 * 11)()
     check(L.dpmm_phase_times(ctx, 0, ph_ms, ph_calls))
-    prune = (ctypes.c_double * 4)()
+    prune = (ctypes.c_double * 6)()
     check(L.dpmm_label_pruning_stats(ctx, prune))
     h2d1, d2h1 = ctypes.c_uint64(), ctypes.c_uint64()
     L.dpmm_transfer_bytes(ctypes.byref(h2d1), ctypes.byref(d2h1))
@@ -377,23 +423,12 @@ def main():
     value = world * N * args.steps / (elapsed_ms / 1e3)
     pk, pk_src = peaks()
     k_mean = float(np.mean(ks)) if ks else float(k_before.value)
-    # dominant kernel: the tensor-core label kernel alone (slot 7), else the whole label phase
-    tc_kernel = ph_calls[7] > 0
-    label_ms = ph_ms[7] / ph_calls[7] if tc_kernel else ph_ms[0] / max(1, ph_calls[0])
-    flops = 2.0 * N * k_mean * D * D
-    achieved = flops / (label_ms / 1e3) / 1e12 if label_ms > 0 else None
-    peak = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
-    roofline = {"kernel": ("k_gauss_labels_tc (N x K whitened contraction, split-BF16 tcgen05, + drain to r)"
-                           if tc_kernel else "label phase (FP32 SIMT contraction + softmax + alias draw)"),
-                "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None,
-                "traffic": label_kernel_traffic(N, k_mean) if tc_kernel else None,
-                "peak_source": f"bf16_tflops of {pk_src}",
-                "launch_ms": label_ms, "launches": int(ph_calls[7] if tc_kernel else ph_calls[0]),
-                "algorithmic": f"2*N*K*D^2 FLOP per launch (one product; the split form issues 3), "
-                               f"K mean {k_mean:.1f}"}
+    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src)
+    # the roofline of the kernel with the most device time in the timed region
+    dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
+    roofline = dict(kernels[dominant], kernel=dominant) if dominant else None
     phases = ["labels", "sub_labels_stats", "stats", "split_hastings", "merge_hastings", "relabel", "params",
-              "label_tc_kernel"]
+              "label_tc_kernel", "label_prune_scan_kernel", "label_prune_draw_kernel", "slot_stats_kernel"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3" if mode != capi.LL_FP32 else "f32",
@@ -406,10 +441,13 @@ def main():
                        "nmi_vs_generating_labels": nmi,
                        "parameter_draws": "host" if args.host_draws else "device",
                        "label_pruning": {"attempts": int(prune[0]), "pruned_phases": int(prune[1]),
-                                         "kept_other_clusters_per_point": prune[2], "margin_nats": prune[3]},
+                                         "kept_other_clusters_per_point": prune[2], "margin_nats": prune[3],
+                                         "last_attempt_kept_per_point": prune[4],
+                                         "last_attempt_chunks_over_capacity": int(prune[5])},
                        "screen": screen_summary(args.screen, scr)},
             "gpu_launches": int(launches),
             "roofline": roofline,
+            "kernel_rooflines": kernels,
             "phase_ms_per_step": {p: ph_ms[i] / args.steps for i, p in enumerate(phases) if ph_calls[i]},
             "clocks": clk.summary()}
     line["clocks"].pop("samples", None)

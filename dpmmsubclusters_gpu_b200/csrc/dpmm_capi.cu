@@ -1099,5 +1099,7 @@ extern "C" dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* c, double* out)
     out[1] = (double)c->prune_used;
     out[2] = c->prune_used ? c->prune_extra / (double)c->prune_used : 0.0;
     out[3] = c->prune_margin;
+    out[4] = c->prune_last_extra;
+    out[5] = (double)c->prune_last_over;
     return DPMM_OK;
 }

@@ -64,7 +64,8 @@ extern std::atomic<uint64_t> g_launches, g_h2d_bytes, g_d2h_bytes;
     } while (0)
 
 enum Phase { PH_LABELS = 0, PH_SUB_STATS = 1, PH_STATS = 2, PH_SPLIT_HR = 3, PH_MERGE_HR = 4, PH_RELABEL = 5,
-             PH_PARAMS = 6, PH_LABEL_KERNEL = 7, PH_COUNT = 8 };
+             PH_PARAMS = 6, PH_LABEL_KERNEL = 7, PH_PRUNE_SCAN = 8, PH_PRUNE_DRAW = 9, PH_SLOT_STATS = 10,
+             PH_COUNT = 11 };
 
 #define DPMM_TRY(expr)                         \
     do {                                       \
@@ -190,6 +191,8 @@ struct dpmm_ctx {
     int prune_wait = 0;            // label phases to run dense before the next attempt
     int64_t prune_tries = 0, prune_used = 0;
     double prune_extra = 0;        // sum over used phases of kept other clusters per point
+    double prune_last_extra = 0;   // the last attempt's kept other clusters per point
+    int64_t prune_last_over = 0;   // ... and its chunks over the candidate-list capacity
     float* d_prune_rh = nullptr;   // [N] r of each point's current cluster, permutation order
     int32_t* d_prune_cand = nullptr; // [max_chunks][17] kept clusters per chunk
     float* d_prune_lam = nullptr;  // [KP], KP = min(k_max, 256) (the pruned phase takes K <= 256)

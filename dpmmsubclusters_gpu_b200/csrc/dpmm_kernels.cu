@@ -594,9 +594,10 @@ __global__ void __launch_bounds__(kPrTh) k_prune_scan(const float* __restrict__ 
     }
 }
 
-// pass 2, one block per chunk: labels.  A chunk without other clusters takes h + 1; otherwise, per
-// tile of kPrTh points, r of the kept clusters (r_h from pass 1), the others at -inf, and the draw
-// (or argmax) of the dense label phase over all K columns.  Shared memory: DP*DP + DP + K*kPrTh floats.
+// pass 2, one block per tile of kPrTh points of a chunk (blockIdx.x = chunk, blockIdx.y = tile): labels.
+// A chunk without other clusters takes h + 1; otherwise r of the kept clusters (r_h from pass 1; every
+// cluster when the chunk kept more than kPrMaxCand), the others at -inf, and the draw (or argmax) of
+// the dense label phase over all K columns.  Shared memory: DP*DP + DP + K*kPrTh floats.
 template <int DP>
 __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ x, const int32_t* __restrict__ perm,
                                                       const int32_t* __restrict__ chunk,
@@ -612,35 +613,38 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
     const int q = blockIdx.x, t = threadIdx.x;
     if (q >= *nchunks) return;
     const int h = chunk[3 * q], start = chunk[3 * q + 1], L = chunk[3 * q + 2];
+    const int base = start + (int)blockIdx.y * kPrTh;
+    if (base >= start + L) return;
     const int32_t* cq = cand + (size_t)q * (kPrMaxCand + 1);
     const int n = cq[0];
+    const int i = base + t;
+    const bool valid = i < start + L;
     if (n == 0) {
-        for (int i = start + t; i < start + L; i += blockDim.x) labels[perm[i]] = h + 1;
+        if (valid) labels[perm[i]] = h + 1;
         return;
     }
-    for (int base = start; base < start + L; base += blockDim.x) {
-        const int i = base + t;
-        const bool valid = i < start + L;
-        const int64_t pt = valid ? perm[i] : 0;
-        float xr[DP];
-        if (valid) load_row<DP>(x, pt, xr);
-        else
+    const bool all = n > kPrMaxCand;      // over capacity: every cluster
+    const int64_t pt = valid ? perm[i] : 0;
+    float xr[DP];
+    if (valid) load_row<DP>(x, pt, xr);
+    else
 #pragma unroll
-            for (int e = 0; e < DP; ++e) xr[e] = 0.f;
-        for (int k = 0; k < K; ++k) sr[k * kPrTh + t] = -INFINITY;
-        sr[h * kPrTh + t] = valid ? rh[i] : 0.f;
-        for (int a = 0; a < n; ++a) {
-            const int k = cq[1 + a];
-            __syncthreads();
-            const float4* src = reinterpret_cast<const float4*>(Wt + (size_t)3 * k * DP * DP);
-            float4* dst = reinterpret_cast<float4*>(sW);
-            for (int e = t; e < DP * DP / 4; e += blockDim.x) dst[e] = src[e];
-            for (int e = t; e < DP; e += blockDim.x) sbv[e] = bvec[(size_t)3 * k * DP + e];
-            __syncthreads();
-            sr[k * kPrTh + t] = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
-        }
-        if (valid) labels[pt] = draw_from_r<kPrTh>(sr, t, K, final_, rng, pt);
+        for (int e = 0; e < DP; ++e) xr[e] = 0.f;
+    for (int k = 0; k < K; ++k) sr[k * kPrTh + t] = -INFINITY;
+    sr[h * kPrTh + t] = valid ? rh[i] : 0.f;
+    const int m = all ? K : n;
+    for (int a = 0; a < m; ++a) {
+        const int k = all ? a : cq[1 + a];
+        if (k == h) continue;
+        __syncthreads();
+        const float4* src = reinterpret_cast<const float4*>(Wt + (size_t)3 * k * DP * DP);
+        float4* dst = reinterpret_cast<float4*>(sW);
+        for (int e = t; e < DP * DP / 4; e += blockDim.x) dst[e] = src[e];
+        for (int e = t; e < DP; e += blockDim.x) sbv[e] = bvec[(size_t)3 * k * DP + e];
+        __syncthreads();
+        sr[k * kPrTh + t] = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
     }
+    if (valid) labels[pt] = draw_from_r<kPrTh>(sr, t, K, final_, rng, pt);
 }
 
 static size_t prune_draw_smem(int DP, int K) { return sizeof(float) * ((size_t)DP * DP + DP + (size_t)K * kPrTh); }
@@ -655,10 +659,14 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     DPMM_CUDA_TRY(cudaMemsetAsync(c->d_prune_cnt, 0, 2 * sizeof(unsigned long long), c->stream));
     const size_t ssm = sizeof(float) * ((size_t)kChunkMax + (size_t)K * (DP + 3));
     DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_scan<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
-    k_prune_scan<DP><<<c->max_chunks, kPrTh, ssm, c->stream>>>(
-        c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c, c->d_mu, c->d_prune_lam, c->d_prune_M,
-        c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand, c->d_prune_cnt);
-    DPMM_LAUNCHED();
+    {
+        KernelTimer kt(c, PH_PRUNE_SCAN);
+        k_prune_scan<DP><<<c->max_chunks, kPrTh, ssm, c->stream>>>(
+            c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c, c->d_mu, c->d_prune_lam,
+            c->d_prune_M, c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand,
+            c->d_prune_cnt);
+        DPMM_LAUNCHED();
+    }
     unsigned long long* h = reinterpret_cast<unsigned long long*>(c->h_pinned);
     int32_t* outside = reinterpret_cast<int32_t*>(h + 2);   // points whose label has no chunk
     DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_prune_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
@@ -666,18 +674,26 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     DPMM_CUDA_TRY(cudaMemcpyAsync(outside, c->d_aux + 8 + K, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->prune_tries += 1;
-    const double extra = (double)h[0] / (double)c->N;
-    if (h[1] > 0 || extra > 0.5 || *outside != 0) {   // the bound keeps too much: the dense phase, and wait
-        c->prune_wait = 8;
+    const double extra = (double)h[0] / (double)c->N;   // kept other clusters per point
+    c->prune_last_extra = extra;
+    c->prune_last_over = (int64_t)h[1];
+    // each kept cluster costs about one more exact r per point; beyond 2 per point the dense phase
+    // (tensor cores where available) is the cheaper one: run it, and wait before the next attempt
+    if (extra > 2.0 || *outside != 0) {
+        c->prune_wait = 4;
         return DPMM_OK;
     }
     const RngArgs r = rng_args(c, d_u);
     const size_t sm = prune_draw_smem(DP, K);
     DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_draw<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_prune_draw<DP><<<c->max_chunks, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
-                                                             c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
-                                                             c->d_prune_cand, c->d_labels);
-    DPMM_LAUNCHED();
+    {
+        KernelTimer kt(c, PH_PRUNE_DRAW);
+        const dim3 grid((unsigned)c->max_chunks, (unsigned)((c->chunk_len + kPrTh - 1) / kPrTh));
+        k_prune_draw<DP><<<grid, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
+                                                        c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
+                                                        c->d_prune_cand, c->d_labels);
+        DPMM_LAUNCHED();
+    }
     c->prune_used += 1;
     c->prune_extra += extra;
     *used = true;
@@ -1509,6 +1525,7 @@ static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, fl
             const size_t sm = SlotStatsShape<DP>::bytes;
             auto kern = k_gauss_slot_stats<DP>;
             DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            KernelTimer kt(c, PH_SLOT_STATS);
             kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu,
                                                         c->d_sub, c->d_part, d_mask);
             DPMM_LAUNCHED();

@@ -319,10 +319,12 @@ dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, 
  * dpmm_create_clusters_labels (without loglik_out) evaluates, for each chunk of points of one current
  * cluster, only the clusters that an upper bound cannot put more than `margin` nats below the chunk's
  * own cluster; the left-out clusters carry less than K e^-margin of each point's probability and get
- * probability 0 in the same draw.  When the bound keeps too much (early iterations) the dense phase
- * runs and the next 8 label phases stay dense.  margin <= 0 switches it off (default 30).
+ * probability 0 in the same draw.  When the bound keeps more than 2 other clusters per point (early
+ * iterations) the dense phase runs and the next 4 label phases stay dense.  margin <= 0 switches it
+ * off (default 30).
  * stats: out[0] attempts, out[1] label phases run pruned, out[2] mean kept other clusters per point
- * in those, out[3] the margin. */
+ * in those, out[3] the margin, out[4] the last attempt's kept other clusters per point, out[5] its
+ * chunks that kept more than 16 (their points are evaluated against every cluster). */
 dpmm_status dpmm_set_label_pruning(dpmm_ctx* ctx, double margin);
 dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* ctx, double* out);
 
@@ -331,10 +333,12 @@ dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
 /* Diagnostics (no counterpart in the reference, which prints per-iteration wall times only):
  * kernels this library has launched in this process; bytes it copied host->device and
- * device->host; device time per phase of a context (ms[8], calls[8]: labels, sub-labels +
- * statistics, statistics only, split ratios, merge ratios, relabels, parameters, and the
- * tensor-core label kernel alone inside the label phase) accumulated while timing is on.  enable = 1 / 0 switches timing on / off and clears the counters, -1 only
- * reads them.  Timing adds one event synchronisation per phase. */
+ * device->host; device time per phase of a context (ms[11], calls[11]: labels, sub-labels +
+ * statistics, statistics only, split ratios, merge ratios, relabels, parameters, then single kernels
+ * inside those phases: the tensor-core label kernel, the pruned label phase's scan and draw kernels,
+ * and the sub-cluster statistics kernel) accumulated while timing is on.  enable = 1 / 0 switches
+ * timing on / off and clears the counters, -1 only reads them.  Timing adds one event
+ * synchronisation per phase and per timed kernel. */
 uint64_t dpmm_kernel_launch_count(void);
 void dpmm_transfer_bytes(uint64_t* h2d, uint64_t* d2h);
 dpmm_status dpmm_phase_times(dpmm_ctx* ctx, int enable, double* ms, int64_t* calls);

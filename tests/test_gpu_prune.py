@@ -31,7 +31,7 @@ def _mixture(seed, N, D, K, spread):
 
 
 def _stats(kern):
-    out = (ctypes.c_double * 4)()
+    out = (ctypes.c_double * 6)()
     check(lib().dpmm_label_pruning_stats(kern.ctx, out))
     return list(out)
 
@@ -75,4 +75,26 @@ def test_unprunable_state_falls_back_to_dense():
         lab[margin] = kern.get_labels()
     st = _stats(kern)
     assert st[0] == 1 and st[1] == 0, st
+    np.testing.assert_array_equal(lab[30.0], lab[0.0])
+
+
+def test_chunk_over_capacity_is_evaluated_against_every_cluster():
+    # 30 separated clusters; 3000 points drawn from all of them carry label 1, so the chunk(s) of
+    # cluster 0 keep more than 16 clusters: those points get every cluster, the rest stay pruned
+    K, N, D = 30, 200000, 8
+    x, z, mus, covs, rng = _mixture(17, N, D, K, 8.0)
+    kern = CudaKernel(prior_type.Gaussian, k_max=32).init(N, x.T, seed=1)
+    kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
+                             np.array([np.linalg.slogdet(c)[1] for c in covs]), np.full(K, 1.0 / K))
+    cur = (z + 1).astype(np.int32)
+    cur[rng.choice(N, 3000, replace=False)] = 1
+    u = uniforms(2 * N, 9)
+    lab = {}
+    for margin in (30.0, 0.0):
+        check(lib().dpmm_set_label_pruning(kern.ctx, margin))
+        kern.set_labels(cur)
+        kern.create_clusters_labels(K, False, u)
+        lab[margin] = kern.get_labels()
+    st = _stats(kern)
+    assert st[1] == 1 and st[5] >= 1, st
     np.testing.assert_array_equal(lab[30.0], lab[0.0])
