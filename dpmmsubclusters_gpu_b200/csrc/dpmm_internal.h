@@ -23,6 +23,10 @@ constexpr int kMaxMultDim = 4096;
 // kChunkUnit and kChunkMax, the smallest that still gives about four waves of blocks.
 constexpr int kChunkUnit = 1024;
 constexpr int kChunkMax = 4096;
+// Pruned label phase: at most kMaxKForPrune clusters; a chunk keeps at most kPrMaxCand other
+// clusters before it is evaluated against every cluster.
+constexpr int kMaxKForPrune = 256;
+constexpr int kPrMaxCand = 16;
 
 // Learned split/merge screen (dpmm_screen.cu): 32 features per candidate, a 32 -> 64 -> 64 -> 1 MLP
 // whose parameters are one FP32 vector W1[64][32], b1[64], W2[64][64], b2[64], w3[64], b3.
@@ -317,6 +321,9 @@ size_t tc_param_bytes(int k_max);          // B tiles + bias records for k_max c
 // tensor-core sub-label kernel (dpmm_tc.cu): draws the sub-labels only (statistics separately)
 bool tc_sub_supported(const dpmm_ctx* c);
 dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout);
+// pass 1 of the pruned label phase on the tensor cores (dpmm_tc.cu; Dp = 32 or 64, packed B tiles)
+bool tc_scan_supported(const dpmm_ctx* c, int K);
+dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)

@@ -386,8 +386,6 @@ dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d
 // it at probability 0, which gives the dense draw's label unless a uniform falls inside that mass.  A
 // chunk left with its own cluster only takes it as every point's label.
 constexpr int kPrTh = 128;       // threads per block
-constexpr int kMaxKForPrune = 256;
-constexpr int kPrMaxCand = 16;   // other clusters a chunk may keep (more: the dense phase runs)
 
 // one block per cluster k: lam[k] = sqrt of the Gershgorin bound of lambda_max(W_k W_k^T) (inflated);
 // for every h: M[h][k] (deflated), v[h][k][DP] and beta[h][k]
@@ -657,9 +655,15 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
                                                  c->d_prune_beta);
     DPMM_LAUNCHED();
     DPMM_CUDA_TRY(cudaMemsetAsync(c->d_prune_cnt, 0, 2 * sizeof(unsigned long long), c->stream));
-    const size_t ssm = sizeof(float) * ((size_t)kChunkMax + (size_t)K * (DP + 3));
-    DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_scan<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
-    {
+    int32_t* d_err = c->d_aux + 7;
+    DPMM_CUDA_TRY(cudaMemsetAsync(d_err, 0, sizeof(int32_t), c->stream));
+    if (tc_scan_supported(c, K)) {
+        // r_h and the point bounds as tensor-core products (r_h then equals the dense tensor-core r)
+        KernelTimer kt(c, PH_PRUNE_SCAN);
+        DPMM_TRY(launch_prune_scan_tc(c, K, d_err));
+    } else {
+        const size_t ssm = sizeof(float) * ((size_t)kChunkMax + (size_t)K * (DP + 3));
+        DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_scan<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ssm));
         KernelTimer kt(c, PH_PRUNE_SCAN);
         k_prune_scan<DP><<<c->max_chunks, kPrTh, ssm, c->stream>>>(
             c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt, c->d_b, c->d_c, c->d_mu, c->d_prune_lam,
@@ -672,7 +676,10 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_prune_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                   c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(outside, c->d_aux + 8 + K, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(outside + 1, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (outside[1])
+        return fail(DPMM_ERR_TIMEOUT, "tensor-core scan: bounded wait expired (code " + std::to_string(outside[1]) + ")");
     c->prune_tries += 1;
     const double extra = (double)h[0] / (double)c->N;   // kept other clusters per point
     c->prune_last_extra = extra;

@@ -792,6 +792,331 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
     }
 }
 
+// ------------------------------------------------------------------------- pruned-phase scan
+// Pass 1 of the pruned label phase (the bounds are stated at k_prune_scan, dpmm_kernels.cu) on the
+// tensor cores, one CTA per chunk of cluster h:
+//   phase 1  per 128-point tile, the gathered rows (split BF16, swizzled) times the dense phase's
+//            packed B tile h / 2 give z_h in accumulator columns (h % 2) * 64 ..; 8 warps drain
+//            r_h = c_h - |z_h - b_h|^2 / 2 (the dense tensor-core phase's r of the point's own
+//            cluster, from the same operands); |x - mu_h|^2 comes from the FP32 rows;
+//   chunk    with the CTA's r_min and radius R the chunk bound leaves out clusters; the others
+//            (ascending) become the rows of a candidate B operand [v_hk] (split BF16, 1-2 tiles);
+//   phase 2  per tile the rows again times the candidate operand give v_hk^T x, and candidate k is
+//            kept when c_k - (v_hk^T x - beta_hk)^2 / 2 >= r_h - margin at some point of the chunk.
+// Shared memory below (about 102 KB: two CTAs per SM); 256 TMEM columns.
+constexpr int kScanMaxK = 256;
+struct ScanSmem {
+    static constexpr size_t a = 0;                               // 32 KB A tile (hi, lo)
+    static constexpr size_t b = a + A_TILE;                      // 64 KB: h's B tile, then candidate tiles
+    static constexpr size_t sq = b + 2 * STAGE_BYTES;            // [2][BM] partial |z - b|^2
+    static constexpr size_t bias = sq + 2 * BM * 4;              // b_h, mu_h: [2][KD] floats
+    static constexpr size_t cb = bias + 2 * KD * 4;              // beta, c of the candidates: [2][kScanMaxK]
+    static constexpr size_t ck = cb + 2 * kScanMaxK * 4;         // candidate clusters [kScanMaxK] ints
+    static constexpr size_t bits = ck + kScanMaxK * 4;           // kept bits [8], warp r_min / R^2 [16], counts [8]
+    static constexpr size_t bar = bits + 32 * 4;                 // mbarrier, tmem slot, flag
+    static constexpr size_t total = bar + 32 + 1024;             // + alignment slack
+};
+static_assert(ScanSmem::bar % 8 == 0, "mbarrier alignment");
+constexpr uint32_t SCAN_TMEM_COLS = 2 * BN;
+
+template <int DP>
+__global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const uint8_t* __restrict__ Btc, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, const float* __restrict__ mu, const float* __restrict__ lam,
+    const float* __restrict__ M, const float* __restrict__ V, const float* __restrict__ beta, int K, float margin,
+    float* __restrict__ rh, int32_t* __restrict__ cand, unsigned long long* __restrict__ cnt,
+    int32_t* __restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem + ScanSmem::a;
+    uint8_t* sB = smem + ScanSmem::b;
+    float* sq = reinterpret_cast<float*>(smem + ScanSmem::sq);
+    float* sbias = reinterpret_cast<float*>(smem + ScanSmem::bias);
+    float* sbeta = reinterpret_cast<float*>(smem + ScanSmem::cb);
+    float* sck = sbeta + kScanMaxK;
+    int32_t* sk = reinterpret_cast<int32_t*>(smem + ScanSmem::ck);
+    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + ScanSmem::bits);
+    float* wred = reinterpret_cast<float*>(kbits + kScanMaxK / 32);
+    int32_t* wcnt = reinterpret_cast<int32_t*>(wred + 16);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + ScanSmem::bar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int q = blockIdx.x;
+    if (q >= *nchunks) return;
+    const int h = chunk[3 * q], start = chunk[3 * q + 1], len = chunk[3 * q + 2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(Btc + (size_t)(h / CPT) * STAGE_BYTES);
+        uint4* dst = reinterpret_cast<uint4*>(sB);
+        for (int e = tid; e < STAGE_BYTES / 16; e += 256) dst[e] = src[e];
+        if (tid < 2 * KD) {
+            const int side = tid / KD, j = tid % KD;
+            sbias[tid] = j < DP ? (side ? mu : bvec)[(size_t)3 * h * DP + j] : 0.f;
+        }
+        if (tid < kScanMaxK / 32) kbits[tid] = 0u;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(SCAN_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t lane_addr = (uint32_t)((warp & 3) * 32) << 16;
+    const float ch = cvec[3 * h];
+
+    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8)
+    float4 pf[4][2];
+    auto load_rows = [&](int t0) {
+        const int ntn = min(BM, len - t0);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pf[u][1] = pf[u][0];
+            if (row < ntn && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + row) * DP + c8 * 8);
+                pf[u][0] = __ldg(src);
+                pf[u][1] = __ldg(src + 1);
+            }
+        }
+    };
+    // A tile (split BF16, 128-byte swizzle) from the rows; with want_r2, the largest |x - mu_h|^2
+    auto build_a = [&](int ntn, bool want_r2, float& r2max) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            const float v[8] = {pf[u][0].x, pf[u][0].y, pf[u][0].z, pf[u][0].w,
+                                pf[u][1].x, pf[u][1].y, pf[u][1].z, pf[u][1].w};
+            __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) bf16_split(v[e], hi[e], lo[e]);
+            const uint32_t off = sw128_offset(row, c8 * 8);
+            *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(hi);
+            *reinterpret_cast<uint4*>(sA + A_BYTES + off) = *reinterpret_cast<const uint4*>(lo);
+            if (want_r2) {
+                float d2 = 0.f;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const float t = v[e] - sbias[KD + c8 * 8 + e];
+                    d2 = fmaf(t, t, d2);
+                }
+                d2 += __shfl_xor_sync(0xffffffffu, d2, 1);
+                d2 += __shfl_xor_sync(0xffffffffu, d2, 2);
+                d2 += __shfl_xor_sync(0xffffffffu, d2, 4);
+                if (row < ntn) r2max = fmaxf(r2max, d2);
+            }
+        }
+    };
+    // one tile's MMAs (12 per 128-column B tile) and the bounded wait for them; block-uniform result
+    uint32_t phase = 0;
+    const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
+    auto mma_tile = [&](int nbt) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            for (int nb = 0; nb < nbt; ++nb) {
+                const uint8_t* bt = sB + (size_t)nb * STAGE_BYTES;
+                const uint64_t db_h = sw128_desc(smem_u32(bt)), db_l = sw128_desc(smem_u32(bt + B_BYTES));
+                const uint32_t td = tmem_base + (uint32_t)(nb * BN);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_l + 2 * ks, db_h + 2 * ks, 1u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_h + 2 * ks, db_l + 2 * ks, 1u);
+            }
+            umma_commit(bar);
+        }
+    };
+    auto mma_wait = [&]() -> bool {
+        if (tid == 0) {
+            if (!mbar_wait_bounded(bar, phase & 1, gerr)) {
+                atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+                *flag = 1;
+            }
+        }
+        ++phase;
+        __syncthreads();
+        if (*flag) return false;
+        tc_fence_after();
+        return true;
+    };
+
+    bool failed = false;
+    // phase 1: r_h, r_min, radius
+    float tmin = INFINITY, r2max = 0.f;
+    if (len > 0) load_rows(0);
+    for (int t0 = 0; t0 < len; t0 += BM) {
+        const int ntn = min(BM, len - t0);
+        build_a(ntn, true, r2max);
+        mma_tile(1);
+        if (t0 + BM < len) load_rows(t0 + BM);   // the next tile's rows load while the MMAs run
+        if (!mma_wait()) { failed = true; break; }
+        {
+            const int part = warp >> 2;
+            float qs = 0.f;
+            if (DP > 32 || part == 0) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + lane_addr + (uint32_t)((h % CPT) * KD + 32 * part), v);
+                const float* bs = sbias + 32 * part;
+                float q1 = 0.f;
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    const float z0 = __uint_as_float(v[j]) - bs[j];
+                    const float z1 = __uint_as_float(v[j + 1]) - bs[j + 1];
+                    qs = fmaf(z0, z0, qs);
+                    q1 = fmaf(z1, z1, q1);
+                }
+                qs += q1;
+            }
+            sq[part * BM + (warp & 3) * 32 + lane] = qs;
+        }
+        tc_fence_before();
+        __syncthreads();
+        if (tid < ntn) {
+            const float r = ch - 0.5f * (sq[tid] + sq[BM + tid]);
+            rh[start + t0 + tid] = r;
+            tmin = fminf(tmin, r);
+        }
+    }
+    int nt = 0;
+    if (!failed) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+            r2max = fmaxf(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
+        }
+        if (lane == 0) {
+            wred[warp] = tmin;
+            wred[8 + warp] = r2max;
+        }
+        __syncthreads();
+        float rmin = wred[0], r2 = wred[8];
+        for (int w = 1; w < 8; ++w) {
+            rmin = fminf(rmin, wred[w]);
+            r2 = fmaxf(r2, wred[8 + w]);
+        }
+        const float R = sqrtf(r2) * 1.0001f + 1e-4f;
+        // chunk bound, thread k: surviving clusters listed in ascending order
+        bool keep_k = false;
+        if (tid < K && tid != h) {
+            const float d = M[(size_t)h * K + tid] - lam[tid] * R;
+            const float ub = cvec[3 * tid] - 0.5f * (d > 0.f ? d * d : 0.f);
+            keep_k = !(ub < rmin - margin);
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, keep_k);
+        if (lane == 0) wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0;
+        for (int w = 0; w < 8; ++w) {
+            const int cw = wcnt[w];
+            off += w < warp ? cw : 0;
+            nt += cw;
+        }
+        if (keep_k) sk[off + __popc(bal & ((1u << lane) - 1u))] = tid;
+        __syncthreads();
+        if (nt > 0) {
+            // candidate operand: row a = v_{h, sk[a]} (split BF16), zero rows up to the tile edge
+            const int nbt = (nt + BN - 1) / BN;
+            for (int e = tid; e < nbt * BN * 8; e += 256) {
+                const int n = e / 8, c8 = e % 8;
+                float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                if (n < nt && c8 * 8 < DP) {
+                    const float4* src = reinterpret_cast<const float4*>(V + ((size_t)h * K + sk[n]) * DP + c8 * 8);
+                    const float4 a = src[0], b = src[1];
+                    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+                    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+                }
+                __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) bf16_split(v[j], hi[j], lo[j]);
+                uint8_t* base = sB + (size_t)(n / BN) * STAGE_BYTES;
+                const uint32_t o = sw128_offset(n % BN, c8 * 8);
+                *reinterpret_cast<uint4*>(base + o) = *reinterpret_cast<const uint4*>(hi);
+                *reinterpret_cast<uint4*>(base + B_BYTES + o) = *reinterpret_cast<const uint4*>(lo);
+            }
+            for (int a = tid; a < nt; a += 256) {
+                sbeta[a] = beta[(size_t)h * K + sk[a]];
+                sck[a] = cvec[3 * sk[a]];
+            }
+            // phase 2: point bound
+            load_rows(0);
+            for (int t0 = 0; t0 < len; t0 += BM) {
+                const int ntn = min(BM, len - t0);
+                float unused = 0.f;
+                build_a(ntn, false, unused);
+                mma_tile(nbt);
+                if (t0 + BM < len) load_rows(t0 + BM);
+                const int row = (warp & 3) * 32 + lane;
+                const bool valid = row < ntn;
+                const float lim = valid ? rh[start + t0 + row] - margin : 0.f;
+                if (!mma_wait()) { failed = true; break; }
+                const int part = warp >> 2;
+                for (int nb = 0; nb < nbt; ++nb) {
+#pragma unroll
+                    for (int s = 0; s < 2; ++s) {
+                        const int a0 = nb * BN + 64 * part + 32 * s;
+                        if (a0 >= nt) continue;   // warp-uniform
+                        uint32_t v[32];
+                        tmem_ld32(tmem_base + lane_addr + (uint32_t)a0, v);
+                        uint32_t m = 0u;
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) {
+                            const int a = a0 + j;
+                            if (a < nt) {
+                                const float p = __uint_as_float(v[j]) - sbeta[a];
+                                const float ub = sck[a] - 0.5f * p * p;
+                                if (!(ub < lim)) m |= 1u << j;
+                            }
+                        }
+                        if (!valid) m = 0u;
+                        m = __reduce_or_sync(0xffffffffu, m);
+                        if (lane == 0 && m) atomicOr(&kbits[a0 >> 5], m);
+                    }
+                }
+                tc_fence_before();
+                __syncthreads();
+            }
+        }
+    }
+    __syncthreads();
+    if (!failed && tid == 0) {
+        int n = 0;
+        int32_t* cq = cand + (size_t)q * (kPrMaxCand + 1);
+        for (int a = 0; a < nt; ++a)
+            if ((kbits[a >> 5] >> (a & 31)) & 1u) {
+                if (n < kPrMaxCand) cq[1 + n] = sk[a];
+                ++n;
+            }
+        cq[0] = n;
+        atomicAdd(&cnt[0], (unsigned long long)n * (unsigned long long)len);
+        if (n > kPrMaxCand) atomicAdd(&cnt[1], 1ull);
+    }
+    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(SCAN_TMEM_COLS));
+    }
+}
+
 }  // namespace tc
 
 constexpr size_t kTcSmemCap = 227 * 1024;
@@ -913,6 +1238,31 @@ dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout)
     if (h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core sub-label kernel: bounded wait expired (code " +
                                                  std::to_string(h_err) + ")");
     return DPMM_OK;
+}
+
+bool tc_scan_supported(const dpmm_ctx* c, int K)
+{
+    return c->ll_mode != DPMM_LL_FP32 && tc_supported(c, K) && K <= tc::kScanMaxK;
+}
+
+template <int DP>
+static dpmm_status launch_prune_scan_tc_t(dpmm_ctx* c, int K, int32_t* err)
+{
+    auto kern = tc::k_prune_scan_tc<DP>;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::ScanSmem::total));
+    kern<<<c->max_chunks, 256, tc::ScanSmem::total, c->stream>>>(
+        c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Btc, c->d_b, c->d_c, c->d_mu, c->d_prune_lam, c->d_prune_M,
+        c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand, c->d_prune_cnt, err);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+// the caller clears *d_err before and reads it after (with the pass's counters)
+dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err)
+{
+    if (!tc_scan_supported(c, K)) return fail(DPMM_ERR_INVALID_ARG, "tensor-core scan: unsupported shape");
+    if (c->Dp == 64) return launch_prune_scan_tc_t<64>(c, K, d_err);
+    return launch_prune_scan_tc_t<32>(c, K, d_err);
 }
 
 }  // namespace dpmm

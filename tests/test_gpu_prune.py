@@ -36,7 +36,8 @@ def _stats(kern):
     return list(out)
 
 
-@pytest.mark.parametrize("D,mode", [(16, None), (64, None), (32, LL_FP32)])
+# D = 32 / 64 in the default mode: the scan runs on the tensor cores; D = 16 and FP32 mode: SIMT
+@pytest.mark.parametrize("D,mode", [(16, None), (64, None), (32, None), (32, LL_FP32)])
 def test_pruned_labels_equal_dense_labels(D, mode):
     K, N = 10, 60000
     x, z, mus, covs, rng = _mixture(D, N, D, K, 6.0)
@@ -78,16 +79,17 @@ def test_unprunable_state_falls_back_to_dense():
     np.testing.assert_array_equal(lab[30.0], lab[0.0])
 
 
-def test_chunk_over_capacity_is_evaluated_against_every_cluster():
-    # 30 separated clusters; 3000 points drawn from all of them carry label 1, so the chunk(s) of
-    # cluster 0 keep more than 16 clusters: those points get every cluster, the rest stay pruned
-    K, N, D = 30, 200000, 8
+@pytest.mark.parametrize("K,N,D,planted", [(30, 200000, 8, 3000), (30, 200000, 64, 3000), (150, 150000, 32, 600)])
+def test_chunk_over_capacity_is_evaluated_against_every_cluster(K, N, D, planted):
+    # separated clusters; points drawn from all of them carry label 1, so the chunk(s) of cluster 0
+    # keep more than 16 clusters: those points get every cluster, the rest stay pruned.  With 150
+    # clusters the chunk bound keeps more than 128 candidates (two candidate tiles on the tensor cores).
     x, z, mus, covs, rng = _mixture(17, N, D, K, 8.0)
-    kern = CudaKernel(prior_type.Gaussian, k_max=32).init(N, x.T, seed=1)
+    kern = CudaKernel(prior_type.Gaussian, k_max=K + 2).init(N, x.T, seed=1)
     kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
                              np.array([np.linalg.slogdet(c)[1] for c in covs]), np.full(K, 1.0 / K))
     cur = (z + 1).astype(np.int32)
-    cur[rng.choice(N, 3000, replace=False)] = 1
+    cur[rng.choice(N, planted, replace=False)] = 1
     u = uniforms(2 * N, 9)
     lab = {}
     for margin in (30.0, 0.0):
