@@ -10,6 +10,11 @@
 
 namespace dpmm {
 
+// Upper-triangle pair count of the scatter matrix, and the index of (i, j), i <= j, in its
+// row-major upper triangle (the layout of the statistics records)
+__host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
+__host__ __device__ constexpr int tri_index(int dp, int i, int j) { return i * dp - i * (i - 1) / 2 + (j - i); }
+
 // Philox4x32-10 (Salmon, Moraes, Dror, Shaw: "Parallel random numbers: as easy as 1, 2, 3",
 // SC'11): ten rounds of the 4x32 bijection keyed by a 64-bit key, with the multipliers and
 // Weyl key increments published in that paper.

@@ -324,6 +324,9 @@ dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout);
 // pass 1 of the pruned label phase on the tensor cores (dpmm_tc.cu; Dp = 32 or 64, packed B tiles)
 bool tc_scan_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err);
+// sub-cluster statistics (sub-labels given) on the tensor cores (dpmm_tc.cu; Dp = 32 or 64)
+bool tc_stats_supported(const dpmm_ctx* c);
+dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)

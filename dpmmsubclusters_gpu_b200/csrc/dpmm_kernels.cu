@@ -863,8 +863,6 @@ dpmm_status build_permutation(dpmm_ctx* c, int K)
 }
 
 // ----------------------------------------------------------------------------- sub-labels + stats
-// Upper-triangle pair count of the scatter matrix
-__host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
 
 // Gaussian: one block per chunk of one cluster (points in permutation order).  Draws the
 // sub-labels (unless draw == 0, in which case the current sub-labels are used) and accumulates
@@ -879,10 +877,6 @@ __host__ __device__ constexpr int tri(int dp) { return dp * (dp + 1) / 2; }
 //           tile; FP64 totals per thread live in shared memory and are summed over the groups at
 //           the end.
 // DP = 128: one thread per point for the draw, one matrix entry per thread through a pair table.
-__host__ __device__ constexpr int tri_index(int dp, int i, int j)   // row-major upper triangle, i <= j
-{
-    return i * dp - i * (i - 1) / 2 + (j - i);
-}
 
 template <int DP>
 struct SubStatsShape {
@@ -1528,6 +1522,7 @@ template <int DP>
 static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, float* d_rout, const uint8_t* d_mask)
 {
     if constexpr (DP <= 64) {
+        if (!draw && tc_stats_supported(c)) return launch_slot_stats_tc(c, d_mask);
         if (!draw) {
             const size_t sm = SlotStatsShape<DP>::bytes;
             auto kern = k_gauss_slot_stats<DP>;

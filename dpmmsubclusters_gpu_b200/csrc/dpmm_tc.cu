@@ -682,23 +682,33 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
     const float cl = cvec[3 * k + 1], cr = cvec[3 * k + 2];
     const float wl = lrw[2 * k], wr = lrw[2 * k + 1];
 
-    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8)
+    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8); a tile's
+    // permutation entries load one tile ahead of its rows
     float4 pf[4][2];
-    auto load_rows = [&](int t0) {
-        const int ntn = min(BM, len - t0);
+    int pq[4];
+    auto load_perm = [&](int t0) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            const int row = (tid >> 3) + 32 * u;
+            pq[u] = t0 + row < len ? __ldg(perm + start + t0 + row) : -1;
+        }
+    };
+    auto load_rows = [&]() {   // rows of the tile whose entries pq holds
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c8 = tid & 7;
             pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
             pf[u][1] = pf[u][0];
-            if (row < ntn && c8 * 8 < DP) {
-                const float4* src = reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + row) * DP + c8 * 8);
+            if (pq[u] >= 0 && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(x + (size_t)pq[u] * DP + c8 * 8);
                 pf[u][0] = __ldg(src);
                 pf[u][1] = __ldg(src + 1);
             }
         }
     };
-    load_rows(0);
+    load_perm(0);
+    load_rows();
+    load_perm(BM);
     uint32_t phase = 0;
     bool failed = false;
     const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
@@ -731,7 +741,10 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
             for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(tmem_base, da_h + 2 * ks, db_l + 2 * ks, 1u);
             umma_commit(bar);
         }
-        if (t0 + BM < len) load_rows(t0 + BM);   // the next tile's rows load while the MMAs run
+        if (t0 + BM < len) {   // the next tile's rows load while the MMAs run
+            load_rows();
+            load_perm(t0 + 2 * BM);
+        }
         if (tid == 0) {
             if (!mbar_wait_bounded(bar, phase & 1, gerr)) {
                 atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
@@ -878,17 +891,25 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
     const uint32_t lane_addr = (uint32_t)((warp & 3) * 32) << 16;
     const float ch = cvec[3 * h];
 
-    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8)
+    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8); a tile's
+    // permutation entries load one tile ahead of its rows
     float4 pf[4][2];
-    auto load_rows = [&](int t0) {
-        const int ntn = min(BM, len - t0);
+    int pq[4];
+    auto load_perm = [&](int t0) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
-            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            const int row = (tid >> 3) + 32 * u;
+            pq[u] = t0 + row < len ? __ldg(perm + start + t0 + row) : -1;
+        }
+    };
+    auto load_rows = [&]() {   // rows of the tile whose entries pq holds
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c8 = tid & 7;
             pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
             pf[u][1] = pf[u][0];
-            if (row < ntn && c8 * 8 < DP) {
-                const float4* src = reinterpret_cast<const float4*>(x + (size_t)__ldg(perm + start + t0 + row) * DP + c8 * 8);
+            if (pq[u] >= 0 && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(x + (size_t)pq[u] * DP + c8 * 8);
                 pf[u][0] = __ldg(src);
                 pf[u][1] = __ldg(src + 1);
             }
@@ -961,12 +982,17 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
     bool failed = false;
     // phase 1: r_h, r_min, radius
     float tmin = INFINITY, r2max = 0.f;
-    if (len > 0) load_rows(0);
+    load_perm(0);
+    load_rows();
+    load_perm(BM);
     for (int t0 = 0; t0 < len; t0 += BM) {
         const int ntn = min(BM, len - t0);
         build_a(ntn, true, r2max);
         mma_tile(1);
-        if (t0 + BM < len) load_rows(t0 + BM);   // the next tile's rows load while the MMAs run
+        if (t0 + BM < len) {   // the next tile's rows load while the MMAs run
+            load_rows();
+            load_perm(t0 + 2 * BM);
+        }
         if (!mma_wait()) { failed = true; break; }
         {
             const int part = warp >> 2;
@@ -1056,13 +1082,18 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
                 sck[a] = cvec[3 * sk[a]];
             }
             // phase 2: point bound
-            load_rows(0);
+            load_perm(0);
+            load_rows();
+            load_perm(BM);
             for (int t0 = 0; t0 < len; t0 += BM) {
                 const int ntn = min(BM, len - t0);
                 float unused = 0.f;
                 build_a(ntn, false, unused);
                 mma_tile(nbt);
-                if (t0 + BM < len) load_rows(t0 + BM);
+                if (t0 + BM < len) {
+                    load_rows();
+                    load_perm(t0 + 2 * BM);
+                }
                 const int row = (warp & 3) * 32 + lane;
                 const bool valid = row < ntn;
                 const float lim = valid ? rh[start + t0 + row] - margin : 0.f;
@@ -1114,6 +1145,342 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(SCAN_TMEM_COLS));
+    }
+}
+
+
+// ------------------------------------------------------------------------- slot statistics
+// Statistics of the two sub-clusters of one chunk (cluster k, sub-labels given) on the tensor
+// cores, Dp = 32 or 64: count, sum c and the upper triangle of sum c c^T over each sub-cluster's
+// points, c = x - mu_k (mu_k the cluster's mean parameter), the partial records of
+// k_gauss_slot_stats (dpmm_kernels.cu).  Per tile of 32 points:
+//   A (128 rows x 32 points, K-major TF32)  row i < Dp: c_i where the sub-label is 1, else 0;
+//                                           row 64 + i: c_i where it is 2
+//   B (Dp + 16 rows x 32 points)            row j < Dp: c_j; row Dp: ones; the rest zero
+//   D = A B^T (M = 128, N = Dp + 16)        D[64 s + i][j] = sum c_i c_j, D[64 s + i][Dp] = sum c_i
+// The operands are split TF32 (hi = rna(c), lo = rna(c - hi), |c - hi - lo| <= 2^-22 |c|) and
+// D = A_hi B_hi + A_lo B_hi + A_hi B_lo (12 tcgen05.mma of K = 8).  The accumulator runs over a
+// group of ST_G tiles (FP32 over 128 points: 48 accumulator roundings) and is then added into FP64
+// registers; two accumulators in TMEM alternate by group.  The products are centred at the mean a
+// of the chunk's first tile (within a cluster's spread of every point, wherever mu_k lies) and the
+// totals moved to mu_k in FP64 at the end:
+//   sum (x-mu)(x-mu)^T = S_a + d S1^T + S1 d^T + n d d^T,  sum (x-mu) = S1 + n d,  d = a - mu.
+// Pipeline: tile t + 3's rows and sub-labels (gathered through permutation entries that were
+// staged three tiles earlier, all by cp.async) are in flight while tile t is split and transposed
+// into the operands; a group's accumulator is drained while the next group's MMAs run.  Every wait
+// is bounded.
+constexpr int ST_P = 32;                   // points per tile: one 128-byte TF32 K row
+constexpr int ST_STAGES = 4;               // staged tiles of rows (3 in flight)
+constexpr int ST_PERM = 8;                 // staged tiles of permutation entries
+constexpr int ST_G = 4;                    // tiles per accumulation group
+constexpr uint32_t ST_TMEM_COLS = 256;     // two accumulators, at columns 0 and 128
+
+template <int DP>
+struct StatSmem {
+    static constexpr int N = DP + 16;                                   // B rows
+    static constexpr int SX = DP + 4;                                   // staged row stride (floats)
+    static constexpr size_t a_hi = 0;                                   // 128 rows x 128 B
+    static constexpr size_t a_lo = a_hi + 128 * 128;
+    static constexpr size_t b_hi = a_lo + 128 * 128;                    // N rows x 128 B
+    static constexpr size_t b_lo = b_hi + (size_t)N * 128;
+    static constexpr size_t stage = b_lo + (size_t)N * 128;             // [ST_STAGES][ST_P][SX] floats
+    static constexpr size_t ssub = stage + (size_t)ST_STAGES * ST_P * SX * 4;   // [ST_STAGES][ST_P] ints
+    static constexpr size_t sperm = ssub + (size_t)ST_STAGES * ST_P * 4;        // [ST_PERM][ST_P] ints
+    static constexpr size_t shift = sperm + (size_t)ST_PERM * ST_P * 4;         // [DP] floats
+    static constexpr size_t bar = shift + (size_t)DP * 4;               // mbarrier, tmem slot, flag
+    static constexpr size_t total = bar + 32 + 1024;                    // + alignment slack
+};
+
+// byte offset of 4-byte element k of row r in a K-major tile with 128-byte swizzle
+__host__ __device__ constexpr uint32_t sw128_offset32(int row, int k)
+{
+    return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 2) ^ (row & 7)) & 7) << 4) + (k & 3) * 4);
+}
+
+// round to TF32 (10 explicit mantissa bits), nearest with ties away from zero: add half of the
+// dropped 13-bit field to the magnitude and clear it (finite inputs; integer pipe)
+__device__ __forceinline__ float tf32_rna(float v)
+{
+    return __uint_as_float((__float_as_uint(v) + 0x1000u) & 0xFFFFE000u);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                          uint32_t accum)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld1(uint32_t taddr, uint32_t& r)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x1.b32 {%0}, [%1];" : "=r"(r) : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, uint32_t src_bytes)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <int DP>
+__global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const float* __restrict__ muv, const int32_t* __restrict__ sub,
+    double* __restrict__ part, const uint8_t* __restrict__ mask, int32_t* __restrict__ err)
+{
+    using L = StatSmem<DP>;
+    constexpr int N = L::N, SX = L::SX;
+    constexpr int SL = 1 + DP + tri(DP);
+    constexpr int C4 = DP / 4;                     // float4 per row
+    constexpr int ITEMS = ST_P * C4 / 256;         // row pieces per thread per tile
+    static_assert(ITEMS >= 1 && ST_P * C4 % 256 == 0, "tile shape");
+    constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    float* stage = reinterpret_cast<float*>(smem + L::stage);
+    int32_t* ssub = reinterpret_cast<int32_t*>(smem + L::ssub);
+    int32_t* sperm = reinterpret_cast<int32_t*>(smem + L::sperm);
+    float* sshift = reinterpret_cast<float*>(smem + L::shift);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    if (mask && !mask[k]) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+    const int ntiles = (len + ST_P - 1) / ST_P;
+
+    // operands zeroed once (rows past Dp stay zero), then the ones row of B
+    for (int e = tid; e < (int)(L::stage / 16); e += 256) reinterpret_cast<uint4*>(smem)[e] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ST_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    if (tid < ST_P) *reinterpret_cast<float*>(smem + L::b_hi + sw128_offset32(DP, tid)) = 1.0f;
+
+    // loader pieces (cp.async; the caller commits)
+    auto issue_perm = [&](int t) {   // permutation entries of tile t (threads 0..31; 0 past the chunk)
+        if (t < ntiles && tid < ST_P) {
+            const int i = t * ST_P + tid;
+            const bool ok = i < len;
+            cp_async4(sperm + (t % ST_PERM) * ST_P + tid, ok ? perm + start + i : perm, ok ? 4u : 0u);
+        }
+    };
+    auto issue_rows = [&](int t) {   // rows and sub-labels of tile t (zero past the chunk)
+        if (t >= ntiles) return;
+        float* sb = stage + (size_t)(t % ST_STAGES) * ST_P * SX;
+        int32_t* sbs = ssub + (t % ST_STAGES) * ST_P;
+        const int32_t* pp = sperm + (t % ST_PERM) * ST_P;
+#pragma unroll
+        for (int u = 0; u < ITEMS; ++u) {
+            const int e = tid + 256 * u, row = e / C4, c4 = e % C4;
+            const bool ok = t * ST_P + row < len;
+            const int64_t pt = ok ? pp[row] : 0;
+            cp_async16(sb + row * SX + 4 * c4, x + (size_t)pt * DP + 4 * c4, ok ? 16u : 0u);
+            if (c4 == 0) cp_async4(sbs + row, sub + pt, ok ? 4u : 0u);
+        }
+    };
+    // prologue: entries of tiles 0..2 (waited), then per tile j < 3 its rows and tile j + 3's entries
+    for (int t = 0; t < 3; ++t) issue_perm(t);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < 3; ++j) {
+        issue_rows(j);
+        issue_perm(j + 3);
+        cp_async_commit();
+    }
+
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint64_t da_h = sw128_desc(smem_u32(smem + L::a_hi)), da_l = sw128_desc(smem_u32(smem + L::a_lo));
+    const uint64_t db_h = sw128_desc(smem_u32(smem + L::b_hi)), db_l = sw128_desc(smem_u32(smem + L::b_lo));
+
+    // drain role: TMEM lane quarter q (accumulator rows 32 q ..), column half hc
+    const int q = warp & 3, hc = warp >> 2;
+    const int slot = q >> 1, fi = (q & 1) * 32 + lane;   // sub-cluster, feature i of this lane's row
+    const bool row_live = (q & 1) * 32 < DP;            // warp-uniform
+    const bool do_s = row_live && (DP > 32 ? (q & 1) <= hc : hc == 0);
+    const bool do_sum = row_live && hc == 0;
+    double acc[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) acc[m] = 0.0;
+    double sacc = 0.0;
+    int cnt_l = 0, cnt_r = 0;
+    auto drain = [&](int g) {   // accumulator of group g (its MMAs complete)
+        const uint32_t base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((g & 1) * 128);
+        if (do_s) {
+            uint32_t v[32];
+            tmem_ld32(base + (uint32_t)(32 * hc), v);
+#pragma unroll
+            for (int m = 0; m < 32; ++m) acc[m] += (double)__uint_as_float(v[m]);
+        }
+        if (do_sum) {
+            uint32_t v1;
+            tmem_ld1(base + (uint32_t)DP, v1);
+            sacc += (double)__uint_as_float(v1);
+        }
+    };
+    // block-uniform: tile t's MMAs (the t-th commit) complete
+    auto wait_mma = [&](int t) -> bool {
+        if (tid == 0 && !mbar_wait_bounded(bar, (uint32_t)(t & 1), gerr)) {
+            atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+            *flag = 1;
+        }
+        __syncthreads();
+        return *flag == 0;
+    };
+
+    bool failed = false;
+    int pending = -1;   // tile whose MMAs were issued and not yet seen complete
+#pragma unroll 1
+    for (int t = 0; t < ntiles; ++t) {
+        cp_async_wait<2>();   // this thread's rows of tile t and entries of tile t + 3 have landed
+        if (t > 0) {
+            if (!wait_mma(t - 1)) { failed = true; break; }
+            pending = -1;
+        } else {
+            __syncthreads();
+            if (tid < DP) {   // centre: mean of the first tile's points
+                const int nv = min(ST_P, len);
+                float a = 0.f;
+                for (int r = 0; r < nv; ++r) a += stage[r * SX + tid];
+                sshift[tid] = a / (float)nv;
+            }
+            __syncthreads();
+        }
+        tc_fence_after();
+        issue_rows(t + 3);
+        issue_perm(t + 6);
+        cp_async_commit();
+        {
+            const float* sb = stage + (size_t)(t % ST_STAGES) * ST_P * SX;
+            const int sv = ssub[(t % ST_STAGES) * ST_P + lane];
+            const bool in_l = sv == 1, in_r = sv == 2;
+            if (warp == 0) {
+                const unsigned bl = __ballot_sync(0xffffffffu, in_l), br = __ballot_sync(0xffffffffu, in_r);
+                cnt_l += __popc(bl);
+                cnt_r += __popc(br);
+            }
+#pragma unroll
+            for (int g = 0; g < DP / 32; ++g) {
+                const float4 v4 = *reinterpret_cast<const float4*>(sb + lane * SX + 32 * g + 4 * warp);
+                const float4 s4 = *reinterpret_cast<const float4*>(sshift + 32 * g + 4 * warp);
+                const float cv[4] = {v4.x - s4.x, v4.y - s4.y, v4.z - s4.z, v4.w - s4.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int f = 32 * g + 4 * warp + e;
+                    const float hi = tf32_rna(cv[e]);
+                    const float lo = tf32_rna(cv[e] - hi);
+                    const uint32_t ob = sw128_offset32(f, lane), orr = sw128_offset32(64 + f, lane);
+                    *reinterpret_cast<float*>(smem + L::b_hi + ob) = hi;
+                    *reinterpret_cast<float*>(smem + L::b_lo + ob) = lo;
+                    *reinterpret_cast<float*>(smem + L::a_hi + ob) = in_l ? hi : 0.f;
+                    *reinterpret_cast<float*>(smem + L::a_lo + ob) = in_l ? lo : 0.f;
+                    *reinterpret_cast<float*>(smem + L::a_hi + orr) = in_r ? hi : 0.f;
+                    *reinterpret_cast<float*>(smem + L::a_lo + orr) = in_r ? lo : 0.f;
+                }
+            }
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        const int grp = t / ST_G;
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t td = tmem_base + (uint32_t)((grp & 1) * 128);
+            const uint32_t first = (t % ST_G) == 0 ? 0u : 1u;   // a fresh accumulator per group
+#pragma unroll
+            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_h + 2 * ks, IDESC, ks != 0 ? 1u : first);
+#pragma unroll
+            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_l + 2 * ks, db_h + 2 * ks, IDESC, 1u);
+#pragma unroll
+            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_l + 2 * ks, IDESC, 1u);
+            umma_commit(bar);
+        }
+        pending = t;
+        // the previous group's last MMAs completed (waited above): drain it while this group runs
+        if (t % ST_G == 0 && grp > 0) drain(grp - 1);
+        tc_fence_before();
+    }
+    if (!failed && ntiles > 0) {
+        if (wait_mma(ntiles - 1)) {
+            pending = -1;
+            tc_fence_after();
+            drain((ntiles - 1) / ST_G);
+        } else {
+            failed = true;
+        }
+    }
+    cp_async_wait<0>();
+    __syncthreads();   // the stage area now holds the sums, counts and d for the move to mu_k
+    double* xs = reinterpret_cast<double*>(smem + L::stage);   // [2][DP] sums S1
+    double* xd = xs + 2 * DP;                                  // [DP] d = a - mu_k
+    double* xn = xd + DP;                                      // [2] counts
+    if (!failed) {
+        if (do_sum) xs[slot * DP + fi] = sacc;
+        if (tid < DP) xd[tid] = ntiles > 0 ? (double)sshift[tid] - (double)muv[(size_t)3 * k * DP + tid] : 0.0;
+        if (tid == 0) {
+            xn[0] = (double)cnt_l;
+            xn[1] = (double)cnt_r;
+        }
+    }
+    __syncthreads();
+    if (!failed) {
+        double* out = part + (size_t)ch * 2 * SL;
+        if (tid < 2) out[(size_t)tid * SL] = xn[tid];
+        const double n = xn[slot];
+        if (do_s) {
+            double* po = out + (size_t)slot * SL + 1 + DP;
+            const double di = xd[fi], si = xs[slot * DP + fi];
+#pragma unroll
+            for (int m = 0; m < 32; ++m) {
+                const int j = 32 * hc + m;
+                if (fi <= j && j < DP) {
+                    const double dj = xd[j], sj = xs[slot * DP + j];
+                    po[tri_index(DP, fi, j)] = acc[m] + di * sj + si * dj + n * di * dj;
+                }
+            }
+        }
+        if (do_sum) out[(size_t)slot * SL + 1 + fi] = sacc + n * xd[fi];
+    }
+    if (failed && tid == 0 && pending >= 0)   // nothing in flight at dealloc
+        mbar_wait_bounded(bar, (uint32_t)(pending & 1), nullptr);
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ST_TMEM_COLS));
     }
 }
 
@@ -1263,6 +1630,41 @@ dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err)
     if (!tc_scan_supported(c, K)) return fail(DPMM_ERR_INVALID_ARG, "tensor-core scan: unsupported shape");
     if (c->Dp == 64) return launch_prune_scan_tc_t<64>(c, K, d_err);
     return launch_prune_scan_tc_t<32>(c, K, d_err);
+}
+
+bool tc_stats_supported(const dpmm_ctx* c)
+{
+    return c->prior == DPMM_PRIOR_GAUSSIAN && (c->Dp == 32 || c->Dp == 64) && c->ll_mode != DPMM_LL_FP32;
+}
+
+template <int DP>
+static dpmm_status launch_slot_stats_tc_t(dpmm_ctx* c, const uint8_t* d_mask, int32_t* err)
+{
+    auto kern = tc::k_slot_stats_tc<DP>;
+    constexpr size_t sm = tc::StatSmem<DP>::total;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu, c->d_sub,
+                                                c->d_part, d_mask, err);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask)
+{
+    if (!tc_stats_supported(c)) return fail(DPMM_ERR_INVALID_ARG, "tensor-core statistics: unsupported shape");
+    int32_t* err = c->d_aux + 3;
+    DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
+    {
+        KernelTimer kt(c, PH_SLOT_STATS);
+        if (c->Dp == 64) DPMM_TRY(launch_slot_stats_tc_t<64>(c, d_mask, err));
+        else DPMM_TRY(launch_slot_stats_tc_t<32>(c, d_mask, err));
+    }
+    int32_t* h_err = reinterpret_cast<int32_t*>(c->h_pinned);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (*h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core statistics: bounded wait expired (code " +
+                                                  std::to_string(*h_err) + ")");
+    return DPMM_OK;
 }
 
 }  // namespace dpmm
