@@ -82,9 +82,10 @@ def padded(d):
     return p
 
 
-def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src):
+def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
     """Per timed kernel (CUDA events around each launch on its stream): algorithmic work per launch,
-    achieved rate and the fraction of the measured peak of its bound."""
+    achieved rate and the fraction of the measured peak of its bound.  tc: the pruned scan and the
+    sub-cluster statistics ran on the tensor cores (padded dimension 32 / 64, mixed mode)."""
     Dp = padded(D)
     hbm = pk.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     bf16 = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
@@ -104,14 +105,23 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src):
     add("k_gauss_labels_tc", 7, "tensor", 2.0 * N * k_mean * D * D, "TFLOP/s", bf16, "bf16_tflops",
         f"2*N*K*D^2 FLOP per launch (one product; the split form issues 3), K mean {k_mean:.1f}",
         label_kernel_traffic(N, k_mean))
-    add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
-        "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
-        "bound), its permutation index and r written; FP32 SIMT work 2*N*Dp^2 FLOP + the bounds")
+    if tc:
+        add("k_prune_scan_tc", 8, "hbm", N * (Dp * 4.0 + 12), "GB/s", hbm, "hbm_gbs",
+            "N*(Dp*4 + 12) B per launch: every point read once from HBM (the bound pass re-reads the "
+            "chunk from L2), its permutation index, r_h written; tensor-core products 3 x 2*N*Dp*64 FLOP "
+            "+ 3 x 2*N*Dp*kept-candidates")
+        add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
+            "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
+            "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP")
+    else:
+        add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
+            "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
+            "bound), its permutation index and r written; FP32 SIMT work 2*N*Dp^2 FLOP + the bounds")
+        add("k_gauss_slot_stats", 10, "hbm", N * (2.0 * Dp * 4 + 12), "GB/s", hbm, "hbm_gbs",
+            "N*(2*Dp*4 + 12) B per launch: every point read once per sub-cluster pass, permutation, "
+            "sub-label; FP32 products N*Dp*(Dp+1)")
     add("k_prune_draw", 9, "hbm", N * 12.0 + kept * N * Dp * 4, "GB/s", hbm, "hbm_gbs",
         "N*12 B (permutation, r, label) + the points of chunks that keep other clusters")
-    add("k_gauss_slot_stats", 10, "hbm", N * (2.0 * Dp * 4 + 12), "GB/s", hbm, "hbm_gbs",
-        "N*(2*Dp*4 + 12) B per launch: every point read once per sub-cluster pass, permutation, "
-        "sub-label; FP32 products N*Dp*(Dp+1)")
     return out
 
 
@@ -423,7 +433,8 @@ def main():
     value = world * N * args.steps / (elapsed_ms / 1e3)
     pk, pk_src = peaks()
     k_mean = float(np.mean(ks)) if ks else float(k_before.value)
-    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src)
+    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src,
+                               padded(D) in (32, 64) and mode != capi.LL_FP32)
     # the roofline of the kernel with the most device time in the timed region
     dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
     roofline = dict(kernels[dominant], kernel=dominant) if dominant else None
