@@ -345,6 +345,45 @@ extern "C" dpmm_status dpmm_synchronize(dpmm_ctx* c)
 }
 
 // ----------------------------------------------------------------- points
+// Pageable host memory is copied through two pinned staging buffers: host threads fill one while
+// the copy engine drains the other (a single pageable cudaMemcpy is staged by the driver through
+// a small bounce buffer, one piece at a time).
+static cudaError_t copy_pageable_staged(void* dst, const void* src, size_t bytes, cudaStream_t st)
+{
+    constexpr size_t kChunk = (size_t)64 << 20;
+    void* hb[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMallocHost(&hb[b], kChunk);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+    }
+    size_t off = 0;
+    for (int i = 0; e == cudaSuccess && off < bytes; ++i, off += kChunk) {
+        const int b = i & 1;
+        const size_t n = std::min(kChunk, bytes - off);
+        if (i >= 2) e = cudaEventSynchronize(ev[b]);   // its previous copy has left the buffer
+        if (e != cudaSuccess) break;
+        const char* s = static_cast<const char*>(src) + off;
+        char* d = static_cast<char*>(hb[b]);
+        constexpr int64_t kParts = 16;
+#pragma omp parallel for schedule(static)
+        for (int64_t q = 0; q < kParts; ++q) {
+            const size_t a = n * (size_t)q / kParts, z = n * (size_t)(q + 1) / kParts;
+            std::memcpy(d + a, s + a, z - a);
+        }
+        e = cudaMemcpyAsync(static_cast<char*>(dst) + off, hb[b], n, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
+    }
+    const cudaError_t es = cudaStreamSynchronize(st);   // nothing reads the buffers after this
+    if (e == cudaSuccess) e = es;
+    for (int b = 0; b < 2; ++b) {
+        if (ev[b]) cudaEventDestroy(ev[b]);
+        if (hb[b]) cudaFreeHost(hb[b]);
+    }
+    return e;
+}
+
 template <typename T>
 static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
 {
@@ -354,12 +393,15 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
     const int D = c->D;
     T* tmp = nullptr;
     DPMM_TRY(dev_alloc(&tmp, (size_t)N * D));
-    // cudaMemcpyDefault: the points may live in host or device memory
-    cudaError_t e = cudaMemcpyAsync(tmp, points, sizeof(T) * (size_t)N * D, cudaMemcpyDefault, c->stream);
+    // the points may live in pageable or pinned host memory or in device memory
+    const size_t bytes = sizeof(T) * (size_t)N * D;
     cudaPointerAttributes pa{};
-    if (cudaPointerGetAttributes(&pa, points) == cudaSuccess && pa.type != cudaMemoryTypeDevice)
-        g_h2d_bytes += sizeof(T) * (size_t)N * D;
+    const bool attr_ok = cudaPointerGetAttributes(&pa, points) == cudaSuccess;
     cudaGetLastError();
+    cudaError_t e = attr_ok && pa.type == cudaMemoryTypeUnregistered
+                        ? copy_pageable_staged(tmp, points, bytes, c->stream)
+                        : cudaMemcpyAsync(tmp, points, bytes, cudaMemcpyDefault, c->stream);
+    if (attr_ok && pa.type != cudaMemoryTypeDevice) g_h2d_bytes += bytes;
     const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     if (e == cudaSuccess && gauss) {
         // FP64 column means (the shift)
