@@ -75,6 +75,23 @@ def label_kernel_traffic(N, K):
     return vals["dram_bytes_per_launch"] * model(N, K) / model(vals["capture_N"], vals["capture_K"])
 
 
+def per_point_traffic(profile, N):
+    """DRAM bytes per launch of a kernel that reads each point once: the ncu capture recorded in
+    profiles/<profile> (dram_bytes_per_launch at capture_N points, D = 64) scaled by N."""
+    vals = {}
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", profile)) as f:
+            for line in f:
+                for key in ("dram_bytes_per_launch", "capture_N"):
+                    if line.strip().startswith(key + ":"):
+                        vals[key] = float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    if len(vals) != 2:
+        return None
+    return vals["dram_bytes_per_launch"] * N / vals["capture_N"]
+
+
 def padded(d):
     p = 4
     while p < d:
@@ -109,10 +126,12 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
         add("k_prune_scan_tc", 8, "hbm", N * (Dp * 4.0 + 12), "GB/s", hbm, "hbm_gbs",
             "N*(Dp*4 + 12) B per launch: every point read once from HBM (the bound pass re-reads the "
             "chunk from L2), its permutation index, r_h written; tensor-core products 3 x 2*N*Dp*64 FLOP "
-            "+ 3 x 2*N*Dp*kept-candidates")
+            "+ 3 x 2*N*Dp*kept-candidates",
+            per_point_traffic("k_prune_scan_tc_N1e6_D64.md", N) if Dp == 64 else None)
         add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
-            "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP")
+            "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP",
+            per_point_traffic("k_slot_stats_tc_N1e6_D64.md", N) if Dp == 64 else None)
     else:
         add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
