@@ -75,6 +75,17 @@ __device__ __forceinline__ void draw_uniform2(const RngArgs& r, int64_t pt, floa
     }
 }
 
+// A label phase that settles a point without drawing still consumes its two uniforms from a
+// stateful per-point stream (cuRAND XORWOW), so later draws stay those of the dense phase; the
+// caller-supplied and counter-based sources need nothing.
+__device__ __forceinline__ void skip_uniform2(const RngArgs& r, int64_t pt)
+{
+    if (!r.ucaller && r.kind == DPMM_RNG_CURAND_XORWOW) {
+        float u1, u2;
+        draw_uniform2(r, pt, u1, u2);
+    }
+}
+
 // One uniform for point pt (initial label draws, cudaKernel.cu:144-170).
 __device__ __forceinline__ float draw_uniform1(const RngArgs& r, int64_t pt)
 {

@@ -395,18 +395,19 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
                                                       float* __restrict__ V, float* __restrict__ beta)
 {
     constexpr int NW = kPrTh / 32;
-    __shared__ float sW[DP * DP];
+    constexpr int SW = DP + 1;   // padded row stride: the z loop's lanes read one column each
+    __shared__ float sW[DP * SW];
     __shared__ double red[NW];
     __shared__ double zs[NW][DP];
     const int k = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    for (int e = t; e < DP * DP; e += blockDim.x) sW[e] = Wt[(size_t)3 * k * DP * DP + e];
+    for (int e = t; e < DP * DP; e += blockDim.x) sW[(e / DP) * SW + e % DP] = Wt[(size_t)3 * k * DP * DP + e];
     __syncthreads();
     double rmax = 0;
     for (int i = t; i < DP; i += blockDim.x) {
         double srow = 0;
         for (int j = 0; j < DP; ++j) {
             double l = 0;
-            for (int cc = 0; cc < DP; ++cc) l += (double)sW[cc * DP + i] * (double)sW[cc * DP + j];
+            for (int cc = 0; cc < DP; ++cc) l += (double)sW[cc * SW + i] * (double)sW[cc * SW + j];
             srow += fabs(l);
         }
         rmax = fmax(rmax, srow);
@@ -426,7 +427,7 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
         double q = 0;
         for (int j = lane; j < DP; j += 32) {   // z = W_k^T (mu_h - mu_k)
             double z = 0;
-            for (int i = 0; i < DP; ++i) z += (double)sW[j * DP + i] * ((double)mh[i] - (double)mk[i]);
+            for (int i = 0; i < DP; ++i) z += (double)sW[j * SW + i] * ((double)mh[i] - (double)mk[i]);
             zs[warp][j] = z;
             q += z * z;
         }
@@ -439,7 +440,7 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
         double bsum = 0;
         for (int i = lane; i < DP; i += 32) {    // v = W_k u, u = z / |z|
             double v = 0;
-            for (int j = 0; j < DP; ++j) v += (double)sW[j * DP + i] * zs[warp][j];
+            for (int j = 0; j < DP; ++j) v += (double)sW[j * SW + i] * zs[warp][j];
             v *= inv;
             vh[i] = (float)v;
             bsum += (double)(float)v * (double)mk[i];
@@ -594,15 +595,18 @@ __global__ void __launch_bounds__(kPrTh) k_prune_scan(const float* __restrict__ 
 
 // pass 2, one block per tile of kPrTh points of a chunk (blockIdx.x = chunk, blockIdx.y = tile): labels.
 // A chunk without other clusters takes h + 1; otherwise r of the kept clusters (r_h from pass 1; every
-// cluster when the chunk kept more than kPrMaxCand), the others at -inf, and the draw (or argmax) of
-// the dense label phase over all K columns.  Shared memory: DP*DP + DP + K*kPrTh floats.
+// cluster when the chunk kept more than kPrMaxCand).  A point whose kept clusters all lie more than the
+// margin below r_h takes h + 1 as well (the chunk bound's guarantee, now from the exact r); the others
+// get the draw (or argmax) of the dense label phase over all K columns, the left-out clusters at -inf.
+// Shared memory: DP*DP + DP + K*kPrTh floats.
 template <int DP>
 __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ x, const int32_t* __restrict__ perm,
                                                       const int32_t* __restrict__ chunk,
                                                       const int32_t* __restrict__ nchunks, const float* __restrict__ Wt,
                                                       const float* __restrict__ bvec, const float* __restrict__ cvec,
                                                       int K, int final_, RngArgs rng, const float* __restrict__ rh,
-                                                      const int32_t* __restrict__ cand, int32_t* __restrict__ labels)
+                                                      const int32_t* __restrict__ cand, float margin,
+                                                      int32_t* __restrict__ labels)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     float* sW = reinterpret_cast<float*>(smem);
@@ -618,7 +622,11 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
     const int i = base + t;
     const bool valid = i < start + L;
     if (n == 0) {
-        if (valid) labels[perm[i]] = h + 1;
+        if (valid) {
+            const int64_t p0 = perm[i];
+            labels[p0] = h + 1;
+            if (!final_) skip_uniform2(rng, p0);   // the argmax of final mode draws nothing
+        }
         return;
     }
     const bool all = n > kPrMaxCand;      // over capacity: every cluster
@@ -629,8 +637,10 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
 #pragma unroll
         for (int e = 0; e < DP; ++e) xr[e] = 0.f;
     for (int k = 0; k < K; ++k) sr[k * kPrTh + t] = -INFINITY;
-    sr[h * kPrTh + t] = valid ? rh[i] : 0.f;
+    const float r_own = valid ? rh[i] : 0.f;
+    sr[h * kPrTh + t] = r_own;
     const int m = all ? K : n;
+    float best_other = -INFINITY;
     for (int a = 0; a < m; ++a) {
         const int k = all ? a : cq[1 + a];
         if (k == h) continue;
@@ -640,9 +650,17 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
         for (int e = t; e < DP * DP / 4; e += blockDim.x) dst[e] = src[e];
         for (int e = t; e < DP; e += blockDim.x) sbv[e] = bvec[(size_t)3 * k * DP + e];
         __syncthreads();
-        sr[k * kPrTh + t] = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
+        const float r = gauss_r_point<DP>(sW, sbv, xr, cvec[3 * k]);
+        sr[k * kPrTh + t] = r;
+        best_other = fmaxf(best_other, r);
     }
-    if (valid) labels[pt] = draw_from_r<kPrTh>(sr, t, K, final_, rng, pt);
+    if (!valid) return;
+    if (best_other < r_own - margin) {
+        labels[pt] = h + 1;
+        if (!final_) skip_uniform2(rng, pt);
+    } else {
+        labels[pt] = draw_from_r<kPrTh>(sr, t, K, final_, rng, pt);
+    }
 }
 
 static size_t prune_draw_smem(int DP, int K) { return sizeof(float) * ((size_t)DP * DP + DP + (size_t)K * kPrTh); }
@@ -698,7 +716,7 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
         const dim3 grid((unsigned)c->max_chunks, (unsigned)((c->chunk_len + kPrTh - 1) / kPrTh));
         k_prune_draw<DP><<<grid, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
                                                         c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
-                                                        c->d_prune_cand, c->d_labels);
+                                                        c->d_prune_cand, c->prune_margin, c->d_labels);
         DPMM_LAUNCHED();
     }
     c->prune_used += 1;
@@ -1575,9 +1593,9 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
     return launch_stats_finalize(c, K, d_mask);
 }
 
-// One block per cluster: chunk partials summed in chunk order (FP64), shifted back to the
-// original coordinates, written as count / sum / full S for slots 3k (cluster = l + r),
-// 3k+1 (l), 3k+2 (r).
+// Blocks (cluster, share of the scatter triangle): chunk partials summed in chunk order (FP64),
+// shifted back to the original coordinates, written as count / sum / full S for slots 3k
+// (cluster = l + r), 3k+1 (l), 3k+2 (r).
 __global__ void k_stats_finalize(const double* __restrict__ part, const int32_t* __restrict__ chunk,
                                  const int32_t* __restrict__ nchunks, const float* __restrict__ muv,
                                  const double* __restrict__ gshift, int D, int Dp, int gauss, int SL, int out_len,
@@ -1613,21 +1631,26 @@ __global__ void k_stats_finalize(const double* __restrict__ part, const int32_t*
     double* out_c = stats + (size_t)(3 * k) * out_len;
     double* out_l = out_c + out_len;
     double* out_r = out_l + out_len;
-    if (threadIdx.x == 0) {
-        out_l[0] = n2[0];
-        out_r[0] = n2[1];
-        out_c[0] = n2[0] + n2[1];
-    }
-    for (int e = threadIdx.x; e < D; e += blockDim.x) {
-        double sl = sm2[e], sr = sm2[D + e];
-        if (gauss) { sl += n2[0] * t[e]; sr += n2[1] * t[e]; }
-        out_l[1 + e] = sl;
-        out_r[1 + e] = sr;
-        out_c[1 + e] = sl + sr;
+    if (blockIdx.y == 0) {
+        if (threadIdx.x == 0) {
+            out_l[0] = n2[0];
+            out_r[0] = n2[1];
+            out_c[0] = n2[0] + n2[1];
+        }
+        for (int e = threadIdx.x; e < D; e += blockDim.x) {
+            double sl = sm2[e], sr = sm2[D + e];
+            if (gauss) { sl += n2[0] * t[e]; sr += n2[1] * t[e]; }
+            out_l[1 + e] = sl;
+            out_r[1 + e] = sr;
+            out_c[1 + e] = sl + sr;
+        }
     }
     if (!gauss) return;
-    // S = Sc + t Sc_sum^T + Sc_sum t^T + n t t^T, with Sc_sum = sum (x - t)
-    for (int e = threadIdx.x; e < T; e += blockDim.x) {
+    // S = Sc + t Sc_sum^T + Sc_sum t^T + n t t^T, with Sc_sum = sum (x - t); block y of the
+    // cluster takes the y-th share of the upper triangle
+    const int per = (T + (int)gridDim.y - 1) / (int)gridDim.y;
+    const int e1 = min(T, per * ((int)blockIdx.y + 1));
+    for (int e = per * (int)blockIdx.y + threadIdx.x; e < e1; e += blockDim.x) {
         int i = 0, rem = e;
         while (rem >= Dp - i) { rem -= Dp - i; ++i; }
         int j = i + rem;
@@ -1653,7 +1676,8 @@ dpmm_status launch_stats_finalize(dpmm_ctx* c, int K, const uint8_t* d_mask)
     size_t sm = sizeof(double) * (2 + 3 * (size_t)c->D);
     if (sm > 48 * 1024)
         DPMM_CUDA_TRY(cudaFuncSetAttribute(k_stats_finalize, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_stats_finalize<<<K, 256, sm, c->stream>>>(c->d_part, c->d_chunk, c->d_nchunks, c->d_mu, c->d_gshift, c->D,
+    const dim3 grid((unsigned)K, gauss ? 8u : 1u);   // the scatter triangle over 8 blocks per cluster
+    k_stats_finalize<<<grid, 256, sm, c->stream>>>(c->d_part, c->d_chunk, c->d_nchunks, c->d_mu, c->d_gshift, c->D,
                                                 c->Dp, gauss, SL, c->stat_len, c->d_stats, d_mask);
     DPMM_LAUNCHED();
     if (!d_mask) {

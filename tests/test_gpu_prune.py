@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from conftest import uniforms
-from dpmmsubclusters_gpu_b200 import CudaKernel, LL_FP32, prior_type
+from dpmmsubclusters_gpu_b200 import RNG_CURAND_XORWOW, CudaKernel, LL_FP32, prior_type
 from dpmmsubclusters_gpu_b200.capi import check, lib
 
 pytestmark = pytest.mark.gpu
@@ -100,3 +100,33 @@ def test_chunk_over_capacity_is_evaluated_against_every_cluster(K, N, D, planted
     st = _stats(kern)
     assert st[1] == 1 and st[5] >= 1, st
     np.testing.assert_array_equal(lab[30.0], lab[0.0])
+
+
+def test_stateful_stream_stays_in_step_with_the_dense_phase():
+    # cuRAND XORWOW keeps one generator state per point: a pruned phase that settles a point without
+    # drawing must still advance it, or the next draws differ from the dense phase's.  Phase 1:
+    # separated clusters (every point settled without a draw); phase 2: clusters 0 and 1 made
+    # identical, so their points draw 50 / 50 from the advanced states.
+    K, N, D = 8, 40000, 16
+    x, z, mus, covs, rng = _mixture(23, N, D, K, 6.0)
+    inv = np.array([np.linalg.inv(c) for c in covs])
+    ld = np.array([np.linalg.slogdet(c)[1] for c in covs])
+    mus2, inv2, ld2 = mus.copy(), inv.copy(), ld.copy()
+    mus2[1], inv2[1], ld2[1] = mus[0], inv[0], ld[0]
+    lab = {}
+    for margin in (30.0, 0.0):
+        kern = CudaKernel(prior_type.Gaussian, k_max=16, rng_kind=RNG_CURAND_XORWOW).init(N, x.T, seed=3)
+        check(lib().dpmm_set_label_pruning(kern.ctx, margin))
+        out = []
+        for m, iv, l in ((mus, inv, ld), (mus2, inv2, ld2)):
+            kern.set_gaussian_params(m, iv, l, np.full(K, 1.0 / K))
+            kern.set_labels((z + 1).astype(np.int32))
+            kern.create_clusters_labels(K, False, None)
+            out.append(kern.get_labels())
+        lab[margin] = out
+        if margin > 0:
+            assert _stats(kern)[1] == 2
+    for a, b in zip(lab[30.0], lab[0.0]):
+        np.testing.assert_array_equal(a, b)
+    moved = (lab[0.0][1] == 2) & (z == 0)
+    assert moved.sum() > 1000   # the second phase does draw between clusters 0 and 1
