@@ -1149,6 +1149,289 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
 }
 
 
+// Single-pass form of the same scan for K - 1 <= kScan1MaxCand: B = [W_h | v_h,k for every k != h]
+// (h's 64 rows copied from the dense phase's packed tile, then one row per other cluster, ascending),
+// so one gather and one group of MMAs per 128-point tile give r_h and every projection.  The drain
+// records, per cluster, whether the point bound keeps it at some point of the chunk; after the last
+// tile the chunk bound (r_min and radius of the whole chunk) is applied to those, which is the same
+// kept set as the two-pass form (chunk bound first, point bound on its survivors).
+constexpr int kScan1MaxCand = 2 * BN - KD;   // 192 other clusters
+template <int DP>
+__global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const uint8_t* __restrict__ Btc, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, const float* __restrict__ mu, const float* __restrict__ lam,
+    const float* __restrict__ M, const float* __restrict__ V, const float* __restrict__ beta, int K, float margin,
+    float* __restrict__ rh, int32_t* __restrict__ cand, unsigned long long* __restrict__ cnt,
+    int32_t* __restrict__ err)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sA = smem + ScanSmem::a;
+    uint8_t* sB = smem + ScanSmem::b;
+    float* sq = reinterpret_cast<float*>(smem + ScanSmem::sq);
+    float* sbias = reinterpret_cast<float*>(smem + ScanSmem::bias);
+    float* sbeta = reinterpret_cast<float*>(smem + ScanSmem::cb);
+    float* sck = sbeta + kScanMaxK;
+    int32_t* skeep = reinterpret_cast<int32_t*>(smem + ScanSmem::ck);   // chunk-bound verdict per candidate
+    uint32_t* kbits = reinterpret_cast<uint32_t*>(smem + ScanSmem::bits);
+    float* wred = reinterpret_cast<float*>(kbits + kScanMaxK / 32);
+    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + ScanSmem::bar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+    const int q = blockIdx.x;
+    if (q >= *nchunks) return;
+    const int h = chunk[3 * q], start = chunk[3 * q + 1], len = chunk[3 * q + 2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+    const int nt = K - 1;                                   // candidate a is cluster a + (a >= h)
+    const int nbt = (KD + nt + BN - 1) / BN;                // B tiles (1 or 2)
+    auto cand_k = [&](int a) { return a + (a >= h ? 1 : 0); };
+
+    {
+        // rows 0..63: cluster h's rows of its packed pair tile (same swizzle phase: 64 is a multiple of 8)
+        const uint8_t* tile = Btc + (size_t)(h / CPT) * STAGE_BYTES + (size_t)(h % CPT) * KD * 128;
+        for (int e = tid; e < 2 * KD * 128 / 16; e += 256) {
+            const int half = e / (KD * 8), o = e % (KD * 8);
+            reinterpret_cast<uint4*>(sB + half * B_BYTES)[o] = reinterpret_cast<const uint4*>(tile + half * B_BYTES)[o];
+        }
+        // rows 64 .. : v_h,k of every other cluster (split BF16), zero up to the tile edge
+        for (int e = tid; e < (nbt * BN - KD) * 8; e += 256) {
+            const int a = e / 8, c8 = e % 8, n = KD + a;
+            float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            if (a < nt && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(V + ((size_t)h * K + cand_k(a)) * DP + c8 * 8);
+                const float4 u0 = src[0], u1 = src[1];
+                v[0] = u0.x; v[1] = u0.y; v[2] = u0.z; v[3] = u0.w;
+                v[4] = u1.x; v[5] = u1.y; v[6] = u1.z; v[7] = u1.w;
+            }
+            __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) bf16_split(v[j], hi[j], lo[j]);
+            uint8_t* base = sB + (size_t)(n / BN) * STAGE_BYTES;
+            const uint32_t o = sw128_offset(n % BN, c8 * 8);
+            *reinterpret_cast<uint4*>(base + o) = *reinterpret_cast<const uint4*>(hi);
+            *reinterpret_cast<uint4*>(base + B_BYTES + o) = *reinterpret_cast<const uint4*>(lo);
+        }
+        for (int a = tid; a < nt; a += 256) {
+            const int k = cand_k(a);
+            sbeta[a] = beta[(size_t)h * K + k];
+            sck[a] = cvec[3 * k];
+        }
+        if (tid < 2 * KD) {
+            const int side = tid / KD, j = tid % KD;
+            sbias[tid] = j < DP ? (side ? mu : bvec)[(size_t)3 * h * DP + j] : 0.f;
+        }
+        if (tid < kScanMaxK / 32) kbits[tid] = 0u;
+    }
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        *flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(SCAN_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t lane_addr = (uint32_t)((warp & 3) * 32) << 16;
+    const float ch = cvec[3 * h];
+
+    // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8); a tile's
+    // permutation entries load one tile ahead of its rows
+    float4 pf[4][2];
+    int pq[4];
+    auto load_perm = [&](int t0) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u;
+            pq[u] = t0 + row < len ? __ldg(perm + start + t0 + row) : -1;
+        }
+    };
+    auto load_rows = [&]() {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int c8 = tid & 7;
+            pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
+            pf[u][1] = pf[u][0];
+            if (pq[u] >= 0 && c8 * 8 < DP) {
+                const float4* src = reinterpret_cast<const float4*>(x + (size_t)pq[u] * DP + c8 * 8);
+                pf[u][0] = __ldg(src);
+                pf[u][1] = __ldg(src + 1);
+            }
+        }
+    };
+
+    uint32_t phase = 0;
+    bool failed = false;
+    float tmin = INFINITY, r2max = 0.f;
+    const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
+    load_perm(0);
+    load_rows();
+    load_perm(BM);
+    for (int t0 = 0; t0 < len; t0 += BM) {
+        const int ntn = min(BM, len - t0);
+        // A tile from the rows, and the largest |x - mu_h|^2
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int row = (tid >> 3) + 32 * u, c8 = tid & 7;
+            const float v[8] = {pf[u][0].x, pf[u][0].y, pf[u][0].z, pf[u][0].w,
+                                pf[u][1].x, pf[u][1].y, pf[u][1].z, pf[u][1].w};
+            __align__(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+            for (int e = 0; e < 8; ++e) bf16_split(v[e], hi[e], lo[e]);
+            const uint32_t off = sw128_offset(row, c8 * 8);
+            *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(hi);
+            *reinterpret_cast<uint4*>(sA + A_BYTES + off) = *reinterpret_cast<const uint4*>(lo);
+            float d2 = 0.f;
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const float tt = v[e] - sbias[KD + c8 * 8 + e];
+                d2 = fmaf(tt, tt, d2);
+            }
+            d2 += __shfl_xor_sync(0xffffffffu, d2, 1);
+            d2 += __shfl_xor_sync(0xffffffffu, d2, 2);
+            d2 += __shfl_xor_sync(0xffffffffu, d2, 4);
+            if (row < ntn) r2max = fmaxf(r2max, d2);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        tc_fence_before();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            for (int nb = 0; nb < nbt; ++nb) {
+                const uint8_t* bt = sB + (size_t)nb * STAGE_BYTES;
+                const uint64_t db_h = sw128_desc(smem_u32(bt)), db_l = sw128_desc(smem_u32(bt + B_BYTES));
+                const uint32_t td = tmem_base + (uint32_t)(nb * BN);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_l + 2 * ks, db_h + 2 * ks, 1u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(td, da_h + 2 * ks, db_l + 2 * ks, 1u);
+            }
+            umma_commit(bar);
+        }
+        if (t0 + BM < len) {   // the next tile's rows load while the MMAs run
+            load_rows();
+            load_perm(t0 + 2 * BM);
+        }
+        if (tid == 0 && !mbar_wait_bounded(bar, phase & 1, gerr)) {
+            atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+            *flag = 1;
+        }
+        ++phase;
+        __syncthreads();
+        if (*flag) { failed = true; break; }
+        tc_fence_after();
+        const int part = warp >> 2, row = (warp & 3) * 32 + lane;
+        {   // r_h from columns 0..63
+            float qs = 0.f;
+            if (DP > 32 || part == 0) {
+                uint32_t v[32];
+                tmem_ld32(tmem_base + lane_addr + (uint32_t)(32 * part), v);
+                const float* bs = sbias + 32 * part;
+                float q1 = 0.f;
+#pragma unroll
+                for (int j = 0; j < 32; j += 2) {
+                    const float z0 = __uint_as_float(v[j]) - bs[j];
+                    const float z1 = __uint_as_float(v[j + 1]) - bs[j + 1];
+                    qs = fmaf(z0, z0, qs);
+                    q1 = fmaf(z1, z1, q1);
+                }
+                qs += q1;
+            }
+            sq[part * BM + row] = qs;
+        }
+        __syncthreads();
+        float r_row = 0.f;
+        if (tid < BM) r_row = ch - 0.5f * (sq[tid] + sq[BM + tid]);
+        __syncthreads();
+        if (tid < BM) {
+            sq[tid] = r_row;
+            if (tid < ntn) {
+                rh[start + t0 + tid] = r_row;
+                tmin = fminf(tmin, r_row);
+            }
+        }
+        __syncthreads();
+        {   // point bound of every candidate: columns 64 + a
+            const bool valid = row < ntn;
+            const float lim = valid ? sq[row] - margin : 0.f;
+            for (int g = 2 + part; 32 * (g - 2) < nt; g += 2) {   // warp-uniform
+                uint32_t v[32];
+                tmem_ld32(tmem_base + lane_addr + (uint32_t)(32 * g), v);
+                const int a0 = 32 * (g - 2);
+                uint32_t m = 0u;
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int a = a0 + j;
+                    if (a < nt) {
+                        const float p = __uint_as_float(v[j]) - sbeta[a];
+                        const float ub = sck[a] - 0.5f * p * p;
+                        if (!(ub < lim)) m |= 1u << j;
+                    }
+                }
+                if (!valid) m = 0u;
+                m = __reduce_or_sync(0xffffffffu, m);
+                if (lane == 0 && m) atomicOr(&kbits[g - 2], m);
+            }
+        }
+        tc_fence_before();
+        __syncthreads();
+    }
+    if (!failed) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            tmin = fminf(tmin, __shfl_xor_sync(0xffffffffu, tmin, o));
+            r2max = fmaxf(r2max, __shfl_xor_sync(0xffffffffu, r2max, o));
+        }
+        if (lane == 0) {
+            wred[warp] = tmin;
+            wred[8 + warp] = r2max;
+        }
+        __syncthreads();
+        float rmin = wred[0], r2 = wred[8];
+        for (int w = 1; w < 8; ++w) {
+            rmin = fminf(rmin, wred[w]);
+            r2 = fmaxf(r2, wred[8 + w]);
+        }
+        const float R = sqrtf(r2) * 1.0001f + 1e-4f;
+        for (int a = tid; a < nt; a += 256) {   // chunk bound
+            const int k = cand_k(a);
+            const float d = M[(size_t)h * K + k] - lam[k] * R;
+            const float ub = cvec[3 * k] - 0.5f * (d > 0.f ? d * d : 0.f);
+            skeep[a] = !(ub < rmin - margin);
+        }
+    }
+    __syncthreads();
+    if (!failed && tid == 0) {
+        int n = 0;
+        int32_t* cq = cand + (size_t)q * (kPrMaxCand + 1);
+        for (int a = 0; a < nt; ++a)
+            if (skeep[a] && ((kbits[a >> 5] >> (a & 31)) & 1u)) {
+                if (n < kPrMaxCand) cq[1 + n] = cand_k(a);
+                ++n;
+            }
+        cq[0] = n;
+        atomicAdd(&cnt[0], (unsigned long long)n * (unsigned long long)len);
+        if (n > kPrMaxCand) atomicAdd(&cnt[1], 1ull);
+    }
+    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(SCAN_TMEM_COLS));
+    }
+}
+
 // ------------------------------------------------------------------------- slot statistics
 // Statistics of the two sub-clusters of one chunk (cluster k, sub-labels given) on the tensor
 // cores, Dp = 32 or 64: count, sum c and the upper triangle of sum c c^T over each sub-cluster's
@@ -1615,7 +1898,8 @@ bool tc_scan_supported(const dpmm_ctx* c, int K)
 template <int DP>
 static dpmm_status launch_prune_scan_tc_t(dpmm_ctx* c, int K, int32_t* err)
 {
-    auto kern = tc::k_prune_scan_tc<DP>;
+    // single pass while [W_h | every other cluster's v] fits two B tiles, else the two-pass form
+    auto kern = K - 1 <= tc::kScan1MaxCand ? tc::k_prune_scan1_tc<DP> : tc::k_prune_scan_tc<DP>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::ScanSmem::total));
     kern<<<c->max_chunks, 256, tc::ScanSmem::total, c->stream>>>(
         c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Btc, c->d_b, c->d_c, c->d_mu, c->d_prune_lam, c->d_prune_M,

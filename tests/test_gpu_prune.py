@@ -79,11 +79,13 @@ def test_unprunable_state_falls_back_to_dense():
     np.testing.assert_array_equal(lab[30.0], lab[0.0])
 
 
-@pytest.mark.parametrize("K,N,D,planted", [(30, 200000, 8, 3000), (30, 200000, 64, 3000), (150, 150000, 32, 600)])
+@pytest.mark.parametrize("K,N,D,planted", [(30, 200000, 8, 3000), (30, 200000, 64, 3000), (150, 150000, 32, 600),
+                                           (200, 200000, 32, 500)])
 def test_chunk_over_capacity_is_evaluated_against_every_cluster(K, N, D, planted):
     # separated clusters; points drawn from all of them carry label 1, so the chunk(s) of cluster 0
-    # keep more than 16 clusters: those points get every cluster, the rest stay pruned.  With 150
-    # clusters the chunk bound keeps more than 128 candidates (two candidate tiles on the tensor cores).
+    # keep more than 16 clusters: those points get every cluster, the rest stay pruned.  At D = 32 / 64
+    # the scan runs on the tensor cores: in one pass up to 193 clusters (150: two B tiles), in two
+    # passes above (200: the chunk bound first, then more than 128 candidates in two tiles).
     x, z, mus, covs, rng = _mixture(17, N, D, K, 8.0)
     kern = CudaKernel(prior_type.Gaussian, k_max=K + 2).init(N, x.T, seed=1)
     kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
