@@ -152,7 +152,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
-                    c->d_prune_beta};
+                    c->d_prune_beta, c->d_prune_list};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -287,6 +287,7 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     if (gauss && Dp <= 64) {
         chk(dev_alloc(&c->d_prune_rh, (size_t)N));
         chk(dev_alloc(&c->d_prune_cand, (size_t)c->max_chunks * 17));
+        chk(dev_alloc(&c->d_prune_list, (size_t)c->max_chunks));
         const size_t KP = (size_t)std::min(KM, 256);   // the pruned phase takes K <= 256
         chk(dev_alloc(&c->d_prune_lam, KP));
         chk(dev_alloc(&c->d_prune_M, KP * KP));

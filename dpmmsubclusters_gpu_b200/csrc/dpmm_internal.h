@@ -199,6 +199,7 @@ struct dpmm_ctx {
     int64_t prune_last_over = 0;   // ... and its chunks over the candidate-list capacity
     float* d_prune_rh = nullptr;   // [N] r of each point's current cluster, permutation order
     int32_t* d_prune_cand = nullptr; // [max_chunks][17] kept clusters per chunk
+    int32_t* d_prune_list = nullptr; // [max_chunks] the chunks that kept other clusters, ascending
     float* d_prune_lam = nullptr;  // [KP], KP = min(k_max, 256) (the pruned phase takes K <= 256)
     float* d_prune_M = nullptr;    // [KP][KP]
     float* d_prune_V = nullptr;    // [KP][KP][Dp] point-bound directions

@@ -593,9 +593,53 @@ __global__ void __launch_bounds__(kPrTh) k_prune_scan(const float* __restrict__ 
     }
 }
 
-// pass 2, one block per tile of kPrTh points of a chunk (blockIdx.x = chunk, blockIdx.y = tile): labels.
-// A chunk without other clusters takes h + 1; otherwise r of the kept clusters (r_h from pass 1; every
-// cluster when the chunk kept more than kPrMaxCand).  A point whose kept clusters all lie more than the
+// The chunks that kept other clusters, in ascending order, and their number (one block).
+__global__ void __launch_bounds__(1024) k_prune_list(const int32_t* __restrict__ nchunks,
+                                                     const int32_t* __restrict__ cand, int32_t* __restrict__ list,
+                                                     int32_t* __restrict__ count)
+{
+    __shared__ int wc[32];
+    const int nc = *nchunks, t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int base = 0;
+    for (int q0 = 0; q0 < nc; q0 += 1024) {
+        const int qq = q0 + t;
+        const bool kept = qq < nc && cand[(size_t)qq * (kPrMaxCand + 1)] > 0;
+        const unsigned bal = __ballot_sync(0xffffffffu, kept);
+        if (lane == 0) wc[warp] = __popc(bal);
+        __syncthreads();
+        int off = 0, tot = 0;
+        for (int w = 0; w < 32; ++w) {
+            off += w < warp ? wc[w] : 0;
+            tot += wc[w];
+        }
+        if (kept) list[base + off + __popc(bal & ((1u << lane) - 1u))] = qq;
+        base += tot;
+        __syncthreads();
+    }
+    if (t == 0) *count = base;
+}
+
+// Chunks that kept no other cluster: every point takes its current label h + 1 (no draw; a stateful
+// per-point stream still advances).  One block per chunk, no shared memory.
+__global__ void __launch_bounds__(256) k_prune_settle(const int32_t* __restrict__ perm,
+                                                      const int32_t* __restrict__ chunk,
+                                                      const int32_t* __restrict__ nchunks,
+                                                      const int32_t* __restrict__ cand, int final_, RngArgs rng,
+                                                      int32_t* __restrict__ labels)
+{
+    const int q = blockIdx.x;
+    if (q >= *nchunks || cand[(size_t)q * (kPrMaxCand + 1)] != 0) return;
+    const int h = chunk[3 * q], start = chunk[3 * q + 1], L = chunk[3 * q + 2];
+    for (int i = start + threadIdx.x; i < start + L; i += blockDim.x) {
+        const int64_t p0 = perm[i];
+        labels[p0] = h + 1;
+        if (!final_) skip_uniform2(rng, p0);   // the argmax of final mode draws nothing
+    }
+}
+
+// pass 2 for the chunks that kept other clusters, one block per tile of kPrTh points (blockIdx.x =
+// position in the list, blockIdx.y = tile): r of the kept clusters (r_h from pass 1; every cluster when
+// the chunk kept more than kPrMaxCand).  A point whose kept clusters all lie more than the
 // margin below r_h takes h + 1 as well (the chunk bound's guarantee, now from the exact r); the others
 // get the draw (or argmax) of the dense label phase over all K columns, the left-out clusters at -inf.
 // Shared memory: DP*DP + DP + K*kPrTh floats.
@@ -606,14 +650,13 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
                                                       const float* __restrict__ bvec, const float* __restrict__ cvec,
                                                       int K, int final_, RngArgs rng, const float* __restrict__ rh,
                                                       const int32_t* __restrict__ cand, float margin,
-                                                      int32_t* __restrict__ labels)
+                                                      const int32_t* __restrict__ list, int32_t* __restrict__ labels)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     float* sW = reinterpret_cast<float*>(smem);
     float* sbv = sW + DP * DP;
     float* sr = sbv + DP;
-    const int q = blockIdx.x, t = threadIdx.x;
-    if (q >= *nchunks) return;
+    const int q = list[blockIdx.x], t = threadIdx.x;
     const int h = chunk[3 * q], start = chunk[3 * q + 1], L = chunk[3 * q + 2];
     const int base = start + (int)blockIdx.y * kPrTh;
     if (base >= start + L) return;
@@ -621,14 +664,6 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
     const int n = cq[0];
     const int i = base + t;
     const bool valid = i < start + L;
-    if (n == 0) {
-        if (valid) {
-            const int64_t p0 = perm[i];
-            labels[p0] = h + 1;
-            if (!final_) skip_uniform2(rng, p0);   // the argmax of final mode draws nothing
-        }
-        return;
-    }
     const bool all = n > kPrMaxCand;      // over capacity: every cluster
     const int64_t pt = valid ? perm[i] : 0;
     float xr[DP];
@@ -689,12 +724,16 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
             c->d_prune_cnt);
         DPMM_LAUNCHED();
     }
+    int32_t* d_nlist = c->d_aux + 2;
+    k_prune_list<<<1, 1024, 0, c->stream>>>(c->d_nchunks, c->d_prune_cand, c->d_prune_list, d_nlist);
+    DPMM_LAUNCHED();
     unsigned long long* h = reinterpret_cast<unsigned long long*>(c->h_pinned);
     int32_t* outside = reinterpret_cast<int32_t*>(h + 2);   // points whose label has no chunk
     DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_prune_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
                                   c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(outside, c->d_aux + 8 + K, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(outside + 1, d_err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(outside + 2, d_nlist, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (outside[1])
         return fail(DPMM_ERR_TIMEOUT, "tensor-core scan: bounded wait expired (code " + std::to_string(outside[1]) + ")");
@@ -713,11 +752,18 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     DPMM_CUDA_TRY(cudaFuncSetAttribute(k_prune_draw<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     {
         KernelTimer kt(c, PH_PRUNE_DRAW);
-        const dim3 grid((unsigned)c->max_chunks, (unsigned)((c->chunk_len + kPrTh - 1) / kPrTh));
-        k_prune_draw<DP><<<grid, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
-                                                        c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
-                                                        c->d_prune_cand, c->prune_margin, c->d_labels);
+        k_prune_settle<<<c->max_chunks, 256, 0, c->stream>>>(c->d_perm, c->d_chunk, c->d_nchunks, c->d_prune_cand,
+                                                             final_, r, c->d_labels);
         DPMM_LAUNCHED();
+        const int nlist = outside[2];
+        if (nlist > 0) {
+            const dim3 grid((unsigned)nlist, (unsigned)((c->chunk_len + kPrTh - 1) / kPrTh));
+            k_prune_draw<DP><<<grid, kPrTh, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Wt,
+                                                            c->d_b, c->d_c, K, final_, r, c->d_prune_rh,
+                                                            c->d_prune_cand, c->prune_margin, c->d_prune_list,
+                                                            c->d_labels);
+            DPMM_LAUNCHED();
+        }
     }
     c->prune_used += 1;
     c->prune_extra += extra;

@@ -627,7 +627,8 @@ struct SubSmem {
     static constexpr size_t a = STAGE_BYTES;              // 32 KB A tile (hi, lo)
     static constexpr size_t q = a + A_TILE;               // r of both sides [2][BM] floats
     static constexpr size_t bias = q + 2 * BM * 4;        // b_l, b_r [2][KD] floats
-    static constexpr size_t bar = bias + 2 * KD * 4;      // mbarrier, tmem slot, flag
+    static constexpr size_t pidx = bias + 2 * KD * 4;     // the tile's permutation entries [2][BM] ints
+    static constexpr size_t bar = pidx + 2 * BM * 4;      // mbarrier, tmem slot, flag
     static constexpr size_t total = bar + 32 + 1024;      // + alignment slack
 };
 
@@ -644,6 +645,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
     uint8_t* sA = smem + SubSmem::a;
     float* sq = reinterpret_cast<float*>(smem + SubSmem::q);
     float* sbias = reinterpret_cast<float*>(smem + SubSmem::bias);
+    int32_t* spidx = reinterpret_cast<int32_t*>(smem + SubSmem::pidx);
     uint64_t* bar = reinterpret_cast<uint64_t*>(smem + SubSmem::bar);
     uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
     volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
@@ -685,7 +687,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
     // gathered rows: item u of this thread is (row tid / 8 + 32 u, 8-float chunk tid % 8); a tile's
     // permutation entries load one tile ahead of its rows
     float4 pf[4][2];
-    int pq[4];
+    int pq[4], pcur[4];   // entries of the tile after the loaded one / of the loaded one
     auto load_perm = [&](int t0) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
@@ -697,6 +699,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int c8 = tid & 7;
+            pcur[u] = pq[u];
             pf[u][0] = make_float4(0.f, 0.f, 0.f, 0.f);
             pf[u][1] = pf[u][0];
             if (pq[u] >= 0 && c8 * 8 < DP) {
@@ -727,6 +730,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
             const uint32_t off = sw128_offset(row, c8 * 8);
             *reinterpret_cast<uint4*>(sA + off) = *reinterpret_cast<const uint4*>(hi);
             *reinterpret_cast<uint4*>(sA + A_BYTES + off) = *reinterpret_cast<const uint4*>(lo);
+            if (c8 == 0) spidx[((t0 / BM) & 1) * BM + row] = pcur[u];   // for the draw, two tiles apart
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
@@ -783,7 +787,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
         tc_fence_before();
         __syncthreads();
         if (tid < nt) {
-            const int64_t pt = perm[start + t0 + tid];
+            const int64_t pt = spidx[((t0 / BM) & 1) * BM + tid];
             float rl = sq[tid], rr = sq[BM + tid];
             if (r_out) { r_out[2 * pt] = rl; r_out[2 * pt + 1] = rr; }
             rl += wl;
