@@ -111,6 +111,17 @@ def _iptr(a):
     return a.ctypes.data_as(ctypes.POINTER(c_int32)) if a is not None else None
 
 
+def nmi_from_table(table):
+    """(NMI, variation of information in nats) from a K x G table of counts (host only)."""
+    t = np.ascontiguousarray(table, np.int64)
+    if t.ndim != 2:
+        raise ValueError("table must be 2-D")
+    nmi, vi = ctypes.c_double(), ctypes.c_double()
+    check(lib().dpmm_nmi_from_table(t.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), t.shape[0], t.shape[1],
+                                    ctypes.byref(nmi), ctypes.byref(vi)))
+    return nmi.value, vi.value
+
+
 def _points_major(all_data, numLabels=None) -> np.ndarray:
     """D x N (reference layout) -> contiguous N x D float64."""
     x = np.asarray(all_data, dtype=np.float64)
@@ -307,6 +318,23 @@ class CudaKernel:
         out = np.empty(self.N, np.int32)
         check(lib().dpmm_get_labels(self.ctx, _iptr(out)))
         return out
+
+    def set_ground_truth(self, gt):
+        """Upload one int32 ground-truth value per point (None clears it) for label_agreement."""
+        if gt is None:
+            check(lib().dpmm_set_ground_truth(self.ctx, None))
+            return
+        a = np.ascontiguousarray(gt, np.int32)
+        if a.size != self.N:
+            raise ValueError("ground truth needs one value per point")
+        check(lib().dpmm_set_ground_truth(self.ctx, _iptr(a)))
+
+    def label_agreement(self, K: int):
+        """(NMI, variation of information in nats) of the current labels 1..K against the ground
+        truth, counted on the device (the verbose-mode score of dp_parallel_sampling.cpp:161-179)."""
+        nmi, vi = ctypes.c_double(), ctypes.c_double()
+        check(lib().dpmm_label_agreement(self.ctx, int(K), ctypes.byref(nmi), ctypes.byref(vi)))
+        return nmi.value, vi.value
 
     def get_sub_labels(self) -> np.ndarray:
         out = np.empty(self.N, np.int32)

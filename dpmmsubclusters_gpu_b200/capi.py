@@ -140,6 +140,9 @@ SIGNATURES = {
     "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
     "dpmm_set_label_pruning": (c_int, [_CTX, c_double]),
     "dpmm_label_pruning_stats": (c_int, [_CTX, _PD]),
+    "dpmm_set_ground_truth": (c_int, [_CTX, _PI32]),
+    "dpmm_label_agreement": (c_int, [_CTX, c_int, _PD, _PD]),
+    "dpmm_nmi_from_table": (c_int, [_PI64, c_int, c_int, _PD, _PD]),
     "dpmm_batch_create": (c_int, [c_int32, POINTER(dpmm_run_desc), _PI64, _PI32, POINTER(_PD), POINTER(c_void_p)]),
     "dpmm_batch_step": (c_int, [c_void_p, c_int32]),
     "dpmm_batch_info": (c_int, [c_void_p, _PI64]),

@@ -6,6 +6,7 @@
 #include <curand_kernel.h>
 
 #include <algorithm>
+#include <unordered_map>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -90,6 +91,31 @@ __global__ void k_count_nonfinite(const float* __restrict__ x, int64_t n, int32_
     if (i < n && !isfinite(x[i])) atomicAdd(bad, 1);
 }
 
+// Contingency table of the labels 1..K against the dense ground-truth ids 0..G-1: table[k][g] =
+// points with label k + 1 and ground truth g (labels outside 1..K are not counted).  Counts per block
+// in shared memory when the table fits, else global atomics.
+constexpr int kCtabSmem = 12288;
+__global__ void __launch_bounds__(256) k_contingency(const int32_t* __restrict__ labels, const int32_t* __restrict__ gt,
+                                                     int64_t N, int K, int G, unsigned long long* __restrict__ table)
+{
+    extern __shared__ unsigned int sct[];
+    const int T = K * G;
+    const bool local = T <= kCtabSmem;
+    if (local)
+        for (int e = threadIdx.x; e < T; e += blockDim.x) sct[e] = 0u;
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+        const int l = labels[i] - 1, g = gt[i];
+        if (l < 0 || l >= K || g < 0 || g >= G) continue;
+        if (local) atomicAdd(&sct[l * G + g], 1u);
+        else atomicAdd(&table[(size_t)l * G + g], 1ull);
+    }
+    __syncthreads();
+    if (local)
+        for (int e = threadIdx.x; e < T; e += blockDim.x)
+            if (sct[e]) atomicAdd(&table[e], (unsigned long long)sct[e]);
+}
+
 }  // namespace dpmm
 
 using namespace dpmm;
@@ -152,7 +178,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
-                    c->d_prune_beta, c->d_prune_list};
+                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -1145,4 +1171,83 @@ extern "C" dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* c, double* out)
     out[4] = c->prune_last_extra;
     out[5] = (double)c->prune_last_over;
     return DPMM_OK;
+}
+
+// ----------------------------------------------------------------- label agreement (verbose mode)
+// NMI = 2 I(X;Y) / (H(X) + H(Y)) as dp_parallel_sampling.cpp:171-179 computes it (through MIToolbox's
+// calcMutualInformation / calcEntropy; the ratio does not depend on the logarithm's base), and the
+// variation of information H(X) + H(Y) - 2 I(X;Y) in nats, from a contingency table.
+extern "C" dpmm_status dpmm_nmi_from_table(const int64_t* table, int K, int G, double* nmi, double* vi)
+{
+    if (!table || K < 1 || G < 1) return fail(DPMM_ERR_INVALID_ARG, "bad contingency table");
+    std::vector<double> a(K, 0.0), b(G, 0.0);
+    double n = 0.0;
+    for (int k = 0; k < K; ++k)
+        for (int g = 0; g < G; ++g) {
+            const double v = (double)table[(size_t)k * G + g];
+            a[k] += v;
+            b[g] += v;
+            n += v;
+        }
+    if (n <= 0) return fail(DPMM_ERR_INVALID_ARG, "empty contingency table");
+    double ha = 0, hb = 0, mi = 0;
+    for (double v : a) if (v > 0) ha -= v / n * std::log(v / n);
+    for (double v : b) if (v > 0) hb -= v / n * std::log(v / n);
+    for (int k = 0; k < K; ++k)
+        for (int g = 0; g < G; ++g) {
+            const double v = (double)table[(size_t)k * G + g];
+            if (v > 0) mi += v / n * std::log(v * n / (a[k] * b[g]));
+        }
+    if (nmi) *nmi = (ha + hb) > 0 ? 2 * mi / (ha + hb) : 1.0;
+    if (vi) *vi = std::max(0.0, ha + hb - 2 * mi);
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_ground_truth(dpmm_ctx* c, const int32_t* gt)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    if (c->d_gt) cudaFree(c->d_gt);
+    if (c->d_ctab) cudaFree(c->d_ctab);
+    c->d_gt = nullptr;
+    c->d_ctab = nullptr;
+    c->gt_G = 0;
+    if (!gt) return DPMM_OK;
+    // dense ids in order of first appearance
+    std::vector<int32_t> ids(c->N);
+    std::unordered_map<int32_t, int32_t> map;
+    for (int64_t i = 0; i < c->N; ++i) {
+        auto it = map.emplace(gt[i], (int32_t)map.size()).first;
+        ids[i] = it->second;
+    }
+    const int G = (int)map.size();
+    if ((size_t)G * (size_t)c->k_max > ((size_t)1 << 26))
+        return fail(DPMM_ERR_INVALID_ARG, "too many ground-truth classes for k_max (k_max x classes > 2^26)");
+    DPMM_TRY(dev_alloc(&c->d_gt, (size_t)c->N));
+    DPMM_TRY(dev_alloc(&c->d_ctab, (size_t)G * c->k_max));
+    DPMM_CUDA_TRY(cudaMemcpy(c->d_gt, ids.data(), sizeof(int32_t) * (size_t)c->N, cudaMemcpyHostToDevice));
+    g_h2d_bytes += sizeof(int32_t) * (size_t)c->N;
+    c->gt_G = G;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_label_agreement(dpmm_ctx* c, int K, double* nmi, double* vi)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    if (!c->d_gt) return fail(DPMM_ERR_STATE, "no ground truth set (dpmm_set_ground_truth)");
+    if (K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [1, k_max]");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    const int G = c->gt_G;
+    const size_t T = (size_t)K * G;
+    DPMM_CUDA_TRY(cudaMemsetAsync(c->d_ctab, 0, sizeof(unsigned long long) * T, c->stream));
+    const size_t sm = T <= (size_t)kCtabSmem ? sizeof(unsigned int) * T : 0;
+    const int64_t blocks = std::min<int64_t>((c->N + 255) / 256, (int64_t)c->num_sms * 4);
+    k_contingency<<<(unsigned)std::max<int64_t>(blocks, 1), 256, sm, c->stream>>>(c->d_labels, c->d_gt, c->N, K, G,
+                                                                              c->d_ctab);
+    DPMM_LAUNCHED();
+    std::vector<int64_t> table(T);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(table.data(), c->d_ctab, sizeof(int64_t) * T, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    g_d2h_bytes += sizeof(int64_t) * T;
+    return dpmm_nmi_from_table(table.data(), K, G, nmi, vi);
 }

@@ -204,6 +204,10 @@ struct dpmm_ctx {
     float* d_prune_M = nullptr;    // [KP][KP]
     float* d_prune_V = nullptr;    // [KP][KP][Dp] point-bound directions
     float* d_prune_beta = nullptr; // [KP][KP]
+    // ground truth for the label agreement scores (dpmm_set_ground_truth)
+    int32_t* d_gt = nullptr;       // [N] dense ground-truth ids 0..gt_G-1
+    int gt_G = 0;
+    unsigned long long* d_ctab = nullptr;   // [k_max][gt_G] contingency counts
     unsigned long long* d_prune_cnt = nullptr;   // [2]
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;

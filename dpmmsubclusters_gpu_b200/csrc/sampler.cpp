@@ -324,7 +324,6 @@ private:
     dpmm_status group_step(bool no_more_splits, bool final_);
     dpmm_status init_first_clusters();
     dpmm_status calculate_posterior(double* out);
-    double nmi(const std::vector<int32_t>& labels) const;
     Config cfg_;
     dpmm_ctx* ctx_;
     int64_t N_;
@@ -963,34 +962,6 @@ dpmm_status Sampler::calculate_posterior(double* out)
     return DPMM_OK;
 }
 
-// NMI = 2 I(X;Y) / (H(X) + H(Y)) (dp_parallel_sampling.cpp:171-179)
-double Sampler::nmi(const std::vector<int32_t>& labels) const
-{
-    const size_t n = std::min(labels.size(), cfg_.gt.size());
-    if (n == 0) return NAN;
-    std::map<int32_t, int> ia, ib;
-    for (size_t i = 0; i < n; ++i) {
-        ia.emplace(cfg_.gt[i], (int)ia.size());
-        ib.emplace(labels[i], (int)ib.size());
-    }
-    std::vector<double> ca(ia.size(), 0), cb(ib.size(), 0), joint(ia.size() * ib.size(), 0);
-    for (size_t i = 0; i < n; ++i) {
-        int a = ia[cfg_.gt[i]], b = ib[labels[i]];
-        ca[a] += 1;
-        cb[b] += 1;
-        joint[(size_t)a * ib.size() + b] += 1;
-    }
-    double ha = 0, hb = 0, mi = 0;
-    for (double v : ca) if (v > 0) ha -= v / n * std::log(v / n);
-    for (double v : cb) if (v > 0) hb -= v / n * std::log(v / n);
-    for (size_t a = 0; a < ca.size(); ++a)
-        for (size_t b = 0; b < cb.size(); ++b) {
-            double v = joint[a * cb.size() + b];
-            if (v > 0) mi += v / n * std::log(v * n / (ca[a] * cb[b]));
-        }
-    return (ha + hb) > 0 ? 2 * mi / (ha + hb) : 1.0;
-}
-
 // dp_parallel_sampling_class::run_model (dp_parallel_sampling.cpp:132-206), n iterations at a time
 dpmm_status Sampler::step(int n, dpmm_model_info* mi)
 {
@@ -1027,10 +998,10 @@ dpmm_status Sampler::end_iteration(const IterState& st, dpmm_model_info* mi)
             double lp = 0;
             DPMM_TRY(calculate_posterior(&lp));
             mi->likelihood_history.push_back(lp);
-            if (!cfg_.gt.empty()) {
-                std::vector<int32_t> lab(N_);
-                DPMM_TRY(dpmm_get_labels(ctx_, lab.data()));
-                mi->nmi_history.push_back(nmi(lab));
+            if (!cfg_.gt.empty()) {   // scored on the device: only the contingency table comes back
+                double v = 0;
+                DPMM_TRY(dpmm_label_agreement(ctx_, (int)clusters_.size(), &v, nullptr));
+                mi->nmi_history.push_back(v);
             }
             std::printf("Iteration: %d || Clusters count: %d || Log posterior: %f || NMI score: %f || Iter Time: %f\n", i,
                         (int)clusters_.size(), mi->likelihood_history.back(),
@@ -1133,6 +1104,10 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
     else
         DPMM_TRY(dpmm_set_prior_multinomial(h->ctx, cfg.hyper.alpha.data()));
     if (h->ctx->d_prune_rh) DPMM_TRY(dpmm_set_label_pruning(h->ctx, cfg.label_prune_margin));
+    if (cfg.verbose && !cfg.gt.empty()) {
+        if ((int64_t)cfg.gt.size() != N) return fail(DPMM_ERR_INVALID_ARG, "ground truth needs one value per point");
+        DPMM_TRY(dpmm_set_ground_truth(h->ctx, cfg.gt.data()));
+    }
     if (cfg.screen_mode == DPMM_SCREEN_ON) {
         if ((int)cfg.screen_params.size() != kScrParams)
             return fail(DPMM_ERR_INVALID_ARG, "screen_mode DPMM_SCREEN_ON needs screen_params");

@@ -328,6 +328,18 @@ dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, 
 dpmm_status dpmm_set_label_pruning(dpmm_ctx* ctx, double margin);
 dpmm_status dpmm_label_pruning_stats(const dpmm_ctx* ctx, double* out);
 
+/* ---- agreement of the labels with a ground truth (verbose mode; replaces the label download and
+ * MIToolbox scoring of dp_parallel_sampling.cpp:161-179) ----------------------------------------
+ * dpmm_set_ground_truth uploads N int32 ground-truth values once (any values: mapped to dense
+ * classes in order of first appearance; NULL clears them).  dpmm_label_agreement counts the (label
+ * 1..K, class) pairs of the current labels on the device and scores the K x classes table on the
+ * host: nmi = 2 I / (H(ground truth) + H(labels)) (1 when both entropies are 0), vi = H + H - 2 I in
+ * nats; either output may be NULL.  dpmm_nmi_from_table is that host part for a caller's K x G
+ * row-major table of counts. */
+dpmm_status dpmm_set_ground_truth(dpmm_ctx* ctx, const int32_t* gt);
+dpmm_status dpmm_label_agreement(dpmm_ctx* ctx, int K, double* nmi, double* vi);
+dpmm_status dpmm_nmi_from_table(const int64_t* table, int K, int G, double* nmi, double* vi);
+
 /* Synchronise the context's stream; returns any pending device error. */
 dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
 
