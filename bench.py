@@ -123,11 +123,13 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
         f"2*N*K*D^2 FLOP per launch (one product; the split form issues 3), K mean {k_mean:.1f}",
         label_kernel_traffic(N, k_mean))
     if tc:
-        add("k_prune_scan_tc", 8, "hbm", N * (Dp * 4.0 + 12), "GB/s", hbm, "hbm_gbs",
-            "N*(Dp*4 + 12) B per launch: every point read once from HBM (the bound pass re-reads the "
-            "chunk from L2), its permutation index, r_h written; tensor-core products 3 x 2*N*Dp*64 FLOP "
-            "+ 3 x 2*N*Dp*kept-candidates",
-            per_point_traffic("k_prune_scan_tc_N1e6_D64.md", N) if Dp == 64 else None)
+        one_pass = k_mean <= 193   # k_prune_scan1_tc; above, the two-pass k_prune_scan_tc
+        add("k_prune_scan1_tc" if one_pass else "k_prune_scan_tc", 8, "hbm", N * (Dp * 4.0 + 12), "GB/s", hbm,
+            "hbm_gbs",
+            "N*(Dp*4 + 12) B per launch: every point read once from HBM, its permutation index, r_h written; "
+            "tensor-core products 3 x 2*N*Dp*(64 + K - 1) FLOP (one pass: r_h and every cluster's bound "
+            "direction)",
+            per_point_traffic("k_prune_scan1_tc_N1e6_D64.md", N) if Dp == 64 and one_pass else None)
         add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
             "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP",

@@ -207,6 +207,7 @@ struct dpmm_ctx {
     // ground truth for the label agreement scores (dpmm_set_ground_truth)
     int32_t* d_gt = nullptr;       // [N] dense ground-truth ids 0..gt_G-1
     int gt_G = 0;
+    bool sub_err_pending = false;  // the sub-label kernel's error word awaits the statistics launch's sync
     unsigned long long* d_ctab = nullptr;   // [k_max][gt_G] contingency counts
     unsigned long long* d_prune_cnt = nullptr;   // [2]
     double* h_pinned = nullptr;    // pinned staging for D2H of results
@@ -325,7 +326,8 @@ dpmm_status pack_tc_points(dpmm_ctx* c);   // A operand from the uploaded points
 size_t tc_param_bytes(int k_max);          // B tiles + bias records for k_max clusters
 // tensor-core sub-label kernel (dpmm_tc.cu): draws the sub-labels only (statistics separately)
 bool tc_sub_supported(const dpmm_ctx* c);
-dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout);
+// defer_check: its error word is read by the statistics launch that follows (one sync for both)
+dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout, bool defer_check = false);
 // pass 1 of the pruned label phase on the tensor cores (dpmm_tc.cu; Dp = 32 or 64, packed B tiles)
 bool tc_scan_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err);

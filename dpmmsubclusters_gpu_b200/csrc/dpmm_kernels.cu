@@ -851,27 +851,49 @@ __global__ void k_scan_bins(int32_t* __restrict__ blk_hist, int nblk, int K, int
 }
 
 // single block: segment starts and the chunk table (cluster, start, len) of <= chunk_len points
-__global__ void k_segments(const int32_t* __restrict__ total, int K, int32_t* __restrict__ seg,
-                           int32_t* __restrict__ chunk, int32_t* __restrict__ nchunks, int max_chunks,
-                           int chunk_len)
+__global__ void __launch_bounds__(1024) k_segments(const int32_t* __restrict__ total, int K,
+                                                   int32_t* __restrict__ seg, int32_t* __restrict__ chunk,
+                                                   int32_t* __restrict__ nchunks, int max_chunks, int chunk_len)
 {
-    if (threadIdx.x != 0) return;
-    int32_t acc = 0, nc = 0;
-    for (int k = 0; k <= K; ++k) {
+    // thread i takes bins [k0, k1); a block scan of the bins' point and chunk totals gives its offsets
+    __shared__ int32_t s_t[1024], s_c[1024];
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    const int items = K + 1;   // cluster bins 0..K-1 and bin K (labels outside 1..K: no chunks)
+    const int per = (items + nthr - 1) / nthr;
+    const int k0 = min(items, tid * per), k1 = min(items, k0 + per);
+    int32_t st = 0, sc = 0;
+    for (int k = k0; k < k1; ++k) {
+        const int32_t t = total[k];
+        st += t;
+        if (k < K) sc += (t + chunk_len - 1) / chunk_len;
+    }
+    s_t[tid] = st;
+    s_c[tid] = sc;
+    __syncthreads();
+    for (int o = 1; o < nthr; o <<= 1) {   // inclusive scan
+        const int32_t a = tid >= o ? s_t[tid - o] : 0, c = tid >= o ? s_c[tid - o] : 0;
+        __syncthreads();
+        s_t[tid] += a;
+        s_c[tid] += c;
+        __syncthreads();
+    }
+    int32_t acc = s_t[tid] - st, nc = s_c[tid] - sc;
+    for (int k = k0; k < k1; ++k) {
         seg[k] = acc;
-        int32_t t = total[k];
-        if (k < K) {
-            for (int32_t s = 0; s < t && nc < max_chunks; s += chunk_len) {
-                chunk[3 * nc + 0] = k;
-                chunk[3 * nc + 1] = acc + s;
-                chunk[3 * nc + 2] = min(chunk_len, t - s);
-                ++nc;
-            }
-        }
+        const int32_t t = total[k];
+        if (k < K)
+            for (int32_t s = 0; s < t; s += chunk_len, ++nc)
+                if (nc < max_chunks) {
+                    chunk[3 * nc + 0] = k;
+                    chunk[3 * nc + 1] = acc + s;
+                    chunk[3 * nc + 2] = min(chunk_len, t - s);
+                }
         acc += t;
     }
-    seg[K + 1] = acc;
-    *nchunks = nc;
+    if (tid == nthr - 1) {
+        seg[K + 1] = s_t[nthr - 1];
+        *nchunks = min(s_c[nthr - 1], max_chunks);
+    }
 }
 
 __global__ void k_scatter(const int32_t* __restrict__ labels, int64_t N, int K, const int32_t* __restrict__ blk_off,
@@ -915,7 +937,7 @@ dpmm_status build_permutation(dpmm_ctx* c, int K)
     int32_t* total = c->d_aux + 8;   // K+1 entries
     k_scan_bins<<<K + 1, 1024, 0, c->stream>>>(c->d_blk_hist, nblk, K, total);
     DPMM_LAUNCHED();
-    k_segments<<<1, 32, 0, c->stream>>>(total, K, c->d_seg, c->d_chunk, c->d_nchunks, c->max_chunks,
+    k_segments<<<1, 1024, 0, c->stream>>>(total, K, c->d_seg, c->d_chunk, c->d_nchunks, c->max_chunks,
                                          c->chunk_len);
     DPMM_LAUNCHED();
     size_t sm = sizeof(int32_t) * 9 * (K + 1);
@@ -1614,7 +1636,9 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
     RngArgs r = rng_args(c, d_u);
     if (draw && !d_mask && tc_sub_supported(c)) {
         // sub-labels on the tensor cores, then the statistics of the drawn sub-labels
-        DPMM_TRY(launch_sub_labels_tc(c, r, d_rout));
+        // its error word is read in the statistics launch's sync when that runs on the tensor cores
+        DPMM_TRY(launch_sub_labels_tc(c, r, d_rout, c->prior == DPMM_PRIOR_GAUSSIAN && c->Dp <= 64 &&
+                                                        tc_stats_supported(c)));
         draw = false;
     }
     if (c->prior == DPMM_PRIOR_GAUSSIAN) {

@@ -1880,12 +1880,16 @@ static dpmm_status launch_sub_labels_tc_t(dpmm_ctx* c, RngArgs r, float* d_rout,
     return DPMM_OK;
 }
 
-dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout)
+dpmm_status launch_sub_labels_tc(dpmm_ctx* c, RngArgs r, float* d_rout, bool defer_check)
 {
     int32_t* err = c->d_aux + 5;
     DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
     if (c->Dp == 64) DPMM_TRY(launch_sub_labels_tc_t<64>(c, r, d_rout, err));
     else DPMM_TRY(launch_sub_labels_tc_t<32>(c, r, d_rout, err));
+    if (defer_check) {
+        c->sub_err_pending = true;
+        return DPMM_OK;
+    }
     int32_t h_err = 0;
     DPMM_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
@@ -1948,8 +1952,14 @@ dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask)
         else DPMM_TRY(launch_slot_stats_tc_t<32>(c, d_mask, err));
     }
     int32_t* h_err = reinterpret_cast<int32_t*>(c->h_pinned);
+    h_err[1] = 0;
     DPMM_CUDA_TRY(cudaMemcpyAsync(h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (c->sub_err_pending)
+        DPMM_CUDA_TRY(cudaMemcpyAsync(h_err + 1, c->d_aux + 5, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->sub_err_pending = false;
+    if (h_err[1]) return fail(DPMM_ERR_TIMEOUT, "tensor-core sub-label kernel: bounded wait expired (code " +
+                                                    std::to_string(h_err[1]) + ")");
     if (*h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core statistics: bounded wait expired (code " +
                                                   std::to_string(*h_err) + ")");
     return DPMM_OK;
