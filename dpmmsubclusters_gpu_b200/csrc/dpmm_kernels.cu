@@ -396,21 +396,38 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
 {
     constexpr int NW = kPrTh / 32;
     constexpr int SW = DP + 1;   // padded row stride: the z loop's lanes read one column each
+    constexpr int TPR = kPrTh / DP < DP ? kPrTh / DP : DP;   // threads per Gershgorin row (each >= 1 column)
+    static_assert(kPrTh % DP == 0 && DP % TPR == 0, "row split");
     __shared__ float sW[DP * SW];
     __shared__ double red[NW];
+    __shared__ double srow_part[kPrTh];
     __shared__ double zs[NW][DP];
+    __shared__ double dm[NW][DP];
     const int k = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
     for (int e = t; e < DP * DP; e += blockDim.x) sW[(e / DP) * SW + e % DP] = Wt[(size_t)3 * k * DP * DP + e];
     __syncthreads();
-    double rmax = 0;
-    for (int i = t; i < DP; i += blockDim.x) {
+    if (t < DP * TPR) {   // Gershgorin row sums of W W^T: row t % DP, column share t / DP, four chains
+        const int i = t % DP, j0 = (t / DP) * (DP / TPR);
         double srow = 0;
-        for (int j = 0; j < DP; ++j) {
-            double l = 0;
-            for (int cc = 0; cc < DP; ++cc) l += (double)sW[cc * SW + i] * (double)sW[cc * SW + j];
-            srow += fabs(l);
+        for (int j = j0; j < j0 + DP / TPR; ++j) {
+            double l0 = 0, l1 = 0, l2 = 0, l3 = 0;
+#pragma unroll
+            for (int cc = 0; cc < DP; cc += 4) {
+                l0 = fma((double)sW[cc * SW + i], (double)sW[cc * SW + j], l0);
+                l1 = fma((double)sW[(cc + 1) * SW + i], (double)sW[(cc + 1) * SW + j], l1);
+                l2 = fma((double)sW[(cc + 2) * SW + i], (double)sW[(cc + 2) * SW + j], l2);
+                l3 = fma((double)sW[(cc + 3) * SW + i], (double)sW[(cc + 3) * SW + j], l3);
+            }
+            srow += fabs((l0 + l1) + (l2 + l3));
         }
-        rmax = fmax(rmax, srow);
+        srow_part[t] = srow;
+    }
+    __syncthreads();
+    double rmax = 0;
+    if (t < DP) {
+        double tot = 0;
+        for (int p = 0; p < TPR; ++p) tot += srow_part[t + p * DP];
+        rmax = tot;
     }
 #pragma unroll
     for (int o = 16; o; o >>= 1) rmax = fmax(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
@@ -424,10 +441,19 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
     const float* mk = mu + (size_t)3 * k * DP;
     for (int h = warp; h < K; h += NW) {
         const float* mh = mu + (size_t)3 * h * DP;
+        for (int i = lane; i < DP; i += 32) dm[warp][i] = (double)mh[i] - (double)mk[i];
+        __syncwarp();
         double q = 0;
         for (int j = lane; j < DP; j += 32) {   // z = W_k^T (mu_h - mu_k)
-            double z = 0;
-            for (int i = 0; i < DP; ++i) z += (double)sW[j * SW + i] * ((double)mh[i] - (double)mk[i]);
+            double z0 = 0, z1 = 0, z2 = 0, z3 = 0;
+#pragma unroll
+            for (int i = 0; i < DP; i += 4) {
+                z0 = fma((double)sW[j * SW + i], dm[warp][i], z0);
+                z1 = fma((double)sW[j * SW + i + 1], dm[warp][i + 1], z1);
+                z2 = fma((double)sW[j * SW + i + 2], dm[warp][i + 2], z2);
+                z3 = fma((double)sW[j * SW + i + 3], dm[warp][i + 3], z3);
+            }
+            const double z = (z0 + z1) + (z2 + z3);
             zs[warp][j] = z;
             q += z * z;
         }
@@ -439,9 +465,15 @@ __global__ void __launch_bounds__(kPrTh) k_prune_prep(const float* __restrict__ 
         float* vh = V + ((size_t)h * K + k) * DP;
         double bsum = 0;
         for (int i = lane; i < DP; i += 32) {    // v = W_k u, u = z / |z|
-            double v = 0;
-            for (int j = 0; j < DP; ++j) v += (double)sW[j * SW + i] * zs[warp][j];
-            v *= inv;
+            double v0 = 0, v1 = 0, v2 = 0, v3 = 0;
+#pragma unroll
+            for (int j = 0; j < DP; j += 4) {
+                v0 = fma((double)sW[j * SW + i], zs[warp][j], v0);
+                v1 = fma((double)sW[(j + 1) * SW + i], zs[warp][j + 1], v1);
+                v2 = fma((double)sW[(j + 2) * SW + i], zs[warp][j + 2], v2);
+                v3 = fma((double)sW[(j + 3) * SW + i], zs[warp][j + 3], v3);
+            }
+            const double v = ((v0 + v1) + (v2 + v3)) * inv;
             vh[i] = (float)v;
             bsum += (double)(float)v * (double)mk[i];
         }
