@@ -776,7 +776,7 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     // each kept cluster costs about one more exact r per point; beyond 2 per point the dense phase
     // (tensor cores where available) is the cheaper one: run it, and wait before the next attempt
     if (extra > 2.0 || *outside != 0) {
-        c->prune_wait = 4;
+        c->prune_wait = 2;
         return DPMM_OK;
     }
     const RngArgs r = rng_args(c, d_u);

@@ -1447,7 +1447,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
 //   D = A B^T (M = 128, N = Dp + 16)        D[64 s + i][j] = sum c_i c_j, D[64 s + i][Dp] = sum c_i
 // The operands are split TF32 (hi = rna(c), lo = rna(c - hi), |c - hi - lo| <= 2^-22 |c|) and
 // D = A_hi B_hi + A_lo B_hi + A_hi B_lo (12 tcgen05.mma of K = 8).  The accumulator runs over a
-// group of ST_G tiles (FP32 over 128 points: 48 accumulator roundings) and is then added into FP64
+// group of ST_G tiles (FP32 over 256 points: 96 accumulator roundings) and is then added into FP64
 // registers; two accumulators in TMEM alternate by group.  The products are centred at the mean a
 // of the chunk's first tile (within a cluster's spread of every point, wherever mu_k lies) and the
 // totals moved to mu_k in FP64 at the end:
@@ -1459,7 +1459,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
 constexpr int ST_P = 32;                   // points per tile: one 128-byte TF32 K row
 constexpr int ST_STAGES = 4;               // staged tiles of rows (3 in flight)
 constexpr int ST_PERM = 8;                 // staged tiles of permutation entries
-constexpr int ST_G = 4;                    // tiles per accumulation group
+constexpr int ST_G = 8;                    // tiles per accumulation group
 constexpr uint32_t ST_TMEM_COLS = 256;     // two accumulators, at columns 0 and 128
 
 template <int DP>

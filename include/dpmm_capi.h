@@ -320,7 +320,7 @@ dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, 
  * cluster, only the clusters that an upper bound cannot put more than `margin` nats below the chunk's
  * own cluster; the left-out clusters carry less than K e^-margin of each point's probability and get
  * probability 0 in the same draw.  When the bound keeps more than 2 other clusters per point (early
- * iterations) the dense phase runs and the next 4 label phases stay dense.  margin <= 0 switches it
+ * iterations) the dense phase runs and the next 2 label phases stay dense.  margin <= 0 switches it
  * off (default 30).
  * stats: out[0] attempts, out[1] label phases run pruned, out[2] mean kept other clusters per point
  * in those, out[3] the margin, out[4] the last attempt's kept other clusters per point, out[5] its
