@@ -348,7 +348,7 @@ private:
         return ncand > cfg_.screen_top && ncand >= min_cand ? USE_SCREEN : USE_FULL;
     }
     dpmm_status screen_log(int K, int kind, const std::vector<uint8_t>& row_ok, const double* hr_of_row);
-    void screen_judge();
+    void screen_assess();
 
 };
 
@@ -818,7 +818,7 @@ dpmm_status Sampler::screen_log(int K, int kind, const std::vector<uint8_t>& row
 }
 
 // after an iteration with a full sweep: switch the screen off when its recall is too low
-void Sampler::screen_judge()
+void Sampler::screen_assess()
 {
     if (!scr_swept_) return;
     scr_swept_ = false;
@@ -885,7 +885,7 @@ dpmm_status Sampler::stage_rest(bool no_more_splits, bool final_)
         DPMM_TRY(check_and_split(final_, idx));
         DPMM_TRY(update_suff_stats_posterior(idx));
         DPMM_TRY(check_and_merge(final_));
-        screen_judge();
+        screen_assess();
     }
     return remove_empty_clusters();
 }
