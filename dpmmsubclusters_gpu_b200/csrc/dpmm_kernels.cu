@@ -1645,7 +1645,7 @@ static dpmm_status launch_gauss_sub_stats_t(dpmm_ctx* c, int draw, RngArgs r, fl
             const size_t sm = SlotStatsShape<DP>::bytes;
             auto kern = k_gauss_slot_stats<DP>;
             DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            KernelTimer kt(c, PH_SLOT_STATS);
+            KernelTimer kt(d_mask ? nullptr : c, PH_SLOT_STATS);   // full launches only (masked: a few clusters)
             kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu,
                                                         c->d_sub, c->d_part, d_mask);
             DPMM_LAUNCHED();

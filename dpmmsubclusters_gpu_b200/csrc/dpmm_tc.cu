@@ -1947,7 +1947,7 @@ dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask)
     int32_t* err = c->d_aux + 3;
     DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
     {
-        KernelTimer kt(c, PH_SLOT_STATS);
+        KernelTimer kt(d_mask ? nullptr : c, PH_SLOT_STATS);   // full launches only (masked: a few clusters)
         if (c->Dp == 64) DPMM_TRY(launch_slot_stats_tc_t<64>(c, d_mask, err));
         else DPMM_TRY(launch_slot_stats_tc_t<32>(c, d_mask, err));
     }

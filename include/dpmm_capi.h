@@ -348,7 +348,8 @@ dpmm_status dpmm_synchronize(dpmm_ctx* ctx);
  * device->host; device time per phase of a context (ms[11], calls[11]: labels, sub-labels +
  * statistics, statistics only, split ratios, merge ratios, relabels, parameters, then single kernels
  * inside those phases: the tensor-core label kernel, the pruned label phase's scan and draw kernels,
- * and the sub-cluster statistics kernel) accumulated while timing is on.  enable = 1 / 0 switches
+ * and the sub-cluster statistics kernel over all clusters; its re-launches for a few clusters after
+ * moves are not timed) accumulated while timing is on.  enable = 1 / 0 switches
  * timing on / off and clears the counters, -1 only reads them.  Timing adds one event
  * synchronisation per phase and per timed kernel. */
 uint64_t dpmm_kernel_launch_count(void);
