@@ -7,11 +7,17 @@ weights, float32 data; NIW(kappa=1, m=0, nu=67, Psi=I), alpha = 10, 300 iteratio
 seeded synthetic draws of that generative model, generated on the device.
 
 A "step" is one sampler iteration (local_clusters_actions::group_step: parameter draws, label
-phase, sub-label + statistics phase, split and merge tests, relabels).  The sampler starts from
-initial_clusters = 100 and runs `--burnin` untimed iterations so that the timed iterations are at
-the configuration's steady state (about 100 clusters, split / merge tests active), then W warm-up
-iterations, then exactly K timed iterations bracketed by a barrier and device synchronisation,
-timed with CUDA events on the sampler's stream.  Inputs (2.56 GB) are larger than L2.
+phase, sub-label + statistics phase, split and merge tests, relabels).  The sampler starts from the
+reference's default of one cluster and runs `--burnin` untimed iterations (130: the split schedule
+doubles the clusters every ~15 iterations and reaches the configuration's 100 by about iteration 120),
+then W warm-up iterations, then exactly K timed iterations bracketed by a barrier and device
+synchronisation, timed with CUDA events on the sampler's stream.  Inputs (2.56 GB) are larger than L2.
+
+The metric compares the product path ("mixed": split-BF16 / split-TF32 tensor-core contractions, pruned
+label phase, device parameter draws, learned split / merge screen) with the plain FP32 form ("plain":
+dense FP32 SIMT label phase, SIMT statistics, host parameter draws, every candidate exact) run on the
+same data, seed and iteration counts in the same invocation: vs_baseline = value / plain's value, and
+both NMIs against the generating labels are reported.  --ablation adds the intermediate arms.
 
 --gpus N (under torchrun) runs N independent replicas, one per GPU, each on its own data set of
 the same shape (weak scaling; the path has no cross-GPU exchange in this form); value sums all
@@ -52,44 +58,30 @@ def peaks():
 
 
 # ----------------------------------------------------------------------------- workload
-LABEL_PROFILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles",
-                             "k_gauss_labels_tc_N1e6_D64.md")
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of single-launch ncu captures of the
+# timed kernels on a smaller case of the same workload (N = 1e6 points, D = 64; `ncu --set full
+# --clock-control none -k regex:<kernel> -c 1` of the C5 generator at N = 1e6), with the number of
+# points (and clusters) of that capture.  bench.py scales them to the timed launch by the kernel's
+# traffic model; they are a cross-check of the algorithmic bytes, not a live measurement.
+NCU_TRAFFIC = {
+    "k_gauss_labels_tc": {"dram_bytes": 619413504, "points": 1_000_000, "clusters": 95},
+    "k_prune_scan1_tc": {"dram_bytes": 270950144, "points": 1_000_000},
+    "k_slot_stats_tc": {"dram_bytes": 290109952, "points": 1_000_000},
+}
 
 
 def label_kernel_traffic(N, K):
-    """DRAM bytes per launch of the tensor-core label kernel: the ncu capture in LABEL_PROFILE
-    (a smaller case of the same kernel), scaled to (N, K) by the kernel's traffic model
-    N * (256 B packed points + 4 K B r + 16 B partials)."""
-    vals = {}
-    try:
-        with open(LABEL_PROFILE) as f:
-            for line in f:
-                for key in ("dram_bytes_per_launch", "capture_N", "capture_K"):
-                    if line.strip().startswith(key + ":"):
-                        vals[key] = float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        return None
-    if len(vals) != 3:
-        return None
+    """DRAM bytes per launch of the dense tensor-core label kernel, scaled from its ncu capture by
+    the kernel's traffic model N * (256 B packed points + 4 K B of r + 16 B partials)."""
+    c = NCU_TRAFFIC["k_gauss_labels_tc"]
     model = lambda n, k: n * (256.0 + 4.0 * k + 16.0)
-    return vals["dram_bytes_per_launch"] * model(N, K) / model(vals["capture_N"], vals["capture_K"])
+    return c["dram_bytes"] * model(N, K) / model(c["points"], c["clusters"])
 
 
-def per_point_traffic(profile, N):
-    """DRAM bytes per launch of a kernel that reads each point once: the ncu capture recorded in
-    profiles/<profile> (dram_bytes_per_launch at capture_N points, D = 64) scaled by N."""
-    vals = {}
-    try:
-        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", profile)) as f:
-            for line in f:
-                for key in ("dram_bytes_per_launch", "capture_N"):
-                    if line.strip().startswith(key + ":"):
-                        vals[key] = float(line.split(":", 1)[1].split()[0])
-    except OSError:
-        return None
-    if len(vals) != 2:
-        return None
-    return vals["dram_bytes_per_launch"] * N / vals["capture_N"]
+def per_point_traffic(kernel, N):
+    """DRAM bytes per launch of a kernel that reads each point once, scaled from its capture by N."""
+    c = NCU_TRAFFIC[kernel]
+    return c["dram_bytes"] * N / c["points"]
 
 
 def padded(d):
@@ -129,11 +121,11 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
             "N*(Dp*4 + 12) B per launch: every point read once from HBM, its permutation index, r_h written; "
             "tensor-core products 3 x 2*N*Dp*(64 + K - 1) FLOP (one pass: r_h and every cluster's bound "
             "direction)",
-            per_point_traffic("k_prune_scan1_tc_N1e6_D64.md", N) if Dp == 64 and one_pass else None)
+            per_point_traffic("k_prune_scan1_tc", N) if Dp == 64 and one_pass else None)
         add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
             "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP",
-            per_point_traffic("k_slot_stats_tc_N1e6_D64.md", N) if Dp == 64 else None)
+            per_point_traffic("k_slot_stats_tc", N) if Dp == 64 else None)
     else:
         add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
@@ -183,6 +175,8 @@ class ClockSampler:
         self.lines = []
 
     def __enter__(self):
+        if self.index < 0:
+            return self
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -262,11 +256,28 @@ def cpu_sample_payload(x_np, n, seed, K, D):
     return (x, mu, inv, logdet, w, u, mu_lr, inv_lr, ld_lr, lrw)
 
 
-def cpu_baseline(x_np, K, D, n=60000):
-    t = _cpu_sample_worker(cpu_sample_payload(x_np, n, 1, K, D))
-    return {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
+def cpu_baseline(K, D, n):
+    """The FP64 C restatement of the per-point phases (label, sub-label and statistics phases) on a
+    bounded sample of n points at the workload's K and D: timed on 1 thread, then on every host core
+    (one process per core, each on its own n-point sample)."""
+    import multiprocessing as mp
+    import numpy as np
+    rng = np.random.default_rng(0)
+    xs = (rng.normal(size=(n, D)) * 5).astype(np.float32)
+    t1 = _cpu_sample_worker(cpu_sample_payload(xs, n, 1, K, D))
+    cores = os.cpu_count() or 1
+    payloads = [cpu_sample_payload((rng.normal(size=(n, D)) * 5).astype(np.float32), n, 2 + i, K, D)
+                for i in range(cores)]
+    with mp.get_context("spawn").Pool(cores) as pool:
+        pool.map(_cpu_sample_worker, [cpu_sample_payload(xs[:64], 64, 1, K, D)] * cores)   # workers warm
+        t0 = time.perf_counter()
+        pool.map(_cpu_sample_worker, payloads)
+        tall = time.perf_counter() - t0
+    return {"value": cores * n / tall, "unit": UNIT, "cores": cores, "kind": "port",
+            "one_thread": {"value": n / t1, "cores": 1, "seconds": t1},
             "sample": f"{n} points x 1 iteration of the per-point phases (K={K}, D={D}) through the FP64 C "
-                      f"restatement (oracle/dpmm_oracle.c), 1 thread; {t:.1f} s"}
+                      f"restatement (oracle/dpmm_oracle.c) per process; {cores} processes on {cores} host "
+                      f"cores: {tall:.1f} s; 1 thread: {t1:.1f} s"}
 
 
 # ----------------------------------------------------------------------------- reference arm
@@ -310,103 +321,85 @@ def run_reference(args, rank, world):
 
 
 # ----------------------------------------------------------------------------- our arm
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--burnin", type=int, default=20)
-    ap.add_argument("--n", type=int, default=10_000_000)
-    ap.add_argument("--d", type=int, default=64)
-    ap.add_argument("--k-true", type=int, default=100)
-    ap.add_argument("--mode", default="auto", choices=["auto", "fp32", "tc"])
-    ap.add_argument("--host-draws", action="store_true",
-                    help="draw the cluster parameters on the host instead of the device")
-    ap.add_argument("--screen", default="on", choices=["on", "off"],
-                    help="learned split/merge screen (exact ratios for the top 16 candidates of each kind)")
-    ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--ref-points-per-core", type=int, default=600)
-    ap.add_argument("--profile-region", action="store_true",
-                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
-    ap.add_argument("--workload", default="c5", choices=["c5", "c4"],
-                    help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time")
-    ap.add_argument("--c4-sets", type=int, default=256)
-    ap.add_argument("--c4-seq-sets", type=int, default=32, help="data sets timed one at a time (a subset)")
-    args = ap.parse_args()
-    assert args.warmup >= 0 and args.steps >= 1
+# Sampler configurations ("arms") timed on the same data, seed and iteration counts.  "mixed" is the
+# product path; "plain" is the plain FP32 form the metric compares it with: the reference's algorithm
+# (dense label phase over all K clusters, per-cluster statistics, every split / merge candidate
+# evaluated exactly, parameters drawn on the host in FP64) with its per-point arithmetic in FP32 SIMT
+# kernels.  The ablation arms switch the mixed path's changes on one at a time.
+ARMS = {
+    "plain": dict(mode="fp32", prune=False, host_draws=True, screen=False,
+                  what="FP32 SIMT dense label phase, SIMT statistics, host FP64 parameter draws, every "
+                       "split / merge candidate exact"),
+    "plain+device_draws": dict(mode="fp32", prune=False, host_draws=False, screen=False,
+                               what="plain + NIW parameter draws on the device"),
+    "plain+device_draws+tensor_cores": dict(mode="tc", prune=False, host_draws=False, screen=False,
+                                            what="+ split-BF16 tcgen05 label / sub-label contractions and "
+                                                 "split-TF32 tcgen05 statistics (dense label phase)"),
+    "plain+device_draws+tensor_cores+pruning": dict(mode="tc", prune=True, host_draws=False, screen=False,
+                                                    what="+ pruned label phase (exact, 30-nat margin)"),
+    "mixed": dict(mode="auto", prune=True, host_draws=False, screen=True,
+                  what="+ learned split / merge screen (top 16 exact, full sweep every 10): the product path"),
+}
 
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference":
-        return run_reference(args, rank, world)
-    if args.workload == "c4":
-        return run_c4(args, rank, world, local)
 
+def make_run_desc(cfg, args, arm, iterations, rank, local, keep):
+    from dpmmsubclusters_gpu_b200 import capi
+    import numpy as np
+    a = ARMS[arm]
+    rd = capi.dpmm_run_desc()
+    rd.prior_type = capi.PRIOR_GAUSSIAN
+    rd.iterations = iterations
+    rd.initial_clusters = args.initial_clusters
+    rd.burnout = 15
+    rd.alpha = cfg["alpha"]
+    rd.seed = 12345 + rank
+    rd.loglik_mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[a["mode"]]
+    rd.rng_kind = capi.RNG_PHILOX
+    rd.k_max = 256
+    rd.device = local
+    m = np.zeros(cfg["D"])
+    psi = np.eye(cfg["D"])
+    keep += [m, psi]
+    rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
+    rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    rd.host_param_draws = int(a["host_draws"])
+    rd.label_prune_margin = 0.0 if a["prune"] else -1.0
+    if a["screen"]:
+        from dpmmsubclusters_gpu_b200.screen import load_params
+        sp = load_params()
+        keep.append(sp)
+        rd.screen_mode = capi.SCREEN_ON
+        rd.screen_params = sp.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+    return rd
+
+
+def run_arm(arm, args, cfg, x, z_np, rank, local, dist, L, clocks=False):
+    """Create a sampler of configuration `arm` on the device-resident points x, run the untimed burn-in
+    and warm-up iterations, then time exactly args.steps iterations with CUDA events on the sampler's
+    stream (barrier + device synchronisation on both sides, max over ranks).  Returns the arm's numbers,
+    the NMI of the final labels against the generating labels and the per-kernel timers."""
     import numpy as np
     import torch
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-
-    from dpmmsubclusters_gpu_b200 import capi
-    from dpmmsubclusters_gpu_b200.capi import check, lib
-    L = lib()
-    cfg = c5_config(args)
+    from dpmmsubclusters_gpu_b200.capi import check
     N, D = cfg["N"], cfg["D"]
-    x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
-    torch.cuda.synchronize()
-
-    mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[args.mode]
-    screen_params = None
-    if args.screen == "on":
-        from dpmmsubclusters_gpu_b200.screen import load_params
-        screen_params = load_params()
-
-    def make_run(iterations):
-        rd = capi.dpmm_run_desc()
-        rd.prior_type = capi.PRIOR_GAUSSIAN
-        rd.iterations = iterations
-        rd.initial_clusters = cfg["K_true"]
-        rd.burnout = 15
-        rd.alpha = cfg["alpha"]
-        rd.seed = 12345 + rank
-        rd.loglik_mode = mode
-        rd.rng_kind = capi.RNG_PHILOX
-        rd.k_max = 256
-        rd.device = local
-        m = np.zeros(D)
-        psi = np.eye(D)
-        rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
-        rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-        rd.host_param_draws = int(args.host_draws)
-        if screen_params is not None:
-            rd.screen_mode = capi.SCREEN_ON
-            rd.screen_params = screen_params.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
-        return rd, (m, psi, screen_params)
-
-    rd, keep = make_run(cfg["iterations"])
+    keep = []
+    rd = make_run_desc(cfg, args, arm, cfg["iterations"], rank, local, keep)
     h = ctypes.c_void_p()
     check(L.dpmm_sampler_create(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1, ctypes.byref(h)))
     ctx = L.dpmm_sampler_context(h)
     stream = torch.cuda.ExternalStream(L.dpmm_sampler_stream(h), device=f"cuda:{local}")
+    t0 = time.perf_counter()
     check(L.dpmm_sampler_step(h, args.burnin + args.warmup))
+    torch.cuda.synchronize()
+    burn_s = time.perf_counter() - t0
     k_before = ctypes.c_int32()
     check(L.dpmm_sampler_num_clusters(h, ctypes.byref(k_before)))
 
-    # ---- timed region
     check(L.dpmm_phase_times(ctx, 1, None, None))
     launches0 = L.dpmm_kernel_launch_count()
-    h2d0, d2h0 = ctypes.c_uint64(), ctypes.c_uint64()
-    L.dpmm_transfer_bytes(ctypes.byref(h2d0), ctypes.byref(d2h0))
     ks = []
-    with ClockSampler(local) as clk:
+    with ClockSampler(local if clocks else -1) as clk:
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -433,14 +426,10 @@ def main():
     check(L.dpmm_phase_times(ctx, 0, ph_ms, ph_calls))
     prune = (ctypes.c_double * 6)()
     check(L.dpmm_label_pruning_stats(ctx, prune))
-    h2d1, d2h1 = ctypes.c_uint64(), ctypes.c_uint64()
-    L.dpmm_transfer_bytes(ctypes.byref(h2d1), ctypes.byref(d2h1))
     if dist:
         t = torch.tensor([elapsed_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         elapsed_ms = float(t.item())
-
-    # quality of the state reached (NMI against the generating labels)
     mi = ctypes.c_void_p()
     check(L.dpmm_sampler_model_info(h, ctypes.byref(mi)))
     lab = np.ctypeslib.as_array(L.dpmm_model_info_labels(mi), shape=(N,)).copy()
@@ -448,51 +437,143 @@ def main():
     check(L.dpmm_model_info_screen_stats(mi, scr.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
     L.dpmm_model_info_free(mi)
     check(L.dpmm_sampler_destroy(h))
-    zt = z.cpu().numpy()
-    nmi = _nmi(lab[::10], zt[::10])
+    return {"arm": arm, "value": N * args.steps / (elapsed_ms / 1e3), "elapsed_ms": elapsed_ms,
+            "ms_per_step": elapsed_ms / args.steps, "ks": ks, "k_before": k_before.value,
+            "nmi": _nmi(lab[::10], z_np[::10]), "launches": int(launches), "ph_ms": list(ph_ms),
+            "ph_calls": list(ph_calls), "prune": list(prune), "screen": scr, "burnin_s": burn_s,
+            "clocks": clk.summary() if clocks else None}
 
-    value = world * N * args.steps / (elapsed_ms / 1e3)
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--burnin", type=int, default=130)
+    ap.add_argument("--initial-clusters", type=int, default=1,
+                    help="clusters the sampler starts from (the reference's default is 1)")
+    ap.add_argument("--n", type=int, default=10_000_000)
+    ap.add_argument("--d", type=int, default=64)
+    ap.add_argument("--k-true", type=int, default=100)
+    ap.add_argument("--arm", default="mixed", choices=sorted(ARMS),
+                    help="the configuration reported as `value` (default: the product path)")
+    ap.add_argument("--compare", default="plain", choices=sorted(ARMS) + ["none"],
+                    help="the arm timed beside it on the same data and iterations (vs_baseline = value / its value)")
+    ap.add_argument("--ablation", action="store_true",
+                    help="also time every intermediate arm (one change at a time) and report them")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--ref-points-per-core", type=int, default=600)
+    ap.add_argument("--cpu-points", type=int, default=20000,
+                    help="points of the CPU baseline sample (timed at 1 thread and at all threads)")
+    ap.add_argument("--profile-region", action="store_true",
+                    help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
+    ap.add_argument("--workload", default="c5", choices=["c5", "c4"],
+                    help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time")
+    ap.add_argument("--c4-sets", type=int, default=256)
+    ap.add_argument("--c4-seq-sets", type=int, default=32, help="data sets timed one at a time (a subset)")
+    args = ap.parse_args()
+    assert args.warmup >= 0 and args.steps >= 1
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    if args.workload == "c4":
+        return run_c4(args, rank, world, local)
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from dpmmsubclusters_gpu_b200.capi import lib
+    L = lib()
+    cfg = c5_config(args)
+    N, D = cfg["N"], cfg["D"]
+    x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
+    z_np = z.cpu().numpy()
+    torch.cuda.synchronize()
+
+    main_arm = run_arm(args.arm, args, cfg, x, z_np, rank, local, dist, L, clocks=True)
+    others = []
+    if args.ablation:
+        others = [a for a in ARMS if a != args.arm]
+    elif args.compare != "none" and args.compare != args.arm:
+        others = [args.compare]
+    other_res = {a: run_arm(a, args, cfg, x, z_np, rank, local, dist, L) for a in others}
+
+    r = main_arm
+    value = world * r["value"]
+    ph_ms, ph_calls, prune, ks = r["ph_ms"], r["ph_calls"], r["prune"], r["ks"]
     pk, pk_src = peaks()
-    k_mean = float(np.mean(ks)) if ks else float(k_before.value)
-    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src,
-                               padded(D) in (32, 64) and mode != capi.LL_FP32)
+    k_mean = float(np.mean(ks)) if ks else float(r["k_before"])
+    tc = padded(D) in (32, 64) and ARMS[args.arm]["mode"] != "fp32"
+    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src, tc)
     # the roofline of the kernel with the most device time in the timed region
     dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
     roofline = dict(kernels[dominant], kernel=dominant) if dominant else None
     phases = ["labels", "sub_labels_stats", "stats", "split_hastings", "merge_hastings", "relabel", "params",
               "label_tc_kernel", "label_prune_scan_kernel", "label_prune_draw_kernel", "slot_stats_kernel"]
+
+    def arm_summary(a):
+        return {"what": ARMS[a["arm"]]["what"], "value": world * a["value"], "unit": UNIT,
+                "ms_per_step": a["ms_per_step"], "nmi_vs_generating_labels": a["nmi"],
+                "clusters_in_timed_steps": a["ks"], "gpu_launches": a["launches"],
+                "phase_ms_per_step": {p: a["ph_ms"][i] / args.steps for i, p in enumerate(phases)
+                                      if a["ph_calls"][i]}}
+
+    cmp_arm = other_res.get(args.compare)
+    vs = value / (world * cmp_arm["value"]) if cmp_arm else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": elapsed_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+bf16x3" if mode != capi.LL_FP32 else "f32",
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": vs,
+            "dtype": "f32+bf16x3" if ARMS[args.arm]["mode"] != "fp32" else "f32",
             "data": "synthetic (seeded draws of the configuration's generative model, generated on device)",
             "config": {"workload": "C5 Gaussian DPMM N=1e7 D=64 100 true clusters (means N(0,25I), "
                                    "cov AA^T/D+0.5I, Dir(2) weights, f32); NIW k=1 m=0 nu=67 Psi=I; alpha=10",
-                       "N": N, "D": D, "initial_clusters": cfg["K_true"], "burnin_iterations": args.burnin,
-                       "clusters_in_timed_steps": ks, "loglik_mode": args.mode,
+                       "N": N, "D": D, "arm": args.arm, "arm_what": ARMS[args.arm]["what"],
+                       "initial_clusters": args.initial_clusters,
+                       "initial_clusters_note": ("head start: the sampler starts from as many clusters as the "
+                                                 "generating model has (the reference's default is 1)"
+                                                 if args.initial_clusters > 1 else "the reference's default"),
+                       "burnin_iterations": args.burnin,
+                       "clusters_in_timed_steps": ks,
                        "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
-                       "nmi_vs_generating_labels": nmi,
-                       "parameter_draws": "host" if args.host_draws else "device",
-                       "label_pruning": {"attempts": int(prune[0]), "pruned_phases": int(prune[1]),
+                       "nmi_vs_generating_labels": r["nmi"],
+                       "parameter_draws": "host" if ARMS[args.arm]["host_draws"] else "device",
+                       "label_pruning": {"enabled": ARMS[args.arm]["prune"], "attempts": int(prune[0]),
+                                         "pruned_phases": int(prune[1]),
                                          "kept_other_clusters_per_point": prune[2], "margin_nats": prune[3],
                                          "last_attempt_kept_per_point": prune[4],
                                          "last_attempt_chunks_over_capacity": int(prune[5])},
-                       "screen": screen_summary(args.screen, scr)},
-            "gpu_launches": int(launches),
+                       "screen": screen_summary("on" if ARMS[args.arm]["screen"] else "off", r["screen"]),
+                       "vs_baseline": (f"value / the '{args.compare}' arm's value, both timed in this run on the "
+                                       "same data, seed, burn-in and timed iterations" if cmp_arm else None)},
+            "gpu_launches": r["launches"],
             "roofline": roofline,
             "kernel_rooflines": kernels,
             "phase_ms_per_step": {p: ph_ms[i] / args.steps for i, p in enumerate(phases) if ph_calls[i]},
-            "clocks": clk.summary()}
+            "clocks": r["clocks"]}
+    if cmp_arm:
+        line["compare"] = dict(arm_summary(cmp_arm), arm=args.compare,
+                               nmi_delta=r["nmi"] - cmp_arm["nmi"], speedup=vs)
+    if args.ablation:
+        line["ablation"] = {a: arm_summary(v) for a, v in list(other_res.items()) + [(args.arm, r)]}
     line["clocks"].pop("samples", None)
     del x
     torch.cuda.empty_cache()
 
     if rank == 0 and not args.no_cpu:
-        import numpy as np2
-        rng = np2.random.default_rng(0)
-        xs = (rng.normal(size=(60000, D)) * 5).astype(np2.float32)
-        line["cpu_baseline"] = cpu_baseline(xs, cfg["K_true"], D)
+        line["cpu_baseline"] = cpu_baseline(cfg["K_true"], D, args.cpu_points)
     if not args.no_e2e:
-        line["e2e"] = run_e2e(args, cfg, rank, local, world, dist, L, make_run)
+        line["e2e"] = run_e2e(args, cfg, rank, local, world, dist, L)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -501,7 +582,7 @@ def main():
     return 0
 
 
-def run_e2e(args, cfg, rank, local, world, dist, L, make_run):
+def run_e2e(args, cfg, rank, local, world, dist, L):
     """The same metric through the public whole-sampler call (dpmm_dp_parallel) from HOST buffers:
     point upload, initialisation, burn-in + warm-up + timed iterations and the label download
     are all inside the timed region (wall clock, max over ranks)."""
@@ -513,7 +594,8 @@ def run_e2e(args, cfg, rank, local, world, dist, L, make_run):
     del x
     torch.cuda.empty_cache()
     iters = args.burnin + args.warmup + args.steps
-    rd, keep = make_run(iters)
+    keep = []
+    rd = make_run_desc(cfg, args, args.arm, iters, rank, local, keep)
     h2d0, d2h0 = ctypes.c_uint64(), ctypes.c_uint64()
     L.dpmm_transfer_bytes(ctypes.byref(h2d0), ctypes.byref(d2h0))
     if dist:

@@ -306,6 +306,13 @@ class CudaKernel:
         u = self._u(uniforms, self.N)
         check(lib().dpmm_sample_sub_labels(self.ctx, _fptr(u)))
 
+    def draw_uniforms(self):
+        """The (N, 2) uniforms the next label / sub-label draw would take from the context's generator;
+        the generator advances as that draw would (dpmm_draw_uniforms)."""
+        u = np.empty(2 * self.N, np.float32)
+        check(lib().dpmm_draw_uniforms(self.ctx, _fptr(u)))
+        return u.reshape(self.N, 2)
+
     def set_labels(self, labels):
         a = np.ascontiguousarray(labels, np.int32)
         check(lib().dpmm_set_labels(self.ctx, _iptr(a)))

@@ -70,6 +70,7 @@ SIGNATURES = {
     "dpmm_upload_points_f32": (c_int, [_CTX, _PF]),
     "dpmm_sample_labels": (c_int, [_CTX, c_int, c_double, _PF]),
     "dpmm_sample_sub_labels": (c_int, [_CTX, _PF]),
+    "dpmm_draw_uniforms": (c_int, [_CTX, _PF]),
     "dpmm_set_labels": (c_int, [_CTX, _PI32]),
     "dpmm_set_sub_labels": (c_int, [_CTX, _PI32]),
     "dpmm_get_labels": (c_int, [_CTX, _PI32]),

@@ -487,6 +487,16 @@ extern "C" dpmm_status dpmm_sample_labels(dpmm_ctx* c, int initial_clusters, dou
     return DPMM_OK;
 }
 
+extern "C" dpmm_status dpmm_draw_uniforms(dpmm_ctx* c, float* u)
+{
+    if (!c || !u) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    DPMM_TRY(launch_draw_uniforms(c, c->d_u));
+    DPMM_CUDA_TRY(cudaMemcpyAsync(u, c->d_u, sizeof(float) * 2 * c->N, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    g_d2h_bytes += sizeof(float) * 2 * c->N;
+    return DPMM_OK;
+}
+
 extern "C" dpmm_status dpmm_sample_sub_labels(dpmm_ctx* c, const float* u)
 {
     if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");

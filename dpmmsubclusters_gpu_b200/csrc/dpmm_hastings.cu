@@ -191,29 +191,63 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_static_merge_hr(const double
 
 }  // namespace dpmm
 
+#include <cuda.h>   // CUcontext / CUresult types only: the two driver calls are fetched through the runtime
+
 #include <mutex>
 
-// Device address of g_merge_scratch, looked up once per device (with that device current) on the
-// first call made on it.
+// Identity of the calling thread's current CUDA context: cuCtxGetId's process-unique id (0 when no
+// context is current yet).  The driver functions come from cudaGetDriverEntryPoint, so the library
+// does not link libcuda itself.
+static dpmm_status current_context_id(unsigned long long* id)
+{
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, nullptr) == cudaSuccess)
+            get_current = (GetCurrent)f;
+        f = nullptr;
+        if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, nullptr) == cudaSuccess) get_id = (GetId)f;
+    });
+    if (!get_current || !get_id) return dpmm::fail(DPMM_ERR_CUDA, "cuCtxGetCurrent / cuCtxGetId unavailable");
+    CUcontext ctx = nullptr;
+    *id = 0;
+    if (get_current(&ctx) != CUDA_SUCCESS) return dpmm::fail(DPMM_ERR_CUDA, "cuCtxGetCurrent failed");
+    if (ctx && get_id(ctx, id) != CUDA_SUCCESS) return dpmm::fail(DPMM_ERR_CUDA, "cuCtxGetId failed");
+    return DPMM_OK;
+}
+
+// Device address of g_merge_scratch in the calling thread's current context.  It is looked up (with
+// that context current) on the first call made in a context and cached per device together with the
+// context's id: when the context changes -- cudaDeviceReset, or a context the caller made current --
+// the module is loaded anew there and the address is looked up again, so a stale address is never used.
 static double* static_scratch_for_current_device(dpmm_status* st)
 {
     static std::mutex mu;
     static double* ptr[128] = {nullptr};
+    static unsigned long long ctx_of[128] = {0};
     int dev = -1;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess || dev < 0 || dev >= 128) {
         *st = e != cudaSuccess ? dpmm::cuda_status(e, "cudaGetDevice") : dpmm::fail(DPMM_ERR_NO_DEVICE, "device ordinal");
         return nullptr;
     }
+    unsigned long long id = 0;
+    if ((*st = current_context_id(&id)) != DPMM_OK) return nullptr;
     std::lock_guard<std::mutex> lock(mu);
-    if (!ptr[dev]) {
+    if (!ptr[dev] || id == 0 || id != ctx_of[dev]) {
         double* p = nullptr;
-        e = cudaGetSymbolAddress((void**)&p, dpmm::g_merge_scratch);
+        e = cudaGetSymbolAddress((void**)&p, dpmm::g_merge_scratch);   // makes the device's context current
         if (e != cudaSuccess || !p) {
             *st = dpmm::cuda_status(e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(g_merge_scratch)");
             return nullptr;
         }
+        if (id == 0 && (*st = current_context_id(&id)) != DPMM_OK) return nullptr;
         ptr[dev] = p;
+        ctx_of[dev] = id;
     }
     *st = DPMM_OK;
     return ptr[dev];

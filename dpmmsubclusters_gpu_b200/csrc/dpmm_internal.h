@@ -290,6 +290,7 @@ dpmm_status make_label_job(dpmm_ctx* c, int K, int final_, LabelJob* job);
 dpmm_status launch_init_curand(dpmm_ctx* c);
 dpmm_status launch_labels_init(dpmm_ctx* c, int initial_clusters, double outlier_mod, const float* d_u);
 dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u);
+dpmm_status launch_draw_uniforms(dpmm_ctx* c, float* d_u);   // 2N uniforms of the next draw
 dpmm_status launch_cluster_labels(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 // the pruned label phase; *used = false when it declined (the caller then runs the dense phase)
 dpmm_status launch_cluster_labels_pruned(dpmm_ctx* c, int K, int final_, const float* d_u, bool* used);

@@ -79,6 +79,25 @@ dpmm_status launch_sub_labels_init(dpmm_ctx* c, const float* d_u)
     return DPMM_OK;
 }
 
+// the two uniforms per point of the next draw, written out (d_u: 2N), advancing the generator
+__global__ void k_draw_uniform2(RngArgs r, int64_t n, float* d_u)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float u1, u2;
+    draw_uniform2(r, i, u1, u2);
+    d_u[2 * i] = u1;
+    d_u[2 * i + 1] = u2;
+}
+
+dpmm_status launch_draw_uniforms(dpmm_ctx* c, float* d_u)
+{
+    RngArgs r = rng_args(c, nullptr);
+    k_draw_uniform2<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(r, c->N, d_u);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
 // ----------------------------------------------------------------------------- label phase
 // Shared epilogue: r values of one point (stride P in shared memory) -> label.
 template <int P>

@@ -114,6 +114,12 @@ dpmm_status dpmm_sample_labels(dpmm_ctx* ctx, int initial_clusters, double outli
                                const float* uniforms /* N or NULL */);
 /* cudaKernel::sample_sub_labels (cudaKernel.cu:1093-1101) */
 dpmm_status dpmm_sample_sub_labels(dpmm_ctx* ctx, const float* uniforms /* N or NULL */);
+/* The two uniforms per point that the next label or sub-label draw would take from the
+ * context's generator (the pair of curand_uniform() calls of cudaKernel.cu:115-116 in
+ * cuRAND-compatible mode), written to uniforms[2N]; the generator advances as that draw
+ * would.  Lets a caller replay the reference's random stream through the caller-uniform
+ * paths. */
+dpmm_status dpmm_draw_uniforms(dpmm_ctx* ctx, float* uniforms /* 2N */);
 
 /* cudaKernel::update_labels (cudaKernel.cu:1145-1148); the set_labels / set_sub_labels
  * seams of the reference's test double (test/myCudaKernel.h). */
@@ -237,8 +243,11 @@ dpmm_status dpmm_merge_hastings(dpmm_ctx* ctx, int K, double alpha, double* merg
  * the work is queued on `stream` (a cudaStream_t; NULL = the default stream) without waiting for it.
  * The kernels' scratch is a file-scope device array for at most 1024 clusters (K > 1024 is rejected
  * with DPMM_ERR_INVALID_ARG); every device that loads the library holds it (8 KB) until exit.  The
- * first call on a device looks up the array's device address, so make that first call before any
- * stream capture.  All calls on a device share the array: calls that overlap on the GPU race.
+ * first call in a context (on a device, and again after cudaDeviceReset or when another context is
+ * made current) looks up the array's device address, so make that first call before any stream
+ * capture.  All calls on a device share the array: calls that overlap on the GPU race.
+ * A NaN entry means an empty cluster, or a psi that is not positive definite (its log determinant,
+ * and so every ratio, is NaN); dpmm_create / dpmm_set_prior reject such a psi with DPMM_ERR_NOT_PD.
  * It calls no cudaMalloc, cudaFree or other allocating routine. */
 dpmm_status dpmm_merge_hastings_static(int32_t prior_type, int32_t D, int32_t K, double alpha, double k0, double v0,
                                        const double* prior, const double* stats, double* merge_log_hr,

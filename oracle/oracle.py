@@ -21,6 +21,18 @@ REF_LIB_PATH = os.path.join(HERE, "_ref", "libdpmm_ref_host.so")
 _lib = None
 _ref = None
 
+
+def reference_dir():
+    """The reference's DPMMSubClusters/ source directory: $DPMM_REFERENCE_DIR, else a `reference/`
+    checkout beside this repository; None when neither exists (e.g. on a machine that only runs the
+    prebuilt checkers in _ref/)."""
+    cands = [os.environ.get("DPMM_REFERENCE_DIR"),
+             os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "DPMMSubClusters")]
+    for c in cands:
+        if c and os.path.isdir(c):
+            return os.path.abspath(c)
+    return None
+
 _pd = POINTER(c_double)
 _pi32 = POINTER(ctypes.c_int32)
 _pi64 = POINTER(c_int64)

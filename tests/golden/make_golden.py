@@ -26,7 +26,10 @@ import os
 import re
 import sys
 
-DEFAULT_REF = "/root/reference/DPMMSubClusters"
+# the reference checkout: argv[1], else $DPMM_REFERENCE_DIR, else `reference/` beside this repository
+DEFAULT_REF = os.environ.get("DPMM_REFERENCE_DIR") or os.path.join(
+    os.path.dirname(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))),
+    "reference", "DPMMSubClusters")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "reference_goldens.json")
 
 WANTED = {

@@ -107,8 +107,9 @@ def test_python_api_layout_checks():
 
 def test_golden_fixture_regenerates(tmp_path):
     """The committed golden fixture is what make_golden.py extracts from the reference's tests."""
-    ref = "/root/reference/DPMMSubClusters"
-    if not os.path.isdir(ref):
+    from oracle.oracle import reference_dir
+    ref = reference_dir()
+    if ref is None:
         pytest.skip("reference sources not mounted")
     import subprocess
     import sys

@@ -8,7 +8,9 @@ import ctypes
 import numpy as np
 import pytest
 
+import parity as P
 from conftest import uniforms
+from oracle import oracle as O
 from dpmmsubclusters_gpu_b200 import RNG_CURAND_XORWOW, CudaKernel, LL_FP32, prior_type
 from dpmmsubclusters_gpu_b200.capi import check, lib
 
@@ -59,6 +61,17 @@ def test_pruned_labels_equal_dense_labels(D, mode):
     assert st[1] == 2, st          # both pruned phases ran pruned
     for final in (False, True):
         np.testing.assert_array_equal(res[(30.0, final)], res[(0.0, final)])
+    # and against the oracle's draw on FP64 log-likelihoods (margin rule of tests/parity.py) on a sample
+    sel = np.arange(0, N, 5)
+    r64 = np.stack([O.gauss_loglik(x[sel], mu[k], inv[k], ld[k], w[k]) for k in range(K)], 1)
+    kern.set_labels((z + 1).astype(np.int32))
+    r = kern.create_clusters_labels(K, False, u, return_loglik=True)
+    path = "fp32" if mode == LL_FP32 or D < 32 else "tc"
+    row_err = P.gauss_ll(r[sel], r64, D, ld, np.log(w), path, f"prune_dense_{path}_D{D}")
+    u2 = u.reshape(N, 2).astype(np.float64)
+    P.labels_vs_fp64(res[(30.0, False)][sel], r64, u2[sel], row_err, f"prune_{path}_D{D}_vs_fp64")
+    P.labels_vs_fp64(res[(30.0, True)][sel], r64, u2[sel], row_err, f"prune_argmax_{path}_D{D}_vs_fp64",
+                     final=True)
 
 
 def test_unprunable_state_falls_back_to_dense():

@@ -98,3 +98,77 @@ def test_static_merge_hastings_rejects_oversize():
     p = ctypes.c_void_p(buf.data_ptr())
     st = lib().dpmm_merge_hastings_static(0, 4, 1025, 1.0, 1.0, 7.0, p, p, p, None)
     assert st == 1 and b"1024" in lib().dpmm_last_error()
+
+
+_RESET_CHILD = r"""
+import ctypes, sys
+import numpy as np
+sys.path.insert(0, sys.argv[1])
+from dpmmsubclusters_gpu_b200 import lib
+L = lib()                                   # loads libcudart.so.12 through the library's runpath
+rt = ctypes.CDLL("libcudart.so.12")         # the same (already loaded) runtime instance
+drv = ctypes.CDLL("libcuda.so.1")
+K, D = 3, 4
+rng = np.random.default_rng(5)
+prior = np.concatenate([np.zeros(D), np.eye(D).reshape(-1)])
+slots = []
+for k in range(K):
+    for s in range(3):
+        x = rng.normal(size=(40 + 10 * k + s, D)) + 2.0 * k
+        slots.append(np.concatenate([[x.shape[0]], x.sum(0), (x.T @ x).T.reshape(-1)]))
+stats = np.concatenate(slots)
+
+def dev(a):
+    p = ctypes.c_void_p()
+    assert rt.cudaMalloc(ctypes.byref(p), ctypes.c_size_t(a.nbytes)) == 0
+    assert rt.cudaMemcpy(p, a.ctypes.data_as(ctypes.c_void_p), ctypes.c_size_t(a.nbytes), 1) == 0
+    return p
+
+def ctx_id():
+    c = ctypes.c_void_p()
+    i = ctypes.c_ulonglong()
+    assert drv.cuCtxGetCurrent(ctypes.byref(c)) == 0 and c.value
+    assert drv.cuCtxGetId(c, ctypes.byref(i)) == 0
+    return i.value
+
+def call():
+    out = np.zeros(K * K)
+    dp, ds, do = dev(prior), dev(stats), dev(out)
+    st = L.dpmm_merge_hastings_static(0, D, K, 2.0, 1.0, D + 3.0, dp, ds, do, None)
+    assert st == 0, L.dpmm_last_error()
+    assert rt.cudaDeviceSynchronize() == 0
+    assert rt.cudaMemcpy(out.ctypes.data_as(ctypes.c_void_p), do, ctypes.c_size_t(out.nbytes), 2) == 0
+    for p in (dp, ds, do):
+        rt.cudaFree(p)
+    return out
+
+a = call()
+id1 = ctx_id()
+assert rt.cudaDeviceReset() == 0
+z = ctypes.c_void_p()
+assert rt.cudaMalloc(ctypes.byref(z), ctypes.c_size_t(256)) == 0    # a new context after the reset
+rt.cudaFree(z)
+if ctx_id() == id1:
+    print("SAME_CONTEXT_ID")
+    sys.exit(0)
+b = call()
+assert np.array_equal(np.isnan(a), np.isnan(b)) and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)])
+assert np.isfinite(a).sum() == K * (K - 1) // 2
+print("OK")
+"""
+
+
+def test_static_merge_hastings_after_device_reset():
+    """After cudaDeviceReset the library's module is loaded anew in a new context: the entry point
+    must look the scratch array's address up again (it keys its cache on the context's id) and give
+    the same ratios.  Runs in a child process without torch, since the reset ends the process's
+    CUDA state."""
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", _RESET_CHILD, root], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout + out.stderr
+    if "SAME_CONTEXT_ID" in out.stdout:
+        pytest.skip("the driver kept the context id across cudaDeviceReset")
+    assert "OK" in out.stdout, out.stdout + out.stderr
