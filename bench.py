@@ -19,9 +19,11 @@ dense FP32 SIMT label phase, SIMT statistics, host parameter draws, every candid
 same data, seed and iteration counts in the same invocation: vs_baseline = value / plain's value, and
 both NMIs against the generating labels are reported.  --ablation adds the intermediate arms.
 
---gpus N (under torchrun) runs N independent replicas, one per GPU, each on its own data set of
-the same shape (weak scaling; the path has no cross-GPU exchange in this form); value sums all
-ranks' points x iterations over the max elapsed time.
+--gpus N (under torchrun): by default one data set of N x 1e7 points (one generative model, each rank
+drawing its own 1e7 points) sharded by points over the ranks: per-point phases on each rank, the
+per-cluster statistics summed over the ranks with NCCL after each statistics phase, every host
+decision replicated (weak scaling; value = all ranks' points x iterations over the max elapsed time).
+--multi-gpu replicas runs N independent samplers instead.
 
 --impl reference times the reference's per-point path on the host cores: the reference has no CPU
 implementation of these phases (every one dispatches to its CUDA back-end), so its FP64
@@ -143,26 +145,33 @@ def c5_config(args):
                 mean_sd=5.0, dirichlet=2.0)
 
 
-def generate_c5_torch(cfg, seed, device):
+def generate_c5_torch(cfg, seed, device, point_seed=None):
+    """Seeded draws of the configuration's generative model on the device: the model (weights, means,
+    covariances) from `seed`, the points (and their generating labels) from `point_seed` (default: the
+    same seed), so shards of one data set share the model and differ in their points."""
     import torch
     torch.manual_seed(seed)
     g = torch.Generator(device=device)
     g.manual_seed(seed)
     N, D, K = cfg["N"], cfg["D"], cfg["K_true"]
     w = torch.distributions.Dirichlet(torch.full((K,), cfg["dirichlet"])).sample()
-    z = torch.multinomial(w.to(device), N, replacement=True, generator=g)
     mus = torch.randn(K, D, device=device, generator=g) * cfg["mean_sd"]
+    Ls = []
+    for k in range(K):
+        A = torch.randn(D, D, device=device, generator=g, dtype=torch.float64)
+        cov = A @ A.T / D + 0.5 * torch.eye(D, device=device, dtype=torch.float64)
+        Ls.append(torch.linalg.cholesky(cov).float())
+    if point_seed is not None:
+        g.manual_seed(point_seed)
+    z = torch.multinomial(w.to(device), N, replacement=True, generator=g)
     x = torch.empty(N, D, device=device, dtype=torch.float32)
     order = torch.argsort(z)
     counts = torch.bincount(z, minlength=K).tolist()
     start = 0
     for k in range(K):
         n = counts[k]
-        A = torch.randn(D, D, device=device, generator=g, dtype=torch.float64)
-        cov = A @ A.T / D + 0.5 * torch.eye(D, device=device, dtype=torch.float64)
-        L = torch.linalg.cholesky(cov).float()
         e = torch.randn(n, D, device=device, generator=g)
-        x[order[start:start + n]] = e @ L.T + mus[k]
+        x[order[start:start + n]] = e @ Ls[k].T + mus[k]
         start += n
     return x.contiguous(), z
 
@@ -352,7 +361,7 @@ def make_run_desc(cfg, args, arm, iterations, rank, local, keep):
     rd.initial_clusters = args.initial_clusters
     rd.burnout = 15
     rd.alpha = cfg["alpha"]
-    rd.seed = 12345 + rank
+    rd.seed = 12345 + (0 if args.multi_gpu == "shard" else rank)   # shards of one run share the seed
     rd.loglik_mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[a["mode"]]
     rd.rng_kind = capi.RNG_PHILOX
     rd.k_max = 256
@@ -374,7 +383,7 @@ def make_run_desc(cfg, args, arm, iterations, rank, local, keep):
     return rd
 
 
-def run_arm(arm, args, cfg, x, z_np, rank, local, dist, L, clocks=False):
+def run_arm(arm, args, cfg, x, z_np, rank, local, dist, L, clocks=False, shard=None):
     """Create a sampler of configuration `arm` on the device-resident points x, run the untimed burn-in
     and warm-up iterations, then time exactly args.steps iterations with CUDA events on the sampler's
     stream (barrier + device synchronisation on both sides, max over ranks).  Returns the arm's numbers,
@@ -386,7 +395,17 @@ def run_arm(arm, args, cfg, x, z_np, rank, local, dist, L, clocks=False):
     keep = []
     rd = make_run_desc(cfg, args, arm, cfg["iterations"], rank, local, keep)
     h = ctypes.c_void_p()
-    check(L.dpmm_sampler_create(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1, ctypes.byref(h)))
+    if shard is not None:
+        # one shard of a data set of world x N points: statistics summed over the ranks (NCCL)
+        from dpmmsubclusters_gpu_b200 import capi
+        sh = capi.dpmm_shard()
+        sh.rank, sh.world, sh.point_offset, sh.n_total = rank, args.gpus_world, rank * N, args.gpus_world * N
+        sh.allreduce = shard.callback
+        keep.append(sh)
+        check(L.dpmm_sampler_create_sharded(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1,
+                                            ctypes.byref(sh), ctypes.byref(h)))
+    else:
+        check(L.dpmm_sampler_create(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1, ctypes.byref(h)))
     ctx = L.dpmm_sampler_context(h)
     stream = torch.cuda.ExternalStream(L.dpmm_sampler_stream(h), device=f"cuda:{local}")
     t0 = time.perf_counter()
@@ -460,6 +479,9 @@ def main():
                     help="the configuration reported as `value` (default: the product path)")
     ap.add_argument("--compare", default="plain", choices=sorted(ARMS) + ["none"],
                     help="the arm timed beside it on the same data and iterations (vs_baseline = value / its value)")
+    ap.add_argument("--multi-gpu", default="shard", choices=["shard", "replicas"],
+                    help="with N > 1 ranks: shard one data set of N x n points by points over the ranks, summing "
+                         "the per-cluster statistics with NCCL (default), or run N independent replicas")
     ap.add_argument("--ablation", action="store_true",
                     help="also time every intermediate arm (one change at a time) and report them")
     ap.add_argument("--no-e2e", action="store_true")
@@ -469,8 +491,11 @@ def main():
                     help="points of the CPU baseline sample (timed at 1 thread and at all threads)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
-    ap.add_argument("--workload", default="c5", choices=["c5", "c4"],
-                    help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time")
+    ap.add_argument("--workload", default="c5", choices=["c5", "c4", "study"],
+                    help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time; study: "
+                         "NMI and final cluster count over 10 sampler seeds, mixed vs plain FP32")
+    ap.add_argument("--study-seeds", type=int, default=10)
+    ap.add_argument("--study-shapes", default="c5r,c2", help="comma list of c5r (C5 at N=1e6) and c2")
     ap.add_argument("--c4-sets", type=int, default=256)
     ap.add_argument("--c4-seq-sets", type=int, default=32, help="data sets timed one at a time (a subset)")
     args = ap.parse_args()
@@ -483,6 +508,8 @@ def main():
         return run_reference(args, rank, world)
     if args.workload == "c4":
         return run_c4(args, rank, world, local)
+    if args.workload == "study":
+        return run_study(args, rank, local)
 
     import numpy as np
     import torch
@@ -497,17 +524,25 @@ def main():
     L = lib()
     cfg = c5_config(args)
     N, D = cfg["N"], cfg["D"]
-    x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
+    args.gpus_world = world
+    sharded = world > 1 and args.multi_gpu == "shard"
+    shard = None
+    if sharded:
+        from dpmmsubclusters_gpu_b200.shard import TorchDistributedExchange
+        shard = TorchDistributedExchange(device=True)
+        x, z = generate_c5_torch(cfg, 1000 + 5, f"cuda:{local}", point_seed=7000 + rank)
+    else:
+        x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
     z_np = z.cpu().numpy()
     torch.cuda.synchronize()
 
-    main_arm = run_arm(args.arm, args, cfg, x, z_np, rank, local, dist, L, clocks=True)
+    main_arm = run_arm(args.arm, args, cfg, x, z_np, rank, local, dist, L, clocks=True, shard=shard)
     others = []
     if args.ablation:
         others = [a for a in ARMS if a != args.arm]
     elif args.compare != "none" and args.compare != args.arm:
         others = [args.compare]
-    other_res = {a: run_arm(a, args, cfg, x, z_np, rank, local, dist, L) for a in others}
+    other_res = {a: run_arm(a, args, cfg, x, z_np, rank, local, dist, L, shard=shard) for a in others}
 
     r = main_arm
     value = world * r["value"]
@@ -539,6 +574,9 @@ def main():
             "config": {"workload": "C5 Gaussian DPMM N=1e7 D=64 100 true clusters (means N(0,25I), "
                                    "cov AA^T/D+0.5I, Dir(2) weights, f32); NIW k=1 m=0 nu=67 Psi=I; alpha=10",
                        "N": N, "D": D, "arm": args.arm, "arm_what": ARMS[args.arm]["what"],
+                       "multi_gpu": ("one data set of %d x N points sharded by points, statistics summed with "
+                                     "NCCL (weak scaling)" % world if sharded else
+                                     "independent replicas" if world > 1 else "one GPU"),
                        "initial_clusters": args.initial_clusters,
                        "initial_clusters_note": ("head start: the sampler starts from as many clusters as the "
                                                  "generating model has (the reference's default is 1)"
@@ -642,6 +680,100 @@ def c4_data(n_sets, seed):
             x[idx] = mus[c] + rng.normal(size=(idx.size, D)) @ L.T
         out.append((x.astype(np.float32).astype(np.float64).T.copy(), z))
     return out
+
+
+def generate_c2_torch(seed, device, N=1_000_000, D=32, K=20):
+    """Seeded draws of the C2 shape: means U(-20, 20)^D, covariances A A^T / D + 0.5 I, Dirichlet(1) weights."""
+    import torch
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    torch.manual_seed(seed)
+    w = torch.distributions.Dirichlet(torch.ones(K)).sample()
+    mus = (torch.rand(K, D, device=device, generator=g) * 40 - 20)
+    z = torch.multinomial(w.to(device), N, replacement=True, generator=g)
+    x = torch.empty(N, D, device=device, dtype=torch.float32)
+    for k in range(K):
+        idx = torch.nonzero(z == k).flatten()
+        A = torch.randn(D, D, device=device, generator=g, dtype=torch.float64)
+        L = torch.linalg.cholesky(A @ A.T / D + 0.5 * torch.eye(D, device=device, dtype=torch.float64)).float()
+        x[idx] = torch.randn(idx.numel(), D, device=device, generator=g) @ L.T + mus[k]
+    return x.contiguous(), z
+
+
+def run_study(args, rank, local):
+    """End-to-end quality of the product path against the plain FP32 form: for each shape, one seeded
+    synthetic data set and sampler seeds 0 .. S-1, both arms run the full iteration count from one
+    initial cluster; reported per seed: NMI against the generating labels, final cluster count and
+    seconds; and the means, spreads and the largest |NMI difference| over the seeds."""
+    import numpy as np
+    import torch
+    if rank != 0:
+        return 0
+    torch.cuda.set_device(local)
+    from dpmmsubclusters_gpu_b200.capi import check, lib
+    L = lib()
+    shapes = {
+        "c5r": dict(desc="C5 shape at N=1e6: D=64, 100 true clusters, means N(0,25I), cov AA^T/D+0.5I, Dir(2) "
+                         "weights; NIW k=1 m=0 nu=67 Psi=I; alpha=10; 150 iterations, burnout 15",
+                    iters=150, burnout=15, alpha=10.0),
+        "c2": dict(desc="C2 shape: N=1e6, D=32, 20 true clusters, means U(-20,20)^D, cov AA^T/D+0.5I, Dir(1) "
+                        "weights; NIW k=1 m=0 nu=35 Psi=I; alpha=10; 200 iterations, burnout 20",
+                   iters=200, burnout=20, alpha=10.0),
+    }
+    out = {"metric": "end-to-end NMI and final cluster count over sampler seeds: mixed+learned vs plain FP32",
+           "unit": "NMI", "data": "synthetic (seeded draws of each shape's generative model, on device)",
+           "impl": "ours", "shapes": {}}
+    for name in args.study_shapes.split(","):
+        sh = shapes[name]
+        if name == "c5r":
+            cfg = dict(N=1_000_000, D=64, K_true=100, alpha=10.0, nu=67.0, kappa=1.0, iterations=sh["iters"],
+                       mean_sd=5.0, dirichlet=2.0)
+            x, z = generate_c5_torch(cfg, 1105, f"cuda:{local}")
+        else:
+            cfg = dict(N=1_000_000, D=32, K_true=20, alpha=10.0, nu=35.0, kappa=1.0, iterations=sh["iters"])
+            x, z = generate_c2_torch(1102, f"cuda:{local}")
+        z_np = z.cpu().numpy()
+        res = {}
+        for arm in ("mixed", "plain"):
+            rows = []
+            for seed in range(args.study_seeds):
+                keep = []
+                a = argparse.Namespace(initial_clusters=1, multi_gpu="replicas")
+                rd = make_run_desc(cfg, a, arm, sh["iters"], 0, local, keep)
+                rd.seed = seed + 1          # seed 0 would mean "time based"
+                rd.burnout = sh["burnout"]
+                rd.alpha = sh["alpha"]
+                h = ctypes.c_void_p()
+                torch.cuda.synchronize()
+                t0 = time.perf_counter()
+                check(L.dpmm_sampler_create(ctypes.byref(rd), cfg["N"], cfg["D"], ctypes.c_void_p(x.data_ptr()), 1,
+                                            ctypes.byref(h)))
+                check(L.dpmm_sampler_step(h, sh["iters"]))
+                kk = ctypes.c_int32()
+                check(L.dpmm_sampler_num_clusters(h, ctypes.byref(kk)))
+                mi = ctypes.c_void_p()
+                check(L.dpmm_sampler_model_info(h, ctypes.byref(mi)))
+                lab = np.ctypeslib.as_array(L.dpmm_model_info_labels(mi), shape=(cfg["N"],)).copy()
+                L.dpmm_model_info_free(mi)
+                check(L.dpmm_sampler_destroy(h))
+                torch.cuda.synchronize()
+                dt = time.perf_counter() - t0
+                rows.append({"seed": seed + 1, "nmi": _nmi(lab, z_np), "final_k": kk.value, "seconds": dt})
+            nm = np.array([r["nmi"] for r in rows])
+            ks = np.array([r["final_k"] for r in rows])
+            res[arm] = {"runs": rows, "nmi_mean": float(nm.mean()), "nmi_std": float(nm.std()),
+                        "final_k_mean": float(ks.mean()), "final_k_std": float(ks.std()),
+                        "final_k_values": sorted(int(k) for k in ks),
+                        "seconds_mean": float(np.mean([r["seconds"] for r in rows]))}
+        dn = [abs(a["nmi"] - b["nmi"]) for a, b in zip(res["mixed"]["runs"], res["plain"]["runs"])]
+        out["shapes"][name] = {"workload": sh["desc"], "true_clusters": cfg["K_true"], "arms": res,
+                               "nmi_mean_difference": res["mixed"]["nmi_mean"] - res["plain"]["nmi_mean"],
+                               "max_abs_nmi_difference_same_seed": float(max(dn)),
+                               "speedup_mean_seconds": res["plain"]["seconds_mean"] / res["mixed"]["seconds_mean"]}
+        del x
+        torch.cuda.empty_cache()
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 def run_c4(args, rank, world, local):

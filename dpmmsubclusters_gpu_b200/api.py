@@ -168,6 +168,19 @@ class dp_parallel_sampling_class:
         if self._from_file:
             raise RuntimeError("dp_parallel needs the (numLabels, all_data, seed, prior) constructor")
         n, dim = self.points.shape
+        rd, keep = self.run_desc(local_hyper_params, alpha_param, iters, init_clusters, verbose, burnout, gt,
+                                 max_clusters, outlier_weight, outlier_params)
+        h = c_void_p()
+        check(lib().dpmm_dp_parallel(byref(rd), n, dim, _dptr(self.points), byref(h)))
+        try:
+            return ModelInfo._from_handle(h)
+        finally:
+            lib().dpmm_model_info_free(h)
+
+    def run_desc(self, local_hyper_params, alpha_param: float, iters: int = 100, init_clusters: int = 1,
+                 verbose: bool = True, burnout: int = 15, gt: Optional[Sequence[int]] = None,
+                 max_clusters: float = DBL_MAX, outlier_weight: float = 0, outlier_params=None):
+        """The dpmm_run_desc of a dp_parallel call, and the arrays it points into (keep them alive)."""
         rd = capi.dpmm_run_desc()
         rd.prior_type = int(self.prior)
         rd.iterations = iters
@@ -206,12 +219,9 @@ class dp_parallel_sampling_class:
             g = np.ascontiguousarray(gt, dtype=np.int32)
             keep.append(g)
             rd.gt = _iptr(g)
-        h = c_void_p()
-        check(lib().dpmm_dp_parallel(byref(rd), n, dim, _dptr(self.points), byref(h)))
-        try:
-            return ModelInfo._from_handle(h)
-        finally:
-            lib().dpmm_model_info_free(h)
+        if self.screen_params is not None:
+            keep.append(self.screen_params)
+        return rd, keep
 
     def _put_screen(self, rd):
         rd.screen_mode = self.screen_mode
@@ -524,6 +534,19 @@ class CudaKernel:
         lml = np.empty(3 * K)
         check(lib().dpmm_sample_gaussian_params(self.ctx, K, seed, draw, _dptr(w), _dptr(lw), _dptr(lml)))
         return lml.reshape(K, 3)
+
+    def sample_multinomial_params(self, K: int, seed: int, draw: int, lr_weights):
+        """Dirichlet draws of every slot on the device (into the label-phase parameters); -> lml (K, 3)"""
+        lw = np.ascontiguousarray(lr_weights, np.float64).reshape(-1)
+        lml = np.empty(3 * K)
+        check(lib().dpmm_sample_multinomial_params(self.ctx, K, seed, draw, _dptr(lw), _dptr(lml)))
+        return lml.reshape(K, 3)
+
+    def get_multinomial_params(self, K: int):
+        """log theta (K, 3, D) of the cluster / l / r slots as the label phases use them"""
+        out = np.empty(3 * K * self.D, np.float32)
+        check(lib().dpmm_get_multinomial_params(self.ctx, K, _fptr(out)))
+        return out.reshape(K, 3, self.D)
 
     def merge_statistics(self, index, new_index):
         i = np.atleast_1d(np.asarray(index, np.int32))

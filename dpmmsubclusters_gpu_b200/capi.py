@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "libdpmm_b200.so")
 DPMM_OK = 0
 STATUS_NAMES = {0: "DPMM_OK", 1: "DPMM_ERR_INVALID_ARG", 2: "DPMM_ERR_OOM", 3: "DPMM_ERR_CUDA", 4: "DPMM_ERR_NOT_PD",
                 5: "DPMM_ERR_TIMEOUT", 6: "DPMM_ERR_NUMERIC", 7: "DPMM_ERR_STATE", 8: "DPMM_ERR_IO",
-                9: "DPMM_ERR_NO_DEVICE"}
+                9: "DPMM_ERR_NO_DEVICE", 10: "DPMM_ERR_EXCHANGE"}
 
 PRIOR_GAUSSIAN, PRIOR_MULTINOMIAL = 0, 1
 RNG_PHILOX, RNG_CURAND_XORWOW = 0, 1
@@ -52,6 +52,15 @@ class dpmm_run_desc(Structure):
                 ("screen_mode", c_int32), ("screen_top", c_int32), ("screen_sweep_every", c_int32),
                 ("screen_min_recall", c_float), ("screen_params", POINTER(c_float)), ("screen_split_min", c_int32),
                 ("host_param_draws", c_int32), ("label_prune_margin", c_float), ("reserved", c_int32 * 1)]
+
+
+# dpmm_allreduce_fn: int (*)(void* user, double* buf, int64_t count, void* stream)
+ALLREDUCE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, c_void_p, c_int64, c_void_p)
+
+
+class dpmm_shard(Structure):
+    _fields_ = [("rank", c_int32), ("world", c_int32), ("point_offset", c_int64), ("n_total", c_int64),
+                ("allreduce", ALLREDUCE_FN), ("user", c_void_p)]
 
 
 # every symbol include/dpmm_capi.h declares, with its ctypes signature
@@ -109,6 +118,9 @@ SIGNATURES = {
     "dpmm_model_info_write_json": (c_int, [c_void_p, c_char_p]),
     "dpmm_model_info_free": (None, [c_void_p]),
     "dpmm_sampler_create": (c_int, [POINTER(dpmm_run_desc), c_int64, c_int32, c_void_p, c_int32, POINTER(c_void_p)]),
+    "dpmm_sampler_create_sharded": (c_int, [POINTER(dpmm_run_desc), c_int64, c_int32, c_void_p, c_int32,
+                                            POINTER(dpmm_shard), POINTER(c_void_p)]),
+    "dpmm_set_shard": (c_int, [_CTX, POINTER(dpmm_shard)]),
     "dpmm_sampler_step": (c_int, [c_void_p, c_int32]),
     "dpmm_sampler_num_clusters": (c_int, [c_void_p, _PI32]),
     "dpmm_sampler_stream": (c_void_p, [c_void_p]),
@@ -135,10 +147,12 @@ SIGNATURES = {
     "dpmm_model_info_screen_log_kind": (POINTER(c_int8), [c_void_p]),
     "dpmm_model_info_screen_log_iter": (_PI32, [c_void_p]),
     "dpmm_sample_gaussian_params": (c_int, [_CTX, c_int, c_uint64, c_uint64, _PD, _PD, _PD]),
+    "dpmm_sample_multinomial_params": (c_int, [_CTX, c_int, c_uint64, c_uint64, _PD, _PD]),
     "dpmm_merge_statistics": (c_int, [_CTX, c_int, _PI32, _PI32]),
     "dpmm_compact_statistics": (c_int, [_CTX, c_int, _PI32]),
     "dpmm_statistics_counts": (c_int, [_CTX, c_int, _PI32, _PI64]),
     "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
+    "dpmm_get_multinomial_params": (c_int, [_CTX, c_int, _PF]),
     "dpmm_set_label_pruning": (c_int, [_CTX, c_double]),
     "dpmm_label_pruning_stats": (c_int, [_CTX, _PD]),
     "dpmm_set_ground_truth": (c_int, [_CTX, _PI32]),

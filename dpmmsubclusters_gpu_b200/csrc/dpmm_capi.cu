@@ -134,6 +134,7 @@ extern "C" const char* dpmm_status_string(dpmm_status s)
         case DPMM_ERR_STATE: return "call out of order";
         case DPMM_ERR_IO: return "I/O or parse error";
         case DPMM_ERR_NO_DEVICE: return "no CUDA device";
+        case DPMM_ERR_EXCHANGE: return "shard exchange failed";
     }
     return "unknown status";
 }
@@ -178,7 +179,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
-                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab};
+                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -212,6 +213,7 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     dpmm_ctx* c = new dpmm_ctx();
     c->device = desc->device;
     c->N = desc->n_points;
+    c->n_total = desc->n_points;
     c->D = desc->dim;
     c->prior = desc->prior_type;
     c->Dp = c->prior == DPMM_PRIOR_GAUSSIAN ? padded_dim(c->D) : mult_padded_dim(c->D);
@@ -438,7 +440,28 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
         if (e == cudaSuccess) {
             std::vector<double> sums(D);
             e = cudaMemcpy(sums.data(), c->d_gshift, sizeof(double) * D, cudaMemcpyDeviceToHost);
-            for (int d = 0; d < D; ++d) c->shift[d] = sums[d] / (double)N;
+            double n = (double)N;
+            if (e == cudaSuccess && c->shard_world > 1) {   // the mean of the whole data set
+                sums.push_back(n);
+                e = cudaMemcpy(c->d_xchg, sums.data(), sizeof(double) * (D + 1), cudaMemcpyHostToDevice);
+                if (e == cudaSuccess) {
+                    const dpmm_status xs = shard_allreduce(c, c->d_xchg, D + 1);
+                    if (xs != DPMM_OK) {
+                        cudaFree(tmp);
+                        return xs;
+                    }
+                    e = cudaMemcpy(sums.data(), c->d_xchg, sizeof(double) * (D + 1), cudaMemcpyDeviceToHost);
+                    n = sums[D];
+                }
+            }
+            // the shift keeps 20 significant bits of the mean: any value near the mean serves, and the
+            // rounding makes it the same whatever order the sums were added in (one context or shards)
+            for (int d = 0; d < D; ++d) {
+                const double m = sums[d] / n;
+                int ex = 0;
+                std::frexp(m, &ex);
+                c->shift[d] = m == 0.0 ? 0.0 : std::ldexp(std::nearbyint(std::ldexp(m, 20 - ex)), ex - 20);
+            }
             if (e == cudaSuccess)
                 e = cudaMemcpy(c->d_gshift, c->shift.data(), sizeof(double) * D, cudaMemcpyHostToDevice);
         }
@@ -460,6 +483,45 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
     c->points_ready = true;
     c->perm_K = -1;
     invalidate_stats(c);
+    return DPMM_OK;
+}
+
+namespace dpmm {
+dpmm_status shard_allreduce(dpmm_ctx* c, double* d_buf, int64_t count)
+{
+    if (c->shard_world <= 1 || count <= 0) return DPMM_OK;
+    const int rc = c->allreduce(c->allreduce_user, d_buf, count, (void*)c->stream);
+    if (rc != 0) return fail(DPMM_ERR_EXCHANGE, "shard allreduce of " + std::to_string(count) +
+                                                    " values failed (code " + std::to_string(rc) + ")");
+    return DPMM_OK;
+}
+}  // namespace dpmm
+
+extern "C" dpmm_status dpmm_set_shard(dpmm_ctx* c, const dpmm_shard* sh)
+{
+    if (!c || !sh) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->points_ready) return fail(DPMM_ERR_STATE, "dpmm_set_shard must come before the points are uploaded");
+    if (sh->world < 1 || sh->rank < 0 || sh->rank >= sh->world)
+        return fail(DPMM_ERR_INVALID_ARG, "shard rank / world out of range");
+    if (sh->world > 1 && !sh->allreduce) return fail(DPMM_ERR_INVALID_ARG, "a sharded context needs an allreduce");
+    if (sh->point_offset < 0 || sh->n_total < c->N || sh->point_offset + c->N > sh->n_total)
+        return fail(DPMM_ERR_INVALID_ARG, "shard point range outside [0, n_total)");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    c->shard_world = sh->world;
+    c->shard_rank = sh->rank;
+    c->pt_offset = sh->point_offset;
+    c->n_total = sh->n_total;
+    c->allreduce = sh->allreduce;
+    c->allreduce_user = sh->user;
+    if (sh->world > 1 && !c->d_xchg) {
+        c->xchg_len = std::max<size_t>((size_t)3 * c->k_max * c->stat_len, (size_t)c->D + 1);
+        DPMM_TRY(dev_alloc(&c->d_xchg, c->xchg_len));
+    }
+    // the per-point XORWOW states are keyed by the global point index
+    if (c->rng_kind == DPMM_RNG_CURAND_XORWOW && c->d_curand) {
+        DPMM_TRY(launch_init_curand(c));
+        DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    }
     return DPMM_OK;
 }
 
@@ -1223,14 +1285,40 @@ extern "C" dpmm_status dpmm_set_ground_truth(dpmm_ctx* c, const int32_t* gt)
     c->d_ctab = nullptr;
     c->gt_G = 0;
     if (!gt) return DPMM_OK;
-    // dense ids in order of first appearance
     std::vector<int32_t> ids(c->N);
-    std::unordered_map<int32_t, int32_t> map;
-    for (int64_t i = 0; i < c->N; ++i) {
-        auto it = map.emplace(gt[i], (int32_t)map.size()).first;
-        ids[i] = it->second;
+    int G = 0;
+    if (c->shard_world > 1) {
+        // the same dense ids on every shard: values in [0, 65536), ids in ascending order of the
+        // values present anywhere in the data set (presence summed over the shards)
+        constexpr int kV = 1 << 16;
+        std::vector<double> present(kV, 0.0);
+        for (int64_t i = 0; i < c->N; ++i) {
+            if (gt[i] < 0 || gt[i] >= kV)
+                return fail(DPMM_ERR_INVALID_ARG, "a sharded context takes ground-truth values in [0, 65536)");
+            present[gt[i]] = 1.0;
+        }
+        double* d_pres = nullptr;
+        DPMM_TRY(dev_alloc(&d_pres, (size_t)kV));
+        DPMM_CUDA_TRY(cudaMemcpy(d_pres, present.data(), sizeof(double) * kV, cudaMemcpyHostToDevice));
+        const dpmm_status xs = shard_allreduce(c, d_pres, kV);
+        cudaError_t e = xs == DPMM_OK ? cudaMemcpy(present.data(), d_pres, sizeof(double) * kV, cudaMemcpyDeviceToHost)
+                                      : cudaSuccess;
+        cudaFree(d_pres);
+        DPMM_TRY(xs);
+        DPMM_CUDA_TRY(e);
+        std::vector<int32_t> id_of(kV, -1);
+        for (int v = 0; v < kV; ++v)
+            if (present[v] > 0) id_of[v] = G++;
+        for (int64_t i = 0; i < c->N; ++i) ids[i] = id_of[gt[i]];
+    } else {
+        // dense ids in order of first appearance
+        std::unordered_map<int32_t, int32_t> map;
+        for (int64_t i = 0; i < c->N; ++i) {
+            auto it = map.emplace(gt[i], (int32_t)map.size()).first;
+            ids[i] = it->second;
+        }
+        G = (int)map.size();
     }
-    const int G = (int)map.size();
     if ((size_t)G * (size_t)c->k_max > ((size_t)1 << 26))
         return fail(DPMM_ERR_INVALID_ARG, "too many ground-truth classes for k_max (k_max x classes > 2^26)");
     DPMM_TRY(dev_alloc(&c->d_gt, (size_t)c->N));
@@ -1259,5 +1347,14 @@ extern "C" dpmm_status dpmm_label_agreement(dpmm_ctx* c, int K, double* nmi, dou
     DPMM_CUDA_TRY(cudaMemcpyAsync(table.data(), c->d_ctab, sizeof(int64_t) * T, cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     g_d2h_bytes += sizeof(int64_t) * T;
+    if (c->shard_world > 1) {   // the whole data set's table (counts below 2^53 are exact as doubles)
+        if (T > c->xchg_len) return fail(DPMM_ERR_INVALID_ARG, "contingency table larger than the exchange buffer");
+        std::vector<double> tv(table.begin(), table.end());
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_xchg, tv.data(), sizeof(double) * T, cudaMemcpyHostToDevice, c->stream));
+        DPMM_TRY(shard_allreduce(c, c->d_xchg, (int64_t)T));
+        DPMM_CUDA_TRY(cudaMemcpyAsync(tv.data(), c->d_xchg, sizeof(double) * T, cudaMemcpyDeviceToHost, c->stream));
+        DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        for (size_t i = 0; i < T; ++i) table[i] = (int64_t)tv[i];
+    }
     return dpmm_nmi_from_table(table.data(), K, G, nmi, vi);
 }

@@ -53,6 +53,7 @@ __device__ __forceinline__ float u01_from_bits(uint32_t x)
 
 __device__ __forceinline__ Philox4 philox_point(const RngArgs& r, int64_t pt)
 {
+    pt += r.offset;   // keyed by the global point index
     return philox4x32_10((uint32_t)pt, (uint32_t)((uint64_t)pt >> 32), (uint32_t)r.ctr,
                          (uint32_t)(r.ctr >> 32), (uint32_t)r.seed, (uint32_t)(r.seed >> 32));
 }

@@ -84,6 +84,7 @@ struct RngArgs {
     uint64_t ctr;                  // Philox draw counter (one per phase call)
     curandStateXORWOW* states;     // per point (compat mode)
     const float* ucaller;          // device copy of caller uniforms (or nullptr)
+    int64_t offset;                // global index of the context's first point (sharded data sets)
 };
 
 }  // namespace dpmm
@@ -213,6 +214,15 @@ struct dpmm_ctx {
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
 
+    // sharding by points (dpmm_set_shard): the aggregates are summed over the ranks by `allreduce`
+    int shard_world = 1, shard_rank = 0;
+    int64_t pt_offset = 0;         // global index of this shard's first point
+    int64_t n_total = 0;           // points of all shards (N when not sharded)
+    dpmm_allreduce_fn allreduce = nullptr;
+    void* allreduce_user = nullptr;
+    double* d_xchg = nullptr;      // staging of the exchanges: [3*k_max*stat_len] doubles (sharded only)
+    size_t xchg_len = 0;
+
     // events for phase timing (bench): device time per phase while `timing` is set
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;   // one kernel inside a phase (PH_LABEL_KERNEL)
@@ -337,6 +347,9 @@ bool tc_stats_supported(const dpmm_ctx* c);
 dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
+// In-place sum over the shards of `count` doubles at d_buf (device, written on the context's stream);
+// nothing to do for a context that is not sharded.
+dpmm_status shard_allreduce(dpmm_ctx* c, double* d_buf, int64_t count);
 // statistics of all points together (niw::create_sufficient_statistics over the whole data set)
 dpmm_status all_points_stats(dpmm_ctx* c, int64_t* count, double* sum, double* S);
 dpmm_status launch_fill_labels(dpmm_ctx* c, int32_t value);

@@ -26,21 +26,23 @@ RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller)
     r.ctr = c->philox_ctr++;
     r.states = c->d_curand;
     r.ucaller = d_ucaller;
+    r.offset = c->pt_offset;
     return r;
 }
 
 static inline int blocks_for(int64_t n, int t) { return (int)((n + t - 1) / t); }
 
 // ----------------------------------------------------------------------------- init draws
-__global__ void k_init_curand(curandStateXORWOW* st, uint64_t seed, int64_t n)
+// per-point XORWOW state, subsequence = the global point index (offset: the shard's first point)
+__global__ void k_init_curand(curandStateXORWOW* st, uint64_t seed, int64_t n, int64_t offset)
 {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) curand_init(seed, (unsigned long long)i, 0, &st[i]);   // cudaKernel.cu:19-25
+    if (i < n) curand_init(seed, (unsigned long long)(i + offset), 0, &st[i]);   // cudaKernel.cu:19-25
 }
 
 dpmm_status launch_init_curand(dpmm_ctx* c)
 {
-    k_init_curand<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(c->d_curand, c->seed, c->N);
+    k_init_curand<<<blocks_for(c->N, 256), 256, 0, c->stream>>>(c->d_curand, c->seed, c->N, c->pt_offset);
     DPMM_LAUNCHED();
     return DPMM_OK;
 }
@@ -1790,6 +1792,21 @@ __global__ void k_stats_finalize(const double* __restrict__ part, const int32_t*
     }
 }
 
+// masked cluster slots between the statistics and the exchange buffer: to_stats = 0 copies
+// src -> dst with zeros in the clusters the mask leaves out; to_stats = 1 copies back the masked ones
+__global__ void k_masked_slots(const double* __restrict__ src, double* __restrict__ dst, int64_t n, int per_cluster,
+                               const uint8_t* __restrict__ mask, int to_stats)
+{
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const bool on = mask[i / per_cluster] != 0;
+    if (to_stats) {
+        if (on) dst[i] = src[i];
+    } else {
+        dst[i] = on ? src[i] : 0.0;
+    }
+}
+
 dpmm_status launch_stats_finalize(dpmm_ctx* c, int K, const uint8_t* d_mask)
 {
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
@@ -1801,6 +1818,20 @@ dpmm_status launch_stats_finalize(dpmm_ctx* c, int K, const uint8_t* d_mask)
     k_stats_finalize<<<grid, 256, sm, c->stream>>>(c->d_part, c->d_chunk, c->d_nchunks, c->d_mu, c->d_gshift, c->D,
                                                 c->Dp, gauss, SL, c->stat_len, c->d_stats, d_mask);
     DPMM_LAUNCHED();
+    if (c->shard_world > 1) {
+        // this shard's statistics of the slots just finalised -> the sums over all shards.  With a
+        // mask only those slots: the others already hold the sums (and the same bookkeeping on every rank)
+        const int64_t n = (int64_t)3 * K * c->stat_len;
+        if (!d_mask) {
+            DPMM_TRY(shard_allreduce(c, c->d_stats, n));
+        } else {
+            k_masked_slots<<<blocks_for(n, 256), 256, 0, c->stream>>>(c->d_stats, c->d_xchg, n, 3 * c->stat_len, d_mask, 0);
+            DPMM_LAUNCHED();
+            DPMM_TRY(shard_allreduce(c, c->d_xchg, n));
+            k_masked_slots<<<blocks_for(n, 256), 256, 0, c->stream>>>(c->d_xchg, c->d_stats, n, 3 * c->stat_len, d_mask, 1);
+            DPMM_LAUNCHED();
+        }
+    }
     if (!d_mask) {
         c->stats_K = K;
         std::fill(c->stats_ok.begin(), c->stats_ok.end(), 0);
@@ -1881,6 +1912,15 @@ dpmm_status launch_sub_count(dpmm_ctx* c, int32_t* h_l, int32_t* h_r)
     int32_t h[2];
     DPMM_CUDA_TRY(cudaMemcpyAsync(h, c->d_aux, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (c->shard_world > 1) {   // counts of the whole data set
+        double v[2] = {(double)h[0], (double)h[1]};
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_xchg, v, sizeof(v), cudaMemcpyHostToDevice, c->stream));
+        DPMM_TRY(shard_allreduce(c, c->d_xchg, 2));
+        DPMM_CUDA_TRY(cudaMemcpyAsync(v, c->d_xchg, sizeof(v), cudaMemcpyDeviceToHost, c->stream));
+        DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+        h[0] = (int32_t)v[0];
+        h[1] = (int32_t)v[1];
+    }
     *h_l = h[0];
     *h_r = h[1];
     return DPMM_OK;

@@ -183,6 +183,44 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __res
     }
 }
 
+// multinomial_prior::sample_distribution (multinomial_prior.cpp:24-49) for every statistics slot: the
+// Dirichlet posterior alpha' = alpha + sum x (multinomial_prior.cpp:12-22), theta = g / sum g with
+// g_d ~ Gamma(alpha'_d, 1) (the gamma normalisation of dirichlet.h:39-48), log theta written into the
+// label-phase parameters; the slot's log marginal likelihood lnG(sum alpha) - lnG(sum alpha')
+// + sum [lnG(alpha'_d) - lnG(alpha_d)] (multinomial_prior.cpp:56-67; 0 for an empty slot, whose
+// posterior is the prior) for the splittable test.  One block per slot; element d draws from the
+// Philox streams 256 d .. 256 d + 201 of (slot, draw).
+__global__ void __launch_bounds__(256) k_draw_dirichlet(const double* __restrict__ stats, int stat_len, int D, int Dp,
+                                                        const double* __restrict__ alpha0, uint64_t seed,
+                                                        uint64_t draw, float* __restrict__ lt,
+                                                        float* __restrict__ cv, double* __restrict__ lml)
+{
+    __shared__ double red[33];
+    const int s = blockIdx.x, t = threadIdx.x;
+    const double* st = stats + (size_t)s * stat_len;
+    const double n = st[0];
+    double gsum = 0, a0 = 0, ap = 0, lg = 0;
+    for (int d = t; d < D; d += blockDim.x) {
+        const double a = alpha0[d], a1 = a + st[1 + d];
+        const double g = fmax(0.5 * chi2_draw(2.0 * a1, seed, draw, (uint32_t)s, (uint32_t)(256 * d)), 1e-300);
+        lt[(size_t)s * Dp + d] = (float)log(g);   // log g for now: the normalisation follows
+        gsum += g;
+        a0 += a;
+        ap += a1;
+        lg += lgamma(a1) - lgamma(a);
+    }
+    gsum = block_sum(gsum, red);
+    a0 = block_sum(a0, red);
+    ap = block_sum(ap, red);
+    lg = block_sum(lg, red);
+    const float lz = (float)log(gsum);
+    for (int d = t; d < Dp; d += blockDim.x) lt[(size_t)s * Dp + d] = d < D ? lt[(size_t)s * Dp + d] - lz : 0.f;
+    if (t == 0) {
+        cv[s] = 0.f;       // the multinomial cluster log-likelihood has no weight term (cudaKernel_multinomial.cu:60-76)
+        lml[s] = n > 0 ? lgamma(a0) - lgamma(ap) + lg : 0.0;
+    }
+}
+
 // merge_clusters_to_splittable for disjoint pairs (i, j): slots 3i, 3i+1 <- c_i + c_j, 3i+2 <- c_j
 __global__ void k_merge_stats(double* __restrict__ stats, int stat_len, const int32_t* __restrict__ pairs)
 {
@@ -275,6 +313,35 @@ extern "C" dpmm_status dpmm_sample_gaussian_params(dpmm_ctx* c, int K, uint64_t 
     return DPMM_OK;
 }
 
+extern "C" dpmm_status dpmm_sample_multinomial_params(dpmm_ctx* c, int K, uint64_t seed, uint64_t draw,
+                                                      const double* lr_weights, double* lml)
+{
+    if (!c || !lr_weights) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_MULTINOMIAL) return fail(DPMM_ERR_INVALID_ARG, "context is not multinomial");
+    if (K < 1 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [1, k_max]");
+    if (!c->prior_set) return fail(DPMM_ERR_STATE, "prior hyper-parameters not set");
+    if (c->stats_K < K) return fail(DPMM_ERR_STATE, "statistics of the K clusters are not on the device");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    std::vector<float> lrw(2 * (size_t)K);
+    for (int k = 0; k < 2 * K; ++k) lrw[k] = (float)std::log(lr_weights[k]);
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    float* hl = reinterpret_cast<float*>(c->h_pinned);
+    std::memcpy(hl, lrw.data(), sizeof(float) * 2 * K);
+    {
+        PhaseTimer pt(c, PH_PARAMS);
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hl, sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
+        g_h2d_bytes.fetch_add(sizeof(float) * 2 * K, std::memory_order_relaxed);
+        k_draw_dirichlet<<<3 * K, 256, 0, c->stream>>>(c->d_stats, c->stat_len, c->D, c->Dp, c->d_prior, seed, draw,
+                                                       c->d_mu, c->d_c, c->d_lml);
+        DPMM_LAUNCHED();
+        c->K_params = K;
+    }
+    if (lml) DPMM_CUDA_TRY(cudaMemcpyAsync(lml, c->d_lml, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (lml) g_d2h_bytes.fetch_add(sizeof(double) * 3 * K, std::memory_order_relaxed);
+    return DPMM_OK;
+}
+
 extern "C" dpmm_status dpmm_merge_statistics(dpmm_ctx* c, int n, const int32_t* index, const int32_t* new_index)
 {
     if (!c || n < 0 || (n > 0 && (!index || !new_index))) return fail(DPMM_ERR_INVALID_ARG, "bad pair list");
@@ -355,6 +422,18 @@ extern "C" dpmm_status dpmm_get_gaussian_params(dpmm_ctx* c, int K, float* wt, f
     if (b) DPMM_CUDA_TRY(cudaMemcpyAsync(b, c->d_b, sizeof(float) * S * Dp, cudaMemcpyDeviceToHost, c->stream));
     if (cv) DPMM_CUDA_TRY(cudaMemcpyAsync(cv, c->d_c, sizeof(float) * S, cudaMemcpyDeviceToHost, c->stream));
     if (mu) DPMM_CUDA_TRY(cudaMemcpyAsync(mu, c->d_mu, sizeof(float) * S * Dp, cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_get_multinomial_params(dpmm_ctx* c, int K, float* log_theta)
+{
+    if (!c || !log_theta) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_MULTINOMIAL) return fail(DPMM_ERR_STATE, "context is not multinomial");
+    if (K < 1 || K > c->K_params) return fail(DPMM_ERR_STATE, "parameters of K clusters are not set");
+    DPMM_CUDA_TRY(cudaSetDevice(c->device));
+    DPMM_CUDA_TRY(cudaMemcpy2DAsync(log_theta, sizeof(float) * c->D, c->d_mu, sizeof(float) * c->Dp, sizeof(float) * c->D,
+                                    3 * (size_t)K, cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
     return DPMM_OK;
 }

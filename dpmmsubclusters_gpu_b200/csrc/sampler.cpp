@@ -95,12 +95,13 @@ struct ScreenRecord {
 
 class Sampler {
 public:
+    // N: this context's points; the data set's total is ctx->n_total (larger for a shard)
     Sampler(const Config& cfg, dpmm_ctx* ctx, int64_t N, int D)
-        : cfg_(cfg), ctx_(ctx), N_(N), D_(D), gen_((unsigned long)cfg.seed)
+        : cfg_(cfg), ctx_(ctx), N_(N), Ntot_(ctx->n_total), D_(D), gen_((unsigned long)cfg.seed)
     {
         // device-resident parameters: the NIW draws run on the device from the device statistics,
         // the host keeps counts only (the outlier cluster's own prior stays on the host path)
-        dev_ = cfg.prior == DPMM_PRIOR_GAUSSIAN && !(cfg.outlier_mod > 0) && !cfg.host_param_draws && D <= 64;
+        dev_ = !(cfg.outlier_mod > 0) && !cfg.host_param_draws && (cfg.prior == DPMM_PRIOR_MULTINOMIAL || D <= 64);
     }
 
     // init_model + init_first_clusters, then iterations first..first+n-1 of run_model
@@ -326,7 +327,8 @@ private:
     dpmm_status calculate_posterior(double* out);
     Config cfg_;
     dpmm_ctx* ctx_;
-    int64_t N_;
+    int64_t N_;      // points of this context (its shard)
+    int64_t Ntot_;   // points of the whole data set
     int D_;
     int iter_ = 0;
     std::mt19937 gen_;
@@ -539,7 +541,10 @@ dpmm_status Sampler::sample_clusters_device()
     mixture_weights();
     std::vector<double> w(K, 0.0), lml(3 * (size_t)K);
     for (int k = 0; k < K && k < (int)weights_.size(); ++k) w[k] = weights_[k];
-    DPMM_TRY(dpmm_sample_gaussian_params(ctx_, K, cfg_.seed, draw_ctr_, w.data(), lrw.data(), lml.data()));
+    if (cfg_.prior == DPMM_PRIOR_MULTINOMIAL)
+        DPMM_TRY(dpmm_sample_multinomial_params(ctx_, K, cfg_.seed, draw_ctr_, lrw.data(), lml.data()));
+    else
+        DPMM_TRY(dpmm_sample_gaussian_params(ctx_, K, cfg_.seed, draw_ctr_, w.data(), lrw.data(), lml.data()));
     draw_ctr_ += 3 * (uint64_t)K;
     const int B = cfg_.burnout;
     for (int i = 0; i < K; ++i) {
@@ -922,7 +927,7 @@ dpmm_status Sampler::init_first_clusters()
         std::mt19937_64 g = draw_gen(draw_ctr_++);
         sc.c.dist = sample(cfg_.hyper, g);
         sc.c.post = cfg_.hyper;
-        sc.c.stats.N = N_;
+        sc.c.stats.N = Ntot_;
         sc.l = sc.c;
         sc.r = sc.c;
         sc.hist = fresh_hist();
@@ -946,7 +951,7 @@ dpmm_status Sampler::init_first_clusters()
 // draws the clusters' marginal likelihoods come from the device statistics
 dpmm_status Sampler::calculate_posterior(double* out)
 {
-    double lp = std::lgamma(cfg_.alpha) - std::lgamma((double)N_ + cfg_.alpha);
+    double lp = std::lgamma(cfg_.alpha) - std::lgamma((double)Ntot_ + cfg_.alpha);
     std::vector<double> dl;
     if (dev_ && !clusters_.empty()) {
         dl.resize(3 * clusters_.size());
@@ -1060,7 +1065,7 @@ struct SamplerHandle {
 
 // dp_parallel_sampling_class(N, x, seed, prior) + global_params::init + init_model + init_first_clusters
 dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* points, bool f32,
-                         std::unique_ptr<SamplerHandle>& out)
+                         std::unique_ptr<SamplerHandle>& out, const dpmm_shard* shard = nullptr)
 {
     auto h = std::make_unique<SamplerHandle>();
     Config& cfg = h->cfg;
@@ -1097,6 +1102,7 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
     desc.device = cfg.device;
     if (desc.k_max < cfg.initial_clusters + 2) desc.k_max = cfg.initial_clusters + 2;
     DPMM_TRY(dpmm_create(&desc, &h->ctx));
+    if (shard) DPMM_TRY(dpmm_set_shard(h->ctx, shard));
     if (f32) DPMM_TRY(dpmm_upload_points_f32(h->ctx, static_cast<const float*>(points)));
     else DPMM_TRY(dpmm_upload_points(h->ctx, static_cast<const double*>(points)));
     if (cfg.prior == DPMM_PRIOR_GAUSSIAN)
@@ -1233,6 +1239,19 @@ extern "C" dpmm_status dpmm_sampler_create(const dpmm_run_desc* run, int64_t n, 
     *out = nullptr;
     auto s = std::make_unique<dpmm_sampler>();
     DPMM_TRY(host::make_sampler(config_from_run(run, n, d), n, d, points, points_f32 != 0, s->h));
+    *out = s.release();
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_sampler_create_sharded(const dpmm_run_desc* run, int64_t n, int32_t d, const void* points,
+                                                   int32_t points_f32, const dpmm_shard* shard, dpmm_sampler** out)
+{
+    if (!run || !points || !out || n <= 0 || d <= 0 || !shard) return fail(DPMM_ERR_INVALID_ARG, "invalid argument");
+    *out = nullptr;
+    if (run->seed == 0 && shard->world > 1)
+        return fail(DPMM_ERR_INVALID_ARG, "a sharded run needs an explicit seed (the same on every rank)");
+    auto s = std::make_unique<dpmm_sampler>();
+    DPMM_TRY(host::make_sampler(config_from_run(run, n, d), n, d, points, points_f32 != 0, s->h, shard));
     *out = s.release();
     return DPMM_OK;
 }

@@ -55,7 +55,8 @@ typedef enum dpmm_status {
     DPMM_ERR_NUMERIC = 6,      /* NaN / Inf in inputs or results */
     DPMM_ERR_STATE = 7,        /* call out of order (e.g. no points uploaded) */
     DPMM_ERR_IO = 8,           /* file could not be read / parsed */
-    DPMM_ERR_NO_DEVICE = 9
+    DPMM_ERR_NO_DEVICE = 9,
+    DPMM_ERR_EXCHANGE = 10     /* a sharded context's allreduce reported a failure */
 } dpmm_status;
 
 /* prior_type (global_params.h:11-15) */
@@ -95,6 +96,31 @@ const char* dpmm_status_string(dpmm_status s);
 const char* dpmm_last_error(void);
 int dpmm_capi_version(void);
 
+/* ------------------------------------------------------------------ sharding by points
+ * No counterpart in the reference (its multi-device code is inactive, cudaKernel.cu:553-554).
+ * A context may hold one shard of a data set split by points over `world` ranks.  Per-point work
+ * (labels, sub-labels, relabels, the pruned label phase) stays on the shard; every aggregate the
+ * context returns or keeps -- the statistics of every cluster slot, the sub-label counts, the
+ * all-points statistics, the label-agreement contingency table, and the mean the points are
+ * shifted by -- is summed over the ranks through `allreduce`, so it is the whole data set's.
+ * Random numbers are keyed by the global point index (point_offset + local index), so a sharded
+ * run draws what one context over all points draws. */
+
+/* In-place sum over all ranks of `count` doubles in device memory at `buf`, which the context has
+ * written on `stream` (a cudaStream_t).  On return buf must hold the sums, identical on every rank,
+ * and work the context queues on `stream` afterwards must see them.  Every rank calls it the same
+ * number of times in the same order.  Returns 0 on success. */
+typedef int (*dpmm_allreduce_fn)(void* user, double* buf, int64_t count, void* stream);
+
+typedef struct dpmm_shard {
+    int32_t rank;               /* 0 .. world-1 */
+    int32_t world;              /* ranks holding shards of the data set */
+    int64_t point_offset;       /* global index of this shard's first point */
+    int64_t n_total;            /* points of all shards together */
+    dpmm_allreduce_fn allreduce;
+    void* user;                 /* passed to allreduce */
+} dpmm_shard;
+
 /* ------------------------------------------------------------------ device back-end */
 
 /* cudaKernel::init (cudaKernel.cu:537-635).  Unlike the reference it does not call
@@ -107,6 +133,9 @@ dpmm_status dpmm_destroy(dpmm_ctx* ctx);
  * points: N*D values, point-major. */
 dpmm_status dpmm_upload_points(dpmm_ctx* ctx, const double* points);
 dpmm_status dpmm_upload_points_f32(dpmm_ctx* ctx, const float* points);
+/* Makes the context one shard of a data set split by points (see dpmm_shard); call it before the
+ * points are uploaded.  In a sharded context dpmm_set_ground_truth takes values in [0, 65536). */
+dpmm_status dpmm_set_shard(dpmm_ctx* ctx, const dpmm_shard* shard);
 
 /* cudaKernel::sample_labels (cudaKernel.cu:1103-1111): labels uniform in
  * [1 + o, initial_clusters + o], o = (outlier_mod > 0). */
@@ -309,6 +338,13 @@ dpmm_status dpmm_screen_train(const float* features, const float* targets, int64
  * DPMM_ERR_NOT_PD. */
 dpmm_status dpmm_sample_gaussian_params(dpmm_ctx* ctx, int K, uint64_t seed, uint64_t draw, const double* weights,
                                         const double* lr_weights, double* lml);
+/* The same for the multinomial prior: multinomial_prior::sample_distribution (multinomial_prior.cpp:
+ * 24-49) for every slot, log theta = log of a Dirichlet(alpha + sum x) draw made on the device from
+ * the slot's statistics; lr_weights[2K]: the sub-cluster weights (the cluster label phase has no
+ * weight term, cudaKernel_multinomial.cu:60-76); lml (nullable, 3K): each slot's log marginal
+ * likelihood (multinomial_prior.cpp:56-67). */
+dpmm_status dpmm_sample_multinomial_params(dpmm_ctx* ctx, int K, uint64_t seed, uint64_t draw,
+                                           const double* lr_weights, double* lml);
 /* merge_clusters_to_splittable (shared_actions.cpp:72-86) applied to the device statistics for each
  * (disjoint) pair: cluster index[t] and its l sub-cluster take c_i + c_j, its r sub-cluster c_j. */
 dpmm_status dpmm_merge_statistics(dpmm_ctx* ctx, int n, const int32_t* index, const int32_t* new_index);
@@ -323,6 +359,9 @@ dpmm_status dpmm_statistics_counts(dpmm_ctx* ctx, int n, const int32_t* indices,
  * (+ log w for cluster slots), mu[3K][Dp] = mu - shift, where shift is the data mean the points are
  * stored relative to.  Any output may be NULL. */
 dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, float* c, float* mu);
+/* Test seam (no counterpart in the reference): log theta[3K][D] of the 3K slots of a multinomial context
+ * as the label phases use them (FP32). */
+dpmm_status dpmm_get_multinomial_params(dpmm_ctx* ctx, int K, float* log_theta);
 
 /* ---- pruned label phase (NIW prior, D <= 64; no counterpart in the reference) -----------------
  * dpmm_create_clusters_labels (without loglik_out) evaluates, for each chunk of points of one current
@@ -426,6 +465,16 @@ typedef struct dpmm_model_info dpmm_model_info;
 typedef struct dpmm_sampler dpmm_sampler;
 dpmm_status dpmm_sampler_create(const dpmm_run_desc* run, int64_t n, int32_t d, const void* points,
                                 int32_t points_f32, dpmm_sampler** out);
+/* The same sampler over one shard of a data set split by points across `shard->world` ranks
+ * (one process or thread per GPU), all ranks calling with the same run descriptor and seed.  The
+ * reference's multi-device code is inactive (cudaKernel.cu:553-554 keeps one device); this is the
+ * data-parallel form of its path: per-point work stays on each rank, the per-cluster statistics are
+ * summed over the ranks through shard->allreduce, and every host decision (split / merge tests,
+ * parameter draws, weights) is then taken identically on every rank from the same numbers with the
+ * same seeded generators.  n and points are this rank's shard; labels in the model info are its
+ * shard's labels. */
+dpmm_status dpmm_sampler_create_sharded(const dpmm_run_desc* run, int64_t n, int32_t d, const void* points,
+                                        int32_t points_f32, const dpmm_shard* shard, dpmm_sampler** out);
 dpmm_status dpmm_sampler_step(dpmm_sampler* s, int32_t n_iters);
 dpmm_status dpmm_sampler_num_clusters(const dpmm_sampler* s, int32_t* k);
 /* stream of the sampler's device work (cudaStream_t), for timing with events */
