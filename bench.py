@@ -140,6 +140,53 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
     return out
 
 
+def c3_config(args):
+    return dict(prior="multinomial", N=1_000_000, D=1000, K_true=50, alpha=10.0, prior_alpha=1.0, iterations=150,
+                burnout=15, theta_dirichlet=0.1, length_mean=200.0)
+
+
+def generate_c3_torch(cfg, seed, device):
+    """Seeded draws of the C3 shape on the device: theta ~ Dirichlet(0.1)^D per component, weights ~
+    Dirichlet(1), vector lengths ~ Poisson(200), counts ~ Multinomial(length, theta_z); returned as float32
+    counts (N x D, every value an integer that BF16 holds exactly below 257) and the component labels."""
+    import torch
+    torch.manual_seed(seed)
+    g = torch.Generator(device=device)
+    g.manual_seed(seed)
+    N, D, K = cfg["N"], cfg["D"], cfg["K_true"]
+    theta = torch.distributions.Dirichlet(torch.full((D,), cfg["theta_dirichlet"])).sample((K,)).to(device)
+    w = torch.distributions.Dirichlet(torch.ones(K)).sample().to(device)
+    z = torch.multinomial(w, N, replacement=True, generator=g)
+    lens = torch.poisson(torch.full((N,), cfg["length_mean"], device=device), generator=g).long()
+    x = torch.zeros(N, D, device=device, dtype=torch.float32)
+    L = int(lens.max().item())
+    for a in range(0, N, 50_000):
+        b = min(N, a + 50_000)
+        cat = torch.multinomial(theta[z[a:b]], L, replacement=True, generator=g)     # (n, L) categories
+        keep = (torch.arange(L, device=device)[None, :] < lens[a:b, None]).float()
+        x[a:b].scatter_add_(1, cat, keep)
+    return x.contiguous(), z
+
+
+def mult_kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, pk, pk_src):
+    """The multinomial label kernel's roofline: HBM-bound, it reads every point's counts once (BF16,
+    padded to whole 64-category blocks) and writes its K values of r and the draw's partials."""
+    hbm = pk.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+    out = {}
+    if ph_calls[7]:
+        ms = ph_ms[7] / ph_calls[7]
+        Dk = (D + 63) // 64 * 64
+        work = N * (2.0 * Dk + 4.0 * k_mean + 16.0)
+        ach = work / (ms / 1e3) / 1e9
+        out["k_mult_labels_tc"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                                   "traffic": None, "launch_ms": ms, "launches": int(ph_calls[7]),
+                                   "total_ms": ph_ms[7], "peak_source": f"hbm_gbs of {pk_src}",
+                                   "algorithmic": "N*(2*Dk + 4*K + 16) B per launch: BF16 counts (Dk = D padded to "
+                                                  "64), r written cluster-major, the draw's partials; tensor-core "
+                                                  "products 3 x 2*N*Dk*Kp FLOP"}
+    return out
+
+
 def c5_config(args):
     return dict(N=args.n, D=args.d, K_true=args.k_true, alpha=10.0, nu=args.d + 3.0, kappa=1.0, iterations=300,
                 mean_sd=5.0, dirichlet=2.0)
@@ -356,22 +403,28 @@ def make_run_desc(cfg, args, arm, iterations, rank, local, keep):
     import numpy as np
     a = ARMS[arm]
     rd = capi.dpmm_run_desc()
-    rd.prior_type = capi.PRIOR_GAUSSIAN
+    mult = cfg.get("prior") == "multinomial"
+    rd.prior_type = capi.PRIOR_MULTINOMIAL if mult else capi.PRIOR_GAUSSIAN
     rd.iterations = iterations
     rd.initial_clusters = args.initial_clusters
-    rd.burnout = 15
+    rd.burnout = cfg.get("burnout", 15)
     rd.alpha = cfg["alpha"]
     rd.seed = 12345 + (0 if args.multi_gpu == "shard" else rank)   # shards of one run share the seed
     rd.loglik_mode = {"auto": capi.LL_AUTO, "fp32": capi.LL_FP32, "tc": capi.LL_TC_BF16X3}[a["mode"]]
     rd.rng_kind = capi.RNG_PHILOX
     rd.k_max = 256
     rd.device = local
-    m = np.zeros(cfg["D"])
-    psi = np.eye(cfg["D"])
-    keep += [m, psi]
-    rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
-    rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-    rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    if mult:
+        al = np.full(cfg["D"], cfg["prior_alpha"])
+        keep.append(al)
+        rd.mult_alpha = al.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    else:
+        m = np.zeros(cfg["D"])
+        psi = np.eye(cfg["D"])
+        keep += [m, psi]
+        rd.niw_k, rd.niw_v = cfg["kappa"], cfg["nu"]
+        rd.niw_m = m.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+        rd.niw_psi = psi.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
     rd.host_param_draws = int(a["host_draws"])
     rd.label_prune_margin = 0.0 if a["prune"] else -1.0
     if a["screen"]:
@@ -491,7 +544,7 @@ def main():
                     help="points of the CPU baseline sample (timed at 1 thread and at all threads)")
     ap.add_argument("--profile-region", action="store_true",
                     help="bracket the timed steps with cudaProfilerStart/Stop (for ncu --profile-from-start off)")
-    ap.add_argument("--workload", default="c5", choices=["c5", "c4", "study"],
+    ap.add_argument("--workload", default="c5", choices=["c5", "c3", "c4", "study"],
                     help="c4: 256 uneven data sets advanced together (BatchSampler) vs one at a time; study: "
                          "NMI and final cluster count over 10 sampler seeds, mixed vs plain FP32")
     ap.add_argument("--study-seeds", type=int, default=10)
@@ -522,7 +575,8 @@ def main():
 
     from dpmmsubclusters_gpu_b200.capi import lib
     L = lib()
-    cfg = c5_config(args)
+    mult = args.workload == "c3"
+    cfg = c3_config(args) if mult else c5_config(args)
     N, D = cfg["N"], cfg["D"]
     args.gpus_world = world
     sharded = world > 1 and args.multi_gpu == "shard"
@@ -530,6 +584,9 @@ def main():
     if sharded:
         from dpmmsubclusters_gpu_b200.shard import TorchDistributedExchange
         shard = TorchDistributedExchange(device=True)
+    if mult:
+        x, z = generate_c3_torch(cfg, 1003 + (0 if sharded else rank), f"cuda:{local}")
+    elif sharded:
         x, z = generate_c5_torch(cfg, 1000 + 5, f"cuda:{local}", point_seed=7000 + rank)
     else:
         x, z = generate_c5_torch(cfg, 1000 + 5 + rank, f"cuda:{local}")
@@ -550,7 +607,10 @@ def main():
     pk, pk_src = peaks()
     k_mean = float(np.mean(ks)) if ks else float(r["k_before"])
     tc = padded(D) in (32, 64) and ARMS[args.arm]["mode"] != "fp32"
-    kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src, tc)
+    if mult:
+        kernels = mult_kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, pk, pk_src)
+    else:
+        kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src, tc)
     # the roofline of the kernel with the most device time in the timed region
     dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
     roofline = dict(kernels[dominant], kernel=dominant) if dominant else None
@@ -571,8 +631,11 @@ def main():
             "scaling": "weak", "vs_baseline": vs,
             "dtype": "f32+bf16x3" if ARMS[args.arm]["mode"] != "fp32" else "f32",
             "data": "synthetic (seeded draws of the configuration's generative model, generated on device)",
-            "config": {"workload": "C5 Gaussian DPMM N=1e7 D=64 100 true clusters (means N(0,25I), "
-                                   "cov AA^T/D+0.5I, Dir(2) weights, f32); NIW k=1 m=0 nu=67 Psi=I; alpha=10",
+            "config": {"workload": ("C3 multinomial DPMM N=1e6 D=1000 50 true components (theta ~ Dir(0.1), "
+                                    "weights Dir(1), lengths Poisson(200), counts BF16-exact); Dirichlet(1) prior; "
+                                    "alpha=10" if mult else
+                                    "C5 Gaussian DPMM N=1e7 D=64 100 true clusters (means N(0,25I), "
+                                    "cov AA^T/D+0.5I, Dir(2) weights, f32); NIW k=1 m=0 nu=67 Psi=I; alpha=10"),
                        "N": N, "D": D, "arm": args.arm, "arm_what": ARMS[args.arm]["what"],
                        "multi_gpu": ("one data set of %d x N points sharded by points, statistics summed with "
                                      "NCCL (weak scaling)" % world if sharded else
@@ -608,9 +671,12 @@ def main():
     del x
     torch.cuda.empty_cache()
 
-    if rank == 0 and not args.no_cpu:
+    if mult:
+        line["metric"] = "sampler points*iters/sec at C3 (multinomial N=1e6 D=1000): mixed+learned vs plain FP32"
+        line["dtype"] = "bf16 counts x bf16x3 log theta, f32 accumulate" if ARMS[args.arm]["mode"] != "fp32" else "f32"
+    if rank == 0 and not args.no_cpu and not mult:
         line["cpu_baseline"] = cpu_baseline(cfg["K_true"], D, args.cpu_points)
-    if not args.no_e2e:
+    if not args.no_e2e and not mult:
         line["e2e"] = run_e2e(args, cfg, rank, local, world, dist, L)
     if dist:
         dist.barrier()

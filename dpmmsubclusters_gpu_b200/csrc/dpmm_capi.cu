@@ -179,7 +179,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
-                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg};
+                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg, c->d_Amult, c->d_Bmult};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -274,6 +274,12 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
             chk(dev_alloc(&c->d_rpart, (size_t)4 * N));
             chk(dev_alloc(&c->d_Bsub, (size_t)KM * 32768));
         }
+    }
+    if (!gauss && c->ll_mode != DPMM_LL_FP32 && c->D <= kMaxMultDim) {
+        chk(dev_alloc(&c->d_Amult, mult_tc_a_bytes(N, c->D)));
+        chk(dev_alloc(&c->d_Bmult, mult_tc_b_bytes(KM, c->D)));
+        chk(dev_alloc(&c->d_rbuf, (size_t)N * KM));
+        chk(dev_alloc(&c->d_rpart, (size_t)4 * N));
     }
     chk(dev_alloc(&c->d_c, (size_t)3 * KM));
     chk(dev_alloc(&c->d_lrw, (size_t)2 * KM));
@@ -477,6 +483,7 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
     cudaFree(tmp);
     if (e != cudaSuccess) return cuda_status(e, "dpmm_upload_points");
     DPMM_TRY(pack_tc_points(c));
+    DPMM_TRY(pack_mult_tc_points(c));
     int32_t bad = 0;
     DPMM_CUDA_TRY(cudaMemcpy(&bad, c->d_aux, sizeof(int32_t), cudaMemcpyDeviceToHost));
     if (bad) return fail(DPMM_ERR_NUMERIC, "points contain NaN or Inf");
@@ -496,6 +503,13 @@ dpmm_status shard_allreduce(dpmm_ctx* c, double* d_buf, int64_t count)
     return DPMM_OK;
 }
 }  // namespace dpmm
+
+extern "C" dpmm_status dpmm_set_wait_test(dpmm_ctx* c, int32_t stall)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    c->stall_tc_mma = stall != 0;
+    return DPMM_OK;
+}
 
 extern "C" dpmm_status dpmm_set_shard(dpmm_ctx* c, const dpmm_shard* sh)
 {
@@ -752,6 +766,7 @@ extern "C" dpmm_status dpmm_set_multinomial_params(dpmm_ctx* c, int K, const dou
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c, hc, sizeof(float) * 3 * K, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hlrw.data(), sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
     c->K_params = K;
+    c->mult_tc_K = -1;
     return DPMM_OK;
 }
 
@@ -795,7 +810,8 @@ extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final
     float* d_rout = nullptr;
     if (loglik_out) DPMM_TRY(dev_alloc(&d_rout, (size_t)c->N * K));
     dpmm_status s;
-    const bool use_tc = c->ll_mode != DPMM_LL_FP32 && tc_supported(c, K);
+    const bool mult_tc = c->prior == DPMM_PRIOR_MULTINOMIAL && tc_mult_supported(c, K);
+    const bool use_tc = c->ll_mode != DPMM_LL_FP32 && (tc_supported(c, K) || mult_tc);
     PhaseTimer pt(c, PH_LABELS);
     bool pruned = false;
     s = DPMM_OK;
@@ -804,7 +820,9 @@ extern "C" dpmm_status dpmm_create_clusters_labels(dpmm_ctx* c, int K, int final
     } else if (c->ll_mode == DPMM_LL_TC_BF16X3 && !use_tc) {
         s = fail(DPMM_ERR_INVALID_ARG, "tensor-core log-likelihood not available for this shape");
     } else {
-        s = use_tc ? launch_cluster_labels_tc(c, K, final_, du, d_rout) : launch_cluster_labels(c, K, final_, du, d_rout);
+        s = mult_tc  ? launch_mult_labels_tc(c, K, final_, du, d_rout)
+            : use_tc ? launch_cluster_labels_tc(c, K, final_, du, d_rout)
+                     : launch_cluster_labels(c, K, final_, du, d_rout);
     }
     if (s == DPMM_OK && d_rout) {
         cudaError_t e = cudaMemcpyAsync(loglik_out, d_rout, sizeof(float) * (size_t)c->N * K, cudaMemcpyDeviceToHost,

@@ -132,6 +132,11 @@ struct dpmm_ctx {
                                    // swizzled tile, packed once when the points are uploaded
     uint8_t* d_Bsub = nullptr;     // tensor-core sub-label phase: per cluster its two sub-cluster
                                    // factors as one 32 KB split-bf16 swizzled B tile
+    uint8_t* d_Amult = nullptr;    // multinomial tensor-core label phase: the counts as BF16, per
+                                   // (128-point tile, 64-category block) one 16 KB swizzled tile
+    uint8_t* d_Bmult = nullptr;    // ... log theta of the clusters as three BF16 parts per block
+    bool mult_tc_ok = false;       // every count is held exactly by BF16 (checked at upload)
+    int mult_tc_K = -1;            // clusters packed in d_Bmult (-1: stale)
     float* d_rbuf = nullptr;       // tensor-core label phase: r cluster-major [k_max][N]
     float* d_rpart = nullptr;      // per point and half: running max, sum of exp (or best, arg) [4][N]
     std::vector<float> h_param_stage;
@@ -213,6 +218,8 @@ struct dpmm_ctx {
     unsigned long long* d_prune_cnt = nullptr;   // [2]
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
+
+    int stall_tc_mma = 0;          // test seam (dpmm_set_wait_test): tensor-core label kernels issue no products
 
     // sharding by points (dpmm_set_shard): the aggregates are summed over the ranks by `allreduce`
     int shard_world = 1, shard_rank = 0;
@@ -334,6 +341,13 @@ bool tc_supported(const dpmm_ctx* c, int K);
 dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 dpmm_status pack_tc_params(dpmm_ctx* c, int K);
 dpmm_status pack_tc_points(dpmm_ctx* c);   // A operand from the uploaded points
+// multinomial label phase on the tensor cores (dpmm_tc.cu)
+bool tc_mult_supported(const dpmm_ctx* c, int K);
+size_t mult_tc_a_bytes(int64_t N, int D);
+size_t mult_tc_b_bytes(int k_max, int D);
+dpmm_status pack_mult_tc_points(dpmm_ctx* c);          // the counts as BF16 tiles (at upload)
+dpmm_status pack_mult_tc_params(dpmm_ctx* c, int K);   // log theta as three BF16 parts
+dpmm_status launch_mult_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout);
 size_t tc_param_bytes(int k_max);          // B tiles + bias records for k_max clusters
 // tensor-core sub-label kernel (dpmm_tc.cu): draws the sub-labels only (statistics separately)
 bool tc_sub_supported(const dpmm_ctx* c);

@@ -335,6 +335,7 @@ extern "C" dpmm_status dpmm_sample_multinomial_params(dpmm_ctx* c, int K, uint64
                                                        c->d_mu, c->d_c, c->d_lml);
         DPMM_LAUNCHED();
         c->K_params = K;
+        c->mult_tc_K = -1;
     }
     if (lml) DPMM_CUDA_TRY(cudaMemcpyAsync(lml, c->d_lml, sizeof(double) * 3 * K, cudaMemcpyDeviceToHost, c->stream));
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));

@@ -337,7 +337,7 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint32_t bytes)
 __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
     const uint8_t* __restrict__ Apack, int64_t N, int ntiles, const uint8_t* __restrict__ Bpack,
     const uint8_t* __restrict__ Bbias, int Dp, int K, int bstages, int final_, float* __restrict__ rbuf,
-    float* __restrict__ part, float* __restrict__ r_out, int32_t* __restrict__ err)
+    float* __restrict__ part, float* __restrict__ r_out, int32_t* __restrict__ err, int stall)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -444,8 +444,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_gauss_labels_tc(
     } else if (warp < WARP_DRAIN0) {
         // ---------------- MMA issuers: warp WARP_MMA0 + h issues the half-h MMAs of every N tile
         // into accumulator 2t + h and commits to the shared barriers (count MMA_WARPS); while one
-        // issuer waits or commits, the other's MMAs keep the tensor pipe fed
-        if (lane == 0) {
+        // issuer waits or commits, the other's MMAs keep the tensor pipe fed.  stall (test seam):
+        // no product is issued, so the waits for them run out and report ERR_TIMEOUT_*
+        if (lane == 0 && !stall) {
             const int h = warp - WARP_MMA0;
             int g = 0, la = 0, issued = 0;
             const uint64_t dah = sw128_desc(smem_u32(sA + (size_t)h * A_TILE));
@@ -1848,7 +1849,8 @@ dpmm_status launch_cluster_labels_tc(dpmm_ctx* c, int K, int final_, const float
         KernelTimer kt(c, PH_LABEL_KERNEL);
         tc::k_gauss_labels_tc<<<grid, tc::THREADS, L.total, c->stream>>>(c->d_Atc, c->N, (int)ntiles, c->d_Btc,
                                                                          tc_bias_base(c), c->Dp, K, bstages, final_,
-                                                                         c->d_rbuf, c->d_rpart, d_rout, err);
+                                                                         c->d_rbuf, c->d_rpart, d_rout, err,
+                                                                         c->stall_tc_mma);
         DPMM_LAUNCHED();
     }
     RngArgs r = rng_args(c, d_u);
@@ -1962,6 +1964,361 @@ dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask)
                                                     std::to_string(h_err[1]) + ")");
     if (*h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core statistics: bounded wait expired (code " +
                                                   std::to_string(*h_err) + ")");
+    return DPMM_OK;
+}
+
+}  // namespace dpmm
+
+namespace dpmm {
+namespace tc {
+
+// ============================================================================= multinomial label phase
+// cudaKernel_multinomial::log_likelihood_labels (cudaKernel_multinomial.cu:22-35, 60-76: r_k(x) =
+// sum_d x_d log theta_kd, no weight term) for every cluster as one contraction on the tensor cores:
+// C[p, k] = sum_d X[p, d] T[k, d] with the counts X stored as BF16 (exact: the upload checks that
+// every count is a BF16 value) and log theta split into three BF16 terms (hi + mid + lo = the FP32
+// value exactly), so r is the FP32 dot product of the SIMT form up to the order of the additions.
+// Operands are packed once in the exact shared-memory image (K-major, 128-byte swizzle): the counts
+// per (128-point tile, 64-category block) at upload, log theta per 64-category block after every
+// parameter update; each pipeline stage is then two cp.async.bulk copies.
+//
+// Persistent CTAs (one per SM) walk the 128-point tiles:
+//   warp 0      producer: per (tile, block) the counts (16 KB) and the three log theta parts
+//               (3 x Kp x 128 B) into a ring of stages
+//   warp 1      allocates TMEM; lane 0 issues per block 4 k-steps x 3 parts of tcgen05.mma
+//               (kind::f16, M = 128, N = Kp, K = 16) into one of two accumulators
+//   warps 2-5   epilogue (TMEM lane quarter = warp % 4): per point the K values of r, written
+//               cluster-major to rbuf[k][point] (32 points per store), and the point's max and sum of
+//               exp (or its first maximum, final mode) as the partials k_draw_labels reads; then the
+//               softmax + alias draw runs in k_draw_labels as for the Gaussian tensor-core phase.
+// Every wait is bounded; on expiry the CTA records the error, stops issuing, waits (bounded) for the
+// copies and products it issued and frees its TMEM.
+constexpr int MT_KB = 64;                          // categories per block: one 128-byte BF16 row
+constexpr int MT_A = BM * MT_KB * 2;               // 16 KB of counts per (tile, block)
+constexpr int MT_PARTS = 3;                        // log theta = hi + mid + lo (BF16)
+constexpr int MT_MAX_KP = 224;                     // clusters per contraction (N of the MMA)
+constexpr int MT_THREADS = 192;
+constexpr int MT_MAX_STAGES = 8;
+
+__host__ __device__ constexpr uint32_t mt_stage_bytes(int Kp) { return (uint32_t)(MT_A + MT_PARTS * Kp * 128); }
+
+__global__ void __launch_bounds__(MT_THREADS, 1) k_mult_labels_tc(
+    const uint8_t* __restrict__ Acnt, int64_t N, int ntiles, int nkb, const uint8_t* __restrict__ Bth, int Kp, int K,
+    int stages, int final_, float* __restrict__ rbuf, float* __restrict__ part, float* __restrict__ r_out,
+    int32_t* __restrict__ err, int stall)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    const uint32_t SB = mt_stage_bytes(Kp);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + (size_t)stages * SB);
+    uint64_t* empty = full + MT_MAX_STAGES;
+    uint64_t* afull = empty + MT_MAX_STAGES;         // [2] accumulator a holds a finished tile
+    uint64_t* aempty = afull + 2;                    // [2] the epilogue has read accumulator a
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(aempty + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+    uint32_t ncols = 32;
+    while (ncols < (uint32_t)(2 * Kp)) ncols <<= 1;
+
+    if (tid == 0) {
+        for (int s = 0; s < stages; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int a = 0; a < 2; ++a) {
+            mbar_init(afull + a, 1);
+            mbar_init(aempty + a, 4);                // one arrival per epilogue warp
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(ncols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+
+    if (warp == 0) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            int64_t g = 0;   // (tile, block) pairs issued
+            bool ok = true;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+                for (int kb = 0; kb < nkb; ++kb, ++g) {
+                    const int s = (int)(g % stages);
+                    if (g >= stages && !mbar_wait_bounded(empty + s, (uint32_t)(((g / stages) - 1) & 1), gerr)) {
+                        atomicCAS(err, 0, ERR_TIMEOUT_EMPTY);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* dst = smem + (size_t)s * SB;
+                    mbar_arrive_expect_tx(full + s, SB);
+                    bulk_copy_g2s(dst, Acnt + ((size_t)tile * nkb + kb) * MT_A, MT_A, full + s);
+                    bulk_copy_g2s(dst + MT_A, Bth + (size_t)kb * MT_PARTS * Kp * 128, MT_PARTS * Kp * 128, full + s);
+                }
+            }
+            // nothing may land in shared memory after the CTA exits: wait for the last use of every stage
+            for (int64_t q = g - 1; q >= 0 && q >= g - stages; --q)
+                mbar_wait_bounded(full + (int)(q % stages), (uint32_t)((q / stages) & 1), nullptr);
+        }
+    } else if (warp == 1) {
+        // ------------------------------------------------------------ MMA issuer (stall, test seam:
+        // nothing is issued, so the waits for the products run out and report ERR_TIMEOUT_*)
+        if (lane == 0 && !stall) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(Kp >> 3) << 17) |
+                                   ((uint32_t)(BM >> 4) << 24);
+            int64_t g = 0;
+            int it = 0;
+            bool ok = true;
+            uint64_t* last = nullptr;   // the barrier of the last commit and its phase
+            uint32_t last_par = 0;
+            for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++it) {
+                const int a = it & 1;
+                if (it >= 2 && !mbar_wait_bounded(aempty + a, (uint32_t)(((it >> 1) - 1) & 1), gerr)) {
+                    atomicCAS(err, 0, ERR_TIMEOUT_TEMPTY);
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t td = tmem_base + (uint32_t)(a * Kp);
+                for (int kb = 0; kb < nkb; ++kb, ++g) {
+                    const int s = (int)(g % stages);
+                    if (!mbar_wait_bounded(full + s, (uint32_t)((g / stages) & 1), gerr)) {
+                        atomicCAS(err, 0, ERR_TIMEOUT_FULL);
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t sa = smem_u32(smem + (size_t)s * SB);
+                    const uint64_t da = sw128_desc(sa);
+#pragma unroll
+                    for (int ks = 0; ks < MT_KB / 16; ++ks)
+#pragma unroll
+                        for (int p = 0; p < MT_PARTS; ++p) {
+                            const uint64_t db = sw128_desc(sa + MT_A + (uint32_t)(p * Kp * 128));
+                            const uint32_t acc = (kb | ks | p) != 0 ? 1u : 0u;
+                            asm volatile(
+                                "{\n\t.reg .pred q;\n\t"
+                                "setp.ne.b32 q, %4, 0;\n\t"
+                                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, q;\n\t}" ::"r"(td),
+                                "l"(da + 2 * ks), "l"(db + 2 * ks), "r"(idesc), "r"(acc)
+                                : "memory");
+                        }
+                    umma_commit(empty + s);
+                    last = empty + s;
+                    last_par = (uint32_t)((g / stages) & 1);
+                }
+                if (!ok) break;
+                umma_commit(afull + a);
+                last = afull + a;
+                last_par = (uint32_t)((it >> 1) & 1);
+            }
+            if (!ok && last) mbar_wait_bounded(last, last_par, nullptr);   // no product in flight at dealloc
+        }
+    } else {
+        // ------------------------------------------------------------ epilogue
+        const int q = warp & 3;
+        const int row = q * 32 + lane;
+        int it = 0;
+        for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+            const int a = it & 1;
+            if (!warp_wait_bounded(afull + a, (uint32_t)((it >> 1) & 1), gerr)) {
+                if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+                break;
+            }
+            tc_fence_after();
+            const int64_t pt = (int64_t)tile * BM + row;
+            const bool live = pt < N;
+            const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * Kp);
+            float mx = -INFINITY;
+            int arg = -1;
+            for (int c0 = 0; c0 < Kp; c0 += 32) {
+                uint32_t v[32];
+                tmem_ld32(taddr + (uint32_t)c0, v);
+#pragma unroll
+                for (int m = 0; m < 32; ++m) {
+                    const int k = c0 + m;
+                    const float r = __uint_as_float(v[m]);
+                    if (k < K) {
+                        if (live) {
+                            rbuf[(size_t)k * N + pt] = r;
+                            if (r_out) r_out[(size_t)pt * K + k] = r;
+                        }
+                        if (r > mx) {   // first maximum wins (cudaKernel.cu:405-424)
+                            mx = r;
+                            arg = k;
+                        }
+                    }
+                }
+            }
+            float sum = 0.f;
+            if (!final_) {
+                for (int c0 = 0; c0 < Kp; c0 += 32) {
+                    uint32_t v[32];
+                    tmem_ld32(taddr + (uint32_t)c0, v);
+#pragma unroll
+                    for (int m = 0; m < 32; ++m)
+                        if (c0 + m < K) sum += __expf(__uint_as_float(v[m]) - mx);
+                }
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(aempty + a);
+            if (live) {
+                // the partials of k_draw_labels: half 0 holds every cluster, half 1 none
+                part[pt] = mx;
+                part[N + pt] = final_ ? __int_as_float(arg) : sum;
+                part[2 * N + pt] = -INFINITY;
+                part[3 * N + pt] = final_ ? __int_as_float(-1) : 0.f;
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ncols));
+    }
+}
+
+// counts (FP32 rows, stride Dp) -> BF16 tiles in the shared-memory image: Apack[(t * nkb + kb)] = 16 KB
+// holding points 128 t .. +127, categories 64 kb .. +63 (zero past N / D).  inexact counts a count
+// that BF16 does not hold exactly.
+__global__ void k_pack_mult_a(const float* __restrict__ x, int64_t N, int D, int Dp, int64_t ntiles, int nkb,
+                              uint8_t* __restrict__ Apack, int32_t* __restrict__ inexact)
+{
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;   // (tile, block, row, 8-chunk)
+    if (e >= ntiles * nkb * BM * 8) return;
+    const int ch = (int)(e % 8), row = (int)((e / 8) % BM);
+    const int64_t tb = e / (8 * BM);
+    const int kb = (int)(tb % nkb);
+    const int64_t t = tb / nkb;
+    const int64_t pt = t * BM + row;
+    __align__(16) __nv_bfloat16 v[8];
+    int bad = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int d = kb * MT_KB + ch * 8 + j;
+        const float f = (pt < N && d < D) ? x[pt * Dp + d] : 0.f;
+        v[j] = __float2bfloat16_rn(f);
+        bad |= __bfloat162float(v[j]) != f;
+    }
+    if (bad) atomicAdd(inexact, 1);
+    *reinterpret_cast<uint4*>(Apack + (size_t)tb * MT_A + sw128_offset(row, ch * 8)) = *reinterpret_cast<const uint4*>(v);
+}
+
+// log theta of the cluster slots (3k, FP32 rows of stride Dp) -> three BF16 parts in the shared-memory
+// image: Bpack[kb][part] = Kp rows x 128 B (zero past K / D)
+__global__ void k_pack_mult_b(const float* __restrict__ lt, int K, int D, int Dp, int Kp, int nkb,
+                              uint8_t* __restrict__ Bpack)
+{
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;   // (block, row, 8-chunk)
+    if (e >= nkb * Kp * 8) return;
+    const int ch = e % 8, k = (e / 8) % Kp, kb = e / (8 * Kp);
+    __align__(16) __nv_bfloat16 hi[8], mid[8], lo[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        const int d = kb * MT_KB + ch * 8 + j;
+        const float f = (k < K && d < D) ? lt[(size_t)3 * k * Dp + d] : 0.f;
+        hi[j] = __float2bfloat16_rn(f);
+        const float r1 = f - __bfloat162float(hi[j]);
+        mid[j] = __float2bfloat16_rn(r1);
+        lo[j] = __float2bfloat16_rn(r1 - __bfloat162float(mid[j]));
+    }
+    uint8_t* base = Bpack + (size_t)kb * MT_PARTS * Kp * 128;
+    const uint32_t off = sw128_offset(k, ch * 8);
+    *reinterpret_cast<uint4*>(base + off) = *reinterpret_cast<const uint4*>(hi);
+    *reinterpret_cast<uint4*>(base + (size_t)Kp * 128 + off) = *reinterpret_cast<const uint4*>(mid);
+    *reinterpret_cast<uint4*>(base + (size_t)2 * Kp * 128 + off) = *reinterpret_cast<const uint4*>(lo);
+}
+
+}  // namespace tc
+
+static int mt_kp(int K) { return std::max(32, (K + 31) / 32 * 32); }
+
+static int mt_stages(int Kp)
+{
+    const size_t avail = kTcSmemCap - 1024 - 256;
+    return (int)std::min<size_t>(tc::MT_MAX_STAGES, avail / tc::mt_stage_bytes(Kp));
+}
+
+bool tc_mult_supported(const dpmm_ctx* c, int K)
+{
+    return c->prior == DPMM_PRIOR_MULTINOMIAL && c->d_Amult != nullptr && c->mult_tc_ok && c->d_rbuf != nullptr &&
+           c->ll_mode != DPMM_LL_FP32 && K >= 1 && K <= c->k_max && mt_kp(K) <= tc::MT_MAX_KP && mt_stages(mt_kp(K)) >= 2;
+}
+
+size_t mult_tc_a_bytes(int64_t N, int D)
+{
+    return (size_t)((N + tc::BM - 1) / tc::BM) * (size_t)((D + tc::MT_KB - 1) / tc::MT_KB) * tc::MT_A;
+}
+
+size_t mult_tc_b_bytes(int k_max, int D)
+{
+    const int kp = std::min(tc::MT_MAX_KP, mt_kp(k_max));
+    return (size_t)((D + tc::MT_KB - 1) / tc::MT_KB) * tc::MT_PARTS * kp * 128;
+}
+
+dpmm_status pack_mult_tc_points(dpmm_ctx* c)
+{
+    if (!c->d_Amult) return DPMM_OK;
+    const int64_t ntiles = (c->N + tc::BM - 1) / tc::BM;
+    const int nkb = (c->D + tc::MT_KB - 1) / tc::MT_KB;
+    int32_t* inexact = c->d_aux + 8;
+    DPMM_CUDA_TRY(cudaMemsetAsync(inexact, 0, sizeof(int32_t), c->stream));
+    const int64_t items = ntiles * nkb * tc::BM * 8;
+    tc::k_pack_mult_a<<<(unsigned)((items + 255) / 256), 256, 0, c->stream>>>(c->d_x, c->N, c->D, c->Dp, ntiles, nkb,
+                                                                             c->d_Amult, inexact);
+    DPMM_LAUNCHED();
+    int32_t h = 0;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(&h, inexact, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->mult_tc_ok = h == 0;   // counts that BF16 does not hold exactly: the FP32 SIMT form only
+    return DPMM_OK;
+}
+
+dpmm_status pack_mult_tc_params(dpmm_ctx* c, int K)
+{
+    if (!c->d_Amult || !c->mult_tc_ok || mt_kp(K) > tc::MT_MAX_KP) return DPMM_OK;
+    const int Kp = mt_kp(K), nkb = (c->D + tc::MT_KB - 1) / tc::MT_KB;
+    const int items = nkb * Kp * 8;
+    tc::k_pack_mult_b<<<(items + 255) / 256, 256, 0, c->stream>>>(c->d_mu, K, c->D, c->Dp, Kp, nkb, c->d_Bmult);
+    DPMM_LAUNCHED();
+    c->mult_tc_K = K;
+    return DPMM_OK;
+}
+
+dpmm_status launch_mult_labels_tc(dpmm_ctx* c, int K, int final_, const float* d_u, float* d_rout)
+{
+    if (!tc_mult_supported(c, K)) return fail(DPMM_ERR_INVALID_ARG, "tensor-core multinomial labels: unsupported shape");
+    if (c->mult_tc_K != K) DPMM_TRY(pack_mult_tc_params(c, K));
+    const int Kp = mt_kp(K), stages = mt_stages(Kp);
+    const size_t sm = 1024 + (size_t)stages * tc::mt_stage_bytes(Kp) + (2 * tc::MT_MAX_STAGES + 4) * 8 + 16;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(tc::k_mult_labels_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    int32_t* err = c->d_aux + 7;
+    DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
+    const int64_t ntiles = (c->N + tc::BM - 1) / tc::BM;
+    const int nkb = (c->D + tc::MT_KB - 1) / tc::MT_KB;
+    const unsigned grid = (unsigned)std::min<int64_t>(ntiles, c->num_sms);
+    {
+        KernelTimer kt(c, PH_LABEL_KERNEL);
+        tc::k_mult_labels_tc<<<grid, tc::MT_THREADS, sm, c->stream>>>(c->d_Amult, c->N, (int)ntiles, nkb, c->d_Bmult,
+                                                                      Kp, K, stages, final_, c->d_rbuf, c->d_rpart,
+                                                                      d_rout, err, c->stall_tc_mma);
+        DPMM_LAUNCHED();
+    }
+    RngArgs r = rng_args(c, d_u);
+    tc::k_draw_labels<<<(unsigned)((c->N + 255) / 256), 256, 0, c->stream>>>(c->d_rbuf, c->d_rpart, c->N, K, final_,
+                                                                            r, c->d_labels);
+    DPMM_LAUNCHED();
+    int32_t h_err = 0;
+    DPMM_CUDA_TRY(cudaMemcpyAsync(&h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core multinomial label kernel: bounded wait expired (code " +
+                                                 std::to_string(h_err) + ")");
     return DPMM_OK;
 }
 
