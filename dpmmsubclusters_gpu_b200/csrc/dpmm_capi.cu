@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <unordered_map>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -214,6 +215,7 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     c->device = desc->device;
     c->N = desc->n_points;
     c->n_total = desc->n_points;
+    if (const char* e = std::getenv("DPMM_STATS_KERNEL")) c->stats_kernel = std::atoi(e) == 2 ? 2 : 1;
     c->D = desc->dim;
     c->prior = desc->prior_type;
     c->Dp = c->prior == DPMM_PRIOR_GAUSSIAN ? padded_dim(c->D) : mult_padded_dim(c->D);

@@ -61,8 +61,29 @@ def counts_shape(seed: int, n: int = 50_000, d: int = 1000, k: int = 50):
     return x, z
 
 
+def mixture_shape(seed: int, n: int, d: int, k: int, mean: str):
+    """The C2 / C5 generative shapes (evaluation only): means U(-20, 20)^D (C2) or N(0, 25 I) (C5),
+    covariances A A^T / D + 0.5 I, Dirichlet(1) (C2) or Dirichlet(2) (C5) weights."""
+    rng = np.random.default_rng(seed)
+    mus = rng.uniform(-20, 20, size=(k, d)) if mean == "uniform" else rng.normal(size=(k, d)) * 5.0
+    w = rng.dirichlet(np.full(k, 1.0 if mean == "uniform" else 2.0))
+    z = rng.choice(k, size=n, p=w)
+    x = np.empty((n, d))
+    for c in range(k):
+        a = rng.normal(size=(d, d))
+        idx = np.flatnonzero(z == c)
+        x[idx] = rng.multivariate_normal(mus[c], a @ a.T / d + 0.5 * np.eye(d), size=idx.size)
+    return x, z
+
+
 def log_run(kind: str, seed: int, init_clusters: int, iters: int):
-    if kind == "gaussian":
+    if kind in ("c2", "c5"):
+        x, _ = (mixture_shape(5000 + seed, 100_000, 32, 20, "uniform") if kind == "c2"
+                else mixture_shape(6000 + seed, 100_000, 64, 100, "normal"))
+        d = x.shape[1]
+        hyper = niw_hyperparams(1.0, np.zeros(d), d + 3.0, np.eye(d))
+        alpha, prior = 10.0, prior_type.Gaussian
+    elif kind == "gaussian":
         x, _ = gaussian_shape(1000 + seed)
         d = x.shape[1]
         hyper = niw_hyperparams(1.0, np.zeros(d), 5.0, np.eye(d))
@@ -91,6 +112,23 @@ def recall_at_top(groups, score, hr, top=TOP, thresh=-1.0):
     return (hits / total if total else float("nan")), int(total)
 
 
+def ranking_report(groups, score, hr, thresh=-1.0):
+    """How well a ranking finds the candidates worth an exact ratio (log ratio > thresh), per group
+    (run, iteration, kind): recall within the top k for k = 1 .. 16, and the exact evaluations needed to
+    reach every positive of a group (the rank of its last positive), summed over the groups."""
+    out = {f"recall_at_{k}": recall_at_top(groups, score, hr, top=k, thresh=thresh)[0] for k in (1, 2, 4, 8, 16)}
+    need = 0
+    for g in groups:
+        pos = hr[g] > thresh
+        if not pos.any():
+            continue
+        order = np.lexsort((g, -score[g]))
+        need += int(np.flatnonzero(pos[order]).max()) + 1
+    out["evaluations_to_reach_every_positive"] = need
+    out["candidates"] = int(sum(len(g) for g in groups if (hr[g] > thresh).any()))
+    return out
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=screen.HERE)
@@ -100,10 +138,16 @@ def main(argv=None):
     ap.add_argument("--dump", default=None, help="also write the logged rows to this .npz")
     args = ap.parse_args(argv)
     t0 = time.time()
-    plan = [("gaussian", s, ic, 100) for s, ic in enumerate([1, 4, 8, 16, 24, 32, 6, 12, 20, 28])]
-    plan += [("counts", s, ic, 60) for s, ic in enumerate([1, 10, 30, 60, 20])]
+    # training shapes (C1: D = 2 Gaussian; C3: D = 1000 counts), then evaluation-only shapes the network
+    # never sees in training (C2: D = 32; C5: D = 64): does the ranking carry over?
+    plan = [("gaussian", s, ic, 100) for s, ic in enumerate([1, 4, 8, 16, 24, 32, 6, 12, 20, 28, 2, 10, 14, 18, 26,
+                                                              30, 36, 40, 3, 22])]
+    plan += [("counts", s, ic, 60) for s, ic in enumerate([1, 10, 30, 60, 20, 5, 40, 80])]
+    evals = [("c2", s, ic, 60) for s, ic in enumerate([1, 8, 30])] + [("c5", s, ic, 40) for s, ic in enumerate([1, 50, 150])]
     if args.quick:
         plan = [("gaussian", 0, 8, 30), ("gaussian", 1, 16, 30), ("counts", 0, 10, 15)]
+        evals = [("c2", 0, 8, 20)]
+    plan = plan + evals
     runs = []
     for i, (kind, seed, ic, iters) in enumerate(plan):
         lg = log_run(kind, seed, ic, iters)
@@ -116,7 +160,9 @@ def main(argv=None):
         np.savez_compressed(args.dump, **{f"{k}_{i}": r[k] for i, r in enumerate(runs) for k in ("f", "hr", "k", "it")},
                             meta=np.array([[r["run"], r["seed"], r["init"], r["kind"] == "gaussian"] for r in runs]))
     rng = np.random.default_rng(args.seed)
-    held = set(rng.choice(len(runs), size=max(1, len(runs) // 5), replace=False).tolist())
+    train_idx = [i for i, r in enumerate(runs) if r["kind"] in ("gaussian", "counts")]
+    eval_idx = [i for i, r in enumerate(runs) if r["kind"] in ("c2", "c5")]
+    held = set(rng.choice(train_idx, size=max(1, len(train_idx) // 5), replace=False).tolist())
 
     def stack(sel):
         rs = [runs[i] for i in sel]
@@ -125,7 +171,7 @@ def main(argv=None):
         G = np.concatenate([r["run"] * 1_000_000 + r["it"] * 2 + r["k"] for r in rs])
         return F, HR, G
 
-    Ftr, HRtr, _ = stack([i for i in range(len(runs)) if i not in held])
+    Ftr, HRtr, _ = stack([i for i in train_idx if i not in held])
     Fte, HRte, Gte = stack(sorted(held))
     # rows far below acceptance carry one target value (-3); keep all rows near it and a share of the rest
     near = HRtr > -60
@@ -144,6 +190,19 @@ def main(argv=None):
     per_shape = {sh: {"trained": recall_at_top(gs, score, HRte)[0],
                       "proxy_feature_only": recall_at_top(gs, Fte[:, 2].astype(np.float64), HRte)[0],
                       "attainable_positives": recall_at_top(gs, score, HRte)[1]} for sh, gs in shape_g.items()}
+    # the rankings on the held-out runs of the training shapes and on the evaluation-only shapes
+    comparison = {}
+    for name, sel in [("held_out_C1_C3_shapes", sorted(held))] + [
+            (f"unseen_{sh}_shape", [i for i in eval_idx if runs[i]["kind"] == sh]) for sh in ("c2", "c5")]:
+        if not sel:
+            continue
+        F, HR, G = stack(sel)
+        gs = [np.flatnonzero(G == g) for g in np.unique(G)]
+        comparison[name] = {"trained": ranking_report(gs, screen.forward(F, params), HR),
+                            "proxy_feature_only": ranking_report(gs, F[:, 2].astype(np.float64), HR),
+                            "untrained_init": ranking_report(gs, screen.forward(F, p0), HR),
+                            "random_order": ranking_report(gs, rng.random(HR.size), HR),
+                            "rows": int(HR.size), "groups": len(gs)}
     os.makedirs(args.out, exist_ok=True)
     screen.save_params(params, os.path.join(args.out, "screen_params.f32"))
     report = {
@@ -156,11 +215,13 @@ def main(argv=None):
                                   "positive": "log ratio > -1", "groups": len(groups), "per_shape": per_shape,
                                   "definition": "hits / sum over groups of min(16, positives); group = "
                                                 "(run, iteration, kind)"},
+        "ranking_comparison": comparison,
         "seconds": round(time.time() - t0, 1),
     }
     with open(os.path.join(args.out, "screen_params.json"), "w") as fh:
         json.dump(report, fh, indent=1)
     print(json.dumps(report["held_out_recall_at_16"]), flush=True)
+    print(json.dumps(comparison), flush=True)
     print(f"[train] final loss {losses[-1]:.5f}, {report['seconds']} s", flush=True)
 
 

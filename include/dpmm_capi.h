@@ -126,7 +126,7 @@ typedef struct dpmm_shard {
 /* cudaKernel::init (cudaKernel.cu:537-635).  Unlike the reference it does not call
  * cudaDeviceReset, so several contexts (samplers) can share a device. */
 dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out);
-/* cudaKernel::release (cudaKernel.cu:691-720) */
+/* cudaKernel::release (cudaKernel.cu:720-749) */
 dpmm_status dpmm_destroy(dpmm_ctx* ctx);
 
 /* The H2D copy of the points inside cudaKernel::init (cudaKernel.cu:622-626).
