@@ -135,8 +135,10 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
         add("k_gauss_slot_stats", 10, "hbm", N * (2.0 * Dp * 4 + 12), "GB/s", hbm, "hbm_gbs",
             "N*(2*Dp*4 + 12) B per launch: every point read once per sub-cluster pass, permutation, "
             "sub-label; FP32 products N*Dp*(Dp+1)")
-    add("k_prune_draw", 9, "hbm", N * 12.0 + kept * N * Dp * 4, "GB/s", hbm, "hbm_gbs",
-        "N*12 B (permutation, r, label) + the points of chunks that keep other clusters")
+    add("k_prune_draw", 9, "hbm", N * 12.0, "GB/s", hbm, "hbm_gbs",
+        "N*12 B (permutation entry, own-cluster r, label) per launch: a lower bound, the rows of the few "
+        "chunks that keep other clusters (%.3f other clusters kept per point in the last attempt) are "
+        "not counted" % kept)
     return out
 
 
@@ -610,7 +612,7 @@ def main():
     if mult:
         kernels = mult_kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, pk, pk_src)
     else:
-        kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[2], pk, pk_src, tc)
+        kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[4], pk, pk_src, tc)
     # the roofline of the kernel with the most device time in the timed region
     dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
     roofline = dict(kernels[dominant], kernel=dominant) if dominant else None

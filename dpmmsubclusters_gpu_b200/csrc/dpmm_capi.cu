@@ -215,7 +215,6 @@ extern "C" dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out)
     c->device = desc->device;
     c->N = desc->n_points;
     c->n_total = desc->n_points;
-    if (const char* e = std::getenv("DPMM_STATS_KERNEL")) c->stats_kernel = std::atoi(e) == 2 ? 2 : 1;
     c->D = desc->dim;
     c->prior = desc->prior_type;
     c->Dp = c->prior == DPMM_PRIOR_GAUSSIAN ? padded_dim(c->D) : mult_padded_dim(c->D);

@@ -219,7 +219,6 @@ struct dpmm_ctx {
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
 
-    int stats_kernel = 1;          // tensor-core statistics kernel form (1: staged rows, 2: register prefetch)
     int stall_tc_mma = 0;          // test seam (dpmm_set_wait_test): tensor-core label kernels issue no products
 
     // sharding by points (dpmm_set_shard): the aggregates are summed over the ranks by `allreduce`

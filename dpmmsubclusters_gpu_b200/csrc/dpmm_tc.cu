@@ -1772,267 +1772,6 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     }
 }
 
-// Second form of the same statistics (same operands, products, groups and partial records): the rows of
-// tile t + 1 are gathered into registers while tile t is split into the operands, and the operands are
-// double-buffered, so the products of tile t - 1 run while tile t is built.  Each warp waits on the
-// mbarrier of the products two tiles back (the buffer it is about to overwrite) instead of a block
-// barrier: one block barrier per 32-point tile (operands complete before the products are issued).
-// Thread (warp w, lane l) holds features 32 g + 4 w + e (e < 4) of point l of the tile; the centre a
-// (mean of the chunk's first tile) is a warp reduction over the lanes.  Shared memory 105 KB (two CTAs
-// per SM).  Every wait is bounded and every abort is decided block-uniformly at the block barrier.
-template <int DP>
-struct Stat2Smem {
-    static constexpr int N = DP + 16;                                  // B rows
-    static constexpr size_t buf = 2 * 128 * 128 + 2 * (size_t)N * 128; // A hi, A lo, B hi, B lo of one tile
-    static constexpr size_t a_hi = 0, a_lo = 128 * 128, b_hi = 2 * 128 * 128, b_lo = b_hi + (size_t)N * 128;
-    static constexpr size_t bar = 2 * buf;                             // 2 mbarriers, tmem slot, flag
-    static constexpr size_t total = bar + 32 + 1024;
-    static_assert(buf % 1024 == 0 && b_lo % 1024 == 0, "swizzle atoms");
-};
-
-template <int DP>
-__global__ void __launch_bounds__(256, 2) k_slot_stats_tc2(
-    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
-    const int32_t* __restrict__ nchunks, const float* __restrict__ muv, const int32_t* __restrict__ sub,
-    double* __restrict__ part, const uint8_t* __restrict__ mask, int32_t* __restrict__ err)
-{
-    using L = Stat2Smem<DP>;
-    constexpr int N = L::N;
-    constexpr int SL = 1 + DP + tri(DP);
-    constexpr int G = DP / 32;                     // float4 per thread per row
-    constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
-    extern __shared__ uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-    uint64_t* bar = reinterpret_cast<uint64_t*>(smem + L::bar);   // [2]: products of tiles of parity 0 / 1
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 2);
-    volatile int* flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
-
-    const int ch = blockIdx.x;
-    if (ch >= *nchunks) return;
-    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
-    if (mask && !mask[k]) return;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const volatile int32_t* gerr = err;
-    const int ntiles = (len + ST_P - 1) / ST_P;
-
-    // both operand buffers zeroed once (rows past Dp stay zero), then the ones rows of B
-    for (int e = tid; e < (int)(2 * L::buf / 16); e += 256) reinterpret_cast<uint4*>(smem)[e] = make_uint4(0u, 0u, 0u, 0u);
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_init(bar + 1, 1);
-        *flag = 0;
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(ST_TMEM_COLS));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-    }
-    __syncthreads();
-    if (tid < 2 * ST_P)
-        *reinterpret_cast<float*>(smem + (tid >> 5) * L::buf + L::b_hi + sw128_offset32(DP, tid & 31)) = 1.0f;
-
-    const int fbase = 4 * warp;   // this thread's features 32 g + fbase + e
-    auto load_row = [&](int p, float4 (&v)[G], int& sl) {
-#pragma unroll
-        for (int g = 0; g < G; ++g)
-            v[g] = p >= 0 ? __ldg(reinterpret_cast<const float4*>(x + (size_t)p * DP + 32 * g + fbase))
-                          : make_float4(0.f, 0.f, 0.f, 0.f);
-        sl = p >= 0 ? __ldg(sub + p) : 0;
-    };
-    auto entry = [&](int t) -> int {
-        const int i = t * ST_P + lane;
-        return (t < ntiles && i < len) ? __ldg(perm + start + i) : -1;
-    };
-    float4 cur[G], nxt[G];
-    int scur = 0, snxt = 0;
-    load_row(entry(0), cur, scur);
-    int pn = entry(1);
-    // centre: mean of the first tile's points, per feature (a warp reduction: every lane holds it)
-    float sh[G][4];
-    {
-        const float inv = 1.0f / (float)max(1, min(ST_P, len));
-#pragma unroll
-        for (int g = 0; g < G; ++g) {
-            const float v4[4] = {cur[g].x, cur[g].y, cur[g].z, cur[g].w};
-#pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                float a = v4[e];
-#pragma unroll
-                for (int o = 16; o; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-                sh[g][e] = a * inv;
-            }
-        }
-    }
-
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    const uint32_t tmem_base = *tmem_slot;
-
-    // drain role: TMEM lane quarter q (accumulator rows 32 q ..), column half hc
-    const int q = warp & 3, hc = warp >> 2;
-    const int slot = q >> 1, fi = (q & 1) * 32 + lane;
-    const bool row_live = (q & 1) * 32 < DP;
-    const bool do_s = row_live && (DP > 32 ? (q & 1) <= hc : hc == 0);
-    const bool do_sum = row_live && hc == 0;
-    double acc[32];
-#pragma unroll
-    for (int m = 0; m < 32; ++m) acc[m] = 0.0;
-    double sacc = 0.0;
-    int cnt_l = 0, cnt_r = 0;
-    auto drain = [&](int g) {
-        const uint32_t base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((g & 1) * 128);
-        if (do_s) {
-            uint32_t v[32];
-            tmem_ld32(base + (uint32_t)(32 * hc), v);
-#pragma unroll
-            for (int m = 0; m < 32; ++m) acc[m] += (double)__uint_as_float(v[m]);
-        }
-        if (do_sum) {
-            uint32_t v1;
-            tmem_ld1(base + (uint32_t)DP, v1);
-            sacc += (double)__uint_as_float(v1);
-        }
-    };
-    // warp-uniform wait for the products of tile t; on expiry the error is recorded and the block stops
-    // at its next barrier
-    auto wait_tile = [&](int t) -> bool {
-        if (warp_wait_bounded(bar + (t & 1), (uint32_t)((t >> 1) & 1), gerr)) return true;
-        if (lane == 0) {
-            atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
-            *flag = 1;
-        }
-        return false;
-    };
-
-    bool failed = false;
-    int issued = -1;   // last tile whose products were issued
-#pragma unroll 1
-    for (int t = 0; t < ntiles; ++t) {
-        const int b = t & 1;
-        uint8_t* buf = smem + (size_t)b * L::buf;
-        // the next tile's rows and the entries of the one after are in flight while this tile is built
-        if (t + 1 < ntiles) load_row(pn, nxt, snxt);
-        const int pn2 = entry(t + 2);
-        const bool ok = t < 2 || wait_tile(t - 2);   // this buffer's previous products have completed
-        tc_fence_after();
-        if (ok) {
-            const bool in_l = scur == 1, in_r = scur == 2;
-            if (warp == 0) {
-                cnt_l += __popc(__ballot_sync(0xffffffffu, in_l));
-                cnt_r += __popc(__ballot_sync(0xffffffffu, in_r));
-            }
-#pragma unroll
-            for (int g = 0; g < G; ++g) {
-                const float cv[4] = {cur[g].x - sh[g][0], cur[g].y - sh[g][1], cur[g].z - sh[g][2],
-                                     cur[g].w - sh[g][3]};
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int f = 32 * g + fbase + e;
-                    const float hi = tf32_rna(cv[e]);
-                    const float lo = tf32_rna(cv[e] - hi);
-                    const uint32_t ob = sw128_offset32(f, lane), orr = ob + 64 * 128;
-                    *reinterpret_cast<float*>(buf + L::b_hi + ob) = hi;
-                    *reinterpret_cast<float*>(buf + L::b_lo + ob) = lo;
-                    *reinterpret_cast<float*>(buf + L::a_hi + ob) = in_l ? hi : 0.f;
-                    *reinterpret_cast<float*>(buf + L::a_lo + ob) = in_l ? lo : 0.f;
-                    *reinterpret_cast<float*>(buf + L::a_hi + orr) = in_r ? hi : 0.f;
-                    *reinterpret_cast<float*>(buf + L::a_lo + orr) = in_r ? lo : 0.f;
-                }
-            }
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        tc_fence_before();
-        __syncthreads();
-        if (*flag) {
-            failed = true;
-            break;
-        }
-        const int grp = t / ST_G;
-        if (tid == 0) {
-            tc_fence_after();
-            const uint32_t td = tmem_base + (uint32_t)((grp & 1) * 128);
-            const uint32_t first = (t % ST_G) == 0 ? 0u : 1u;   // a fresh accumulator per group
-            const uint64_t da_h = sw128_desc(smem_u32(buf + L::a_hi)), da_l = sw128_desc(smem_u32(buf + L::a_lo));
-            const uint64_t db_h = sw128_desc(smem_u32(buf + L::b_hi)), db_l = sw128_desc(smem_u32(buf + L::b_lo));
-#pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_h + 2 * ks, IDESC, ks != 0 ? 1u : first);
-#pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_l + 2 * ks, db_h + 2 * ks, IDESC, 1u);
-#pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_l + 2 * ks, IDESC, 1u);
-            umma_commit(bar + b);
-        }
-        issued = t;
-        // a new group: the previous group's accumulator is complete once tile t - 1's products are
-        if (t % ST_G == 0 && grp > 0 && wait_tile(t - 1)) {
-            tc_fence_after();
-            drain(grp - 1);
-        }
-        tc_fence_before();
-#pragma unroll
-        for (int g = 0; g < G; ++g) cur[g] = nxt[g];
-        scur = snxt;
-        pn = pn2;
-    }
-    if (!failed && ntiles > 0 && wait_tile(ntiles - 1)) {
-        tc_fence_after();
-        drain((ntiles - 1) / ST_G);
-    }
-    tc_fence_before();
-    __syncthreads();   // the operand buffers now hold the sums, counts and d for the move to mu_k
-    failed = failed || *flag;
-    double* xs = reinterpret_cast<double*>(smem);   // [2][DP] sums S1
-    double* xd = xs + 2 * DP;                        // [DP] d = a - mu_k
-    double* xn = xd + DP;                            // [2] counts
-    if (!failed) {
-        if (do_sum) xs[slot * DP + fi] = sacc;
-        if (lane < 4 * G) {   // lane 4 g + e of warp w writes feature 32 g + 4 w + e
-            const int g = lane >> 2, e = lane & 3, f = 32 * g + fbase + e;
-            float a = 0.f;
-#pragma unroll
-            for (int gg = 0; gg < G; ++gg)
-#pragma unroll
-                for (int ee = 0; ee < 4; ++ee)
-                    if (gg == g && ee == e) a = sh[gg][ee];
-            xd[f] = ntiles > 0 ? (double)a - (double)muv[(size_t)3 * k * DP + f] : 0.0;
-        }
-        if (tid == 0) {
-            xn[0] = (double)cnt_l;
-            xn[1] = (double)cnt_r;
-        }
-    }
-    __syncthreads();
-    if (!failed) {
-        double* out = part + (size_t)ch * 2 * SL;
-        if (tid < 2) out[(size_t)tid * SL] = xn[tid];
-        const double n = xn[slot];
-        if (do_s) {
-            double* po = out + (size_t)slot * SL + 1 + DP;
-            const double di = xd[fi], si = xs[slot * DP + fi];
-#pragma unroll
-            for (int m = 0; m < 32; ++m) {
-                const int j = 32 * hc + m;
-                if (fi <= j && j < DP) {
-                    const double dj = xd[j], sj = xs[slot * DP + j];
-                    po[tri_index(DP, fi, j)] = acc[m] + di * sj + si * dj + n * di * dj;
-                }
-            }
-        }
-        if (do_sum) out[(size_t)slot * SL + 1 + fi] = sacc + n * xd[fi];
-    }
-    if (failed && tid == 0 && issued >= 0)   // nothing in flight at dealloc
-        mbar_wait_bounded(bar + (issued & 1), (uint32_t)((issued >> 1) & 1), nullptr);
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-        tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ST_TMEM_COLS));
-    }
-}
-
 }  // namespace tc
 
 constexpr size_t kTcSmemCap = 227 * 1024;
@@ -2195,15 +1934,6 @@ bool tc_stats_supported(const dpmm_ctx* c)
 template <int DP>
 static dpmm_status launch_slot_stats_tc_t(dpmm_ctx* c, const uint8_t* d_mask, int32_t* err)
 {
-    if (c->stats_kernel == 2) {
-        auto kern2 = tc::k_slot_stats_tc2<DP>;
-        constexpr size_t sm2 = tc::Stat2Smem<DP>::total;
-        DPMM_CUDA_TRY(cudaFuncSetAttribute(kern2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
-        kern2<<<c->max_chunks, 256, sm2, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu, c->d_sub,
-                                                      c->d_part, d_mask, err);
-        DPMM_LAUNCHED();
-        return DPMM_OK;
-    }
     auto kern = tc::k_slot_stats_tc<DP>;
     constexpr size_t sm = tc::StatSmem<DP>::total;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

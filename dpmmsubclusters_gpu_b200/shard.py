@@ -106,11 +106,13 @@ class LocalGroupExchange:
     buffer is copied to the host, the sums are formed in rank order (so every rank gets the same
     values) and copied back.  device=False: the buffers are host memory."""
 
-    def __init__(self, world: int, device: bool = True):
+    def __init__(self, world: int, device: bool = True, timeout: float = 300.0):
         self.world = world
         self.device = device
         self._rt = _cudart() if device else None
-        self._barrier = threading.Barrier(world)
+        # a rank that never arrives (it failed, or took another path) breaks the exchange after `timeout`
+        # seconds: the waiting ranks' samplers then report DPMM_ERR_EXCHANGE instead of waiting forever
+        self._barrier = threading.Barrier(world, timeout=timeout)
         self._parts = [None] * world
         self._sum = None
         self.ranks = [self._Rank(self, r) for r in range(world)]
