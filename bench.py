@@ -143,7 +143,7 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
 
 
 def c3_config(args):
-    return dict(prior="multinomial", N=1_000_000, D=1000, K_true=50, alpha=10.0, prior_alpha=1.0, iterations=150,
+    return dict(prior="multinomial", N=args.c3_n, D=1000, K_true=50, alpha=10.0, prior_alpha=1.0, iterations=150,
                 burnout=15, theta_dirichlet=0.1, length_mean=200.0)
 
 
@@ -551,6 +551,7 @@ def main():
                          "NMI and final cluster count over 10 sampler seeds, mixed vs plain FP32")
     ap.add_argument("--study-seeds", type=int, default=10)
     ap.add_argument("--study-shapes", default="c5r,c2", help="comma list of c5r (C5 at N=1e6) and c2")
+    ap.add_argument("--c3-n", type=int, default=1_000_000, help="points of the multinomial workload")
     ap.add_argument("--c4-sets", type=int, default=256)
     ap.add_argument("--c4-seq-sets", type=int, default=32, help="data sets timed one at a time (a subset)")
     args = ap.parse_args()
