@@ -69,6 +69,7 @@ NCU_TRAFFIC = {
     "k_gauss_labels_tc": {"dram_bytes": 619413504, "points": 1_000_000, "clusters": 95},
     "k_prune_scan1_tc": {"dram_bytes": 270950144, "points": 1_000_000},
     "k_slot_stats_tc": {"dram_bytes": 290109952, "points": 1_000_000},
+    "k_mult_labels_tc": {"dram_bytes": 417898240, "points": 200_000},
 }
 
 
@@ -135,7 +136,7 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
         add("k_gauss_slot_stats", 10, "hbm", N * (2.0 * Dp * 4 + 12), "GB/s", hbm, "hbm_gbs",
             "N*(2*Dp*4 + 12) B per launch: every point read once per sub-cluster pass, permutation, "
             "sub-label; FP32 products N*Dp*(Dp+1)")
-    add("k_prune_draw", 9, "hbm", N * 12.0, "GB/s", hbm, "hbm_gbs",
+    add("k_prune_settle+k_prune_draw", 9, "hbm", N * 12.0, "GB/s", hbm, "hbm_gbs",
         "N*12 B (permutation entry, own-cluster r, label) per launch: a lower bound, the rows of the few "
         "chunks that keep other clusters (%.3f other clusters kept per point in the last attempt) are "
         "not counted" % kept)
@@ -181,7 +182,7 @@ def mult_kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, pk, pk_src):
         work = N * (2.0 * Dk + 4.0 * k_mean + 16.0)
         ach = work / (ms / 1e3) / 1e9
         out["k_mult_labels_tc"] = {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                                   "traffic": None, "launch_ms": ms, "launches": int(ph_calls[7]),
+                                   "traffic": per_point_traffic("k_mult_labels_tc", N) if D == 1000 else None, "launch_ms": ms, "launches": int(ph_calls[7]),
                                    "total_ms": ph_ms[7], "peak_source": f"hbm_gbs of {pk_src}",
                                    "algorithmic": "N*(2*Dk + 4*K + 16) B per launch: BF16 counts (Dk = D padded to "
                                                   "64), r written cluster-major, the draw's partials; tensor-core "
