@@ -94,10 +94,11 @@ def padded(d):
     return p
 
 
-def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
+def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc, fused=False):
     """Per timed kernel (CUDA events around each launch on its stream): algorithmic work per launch,
     achieved rate and the fraction of the measured peak of its bound.  tc: the pruned scan and the
-    sub-cluster statistics ran on the tensor cores (padded dimension 32 / 64, mixed mode)."""
+    sub-cluster statistics ran on the tensor cores (padded dimension 32 / 64, mixed mode); fused: the
+    sub-labels and statistics ran as one kernel (k_sub_stats_tc, timed in the statistics slot)."""
     Dp = padded(D)
     hbm = pk.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
     bf16 = pk.get("bf16_tflops", FALLBACK_PEAKS["bf16_tflops"])
@@ -125,10 +126,16 @@ def kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, kept, pk, pk_src, tc):
             "tensor-core products 3 x 2*N*Dp*(64 + K - 1) FLOP (one pass: r_h and every cluster's bound "
             "direction)",
             per_point_traffic("k_prune_scan1_tc", N) if Dp == 64 and one_pass else None)
-        add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
-            "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
-            "split-TF32 Gram products 3 x 2*N*128*(Dp+16) FLOP",
-            per_point_traffic("k_slot_stats_tc", N) if Dp == 64 else None)
+        if fused:
+            add("k_sub_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
+                "N*(Dp*4 + 8) B per launch: every point gathered once (its row), its permutation index read "
+                "and its sub-label written; tensor-core products 3 x 2*N*128*64 FLOP (sub-labels, split BF16) "
+                "+ 3 x 2*N*128*(Dp+32) FLOP (statistics, split TF32)")
+        else:
+            add("k_slot_stats_tc", 10, "hbm", N * (Dp * 4.0 + 8), "GB/s", hbm, "hbm_gbs",
+                "N*(Dp*4 + 8) B per launch: every point, its permutation index and sub-label read once; "
+                "split-TF32 Gram products 3 x 2*N*128*(Dp+32) FLOP",
+                per_point_traffic("k_slot_stats_tc", N) if Dp == 64 else None)
     else:
         add("k_prune_scan", 8, "hbm", N * (2.0 * Dp * 4 + 8), "GB/s", hbm, "hbm_gbs",
             "N*(2*Dp*4 + 8) B per launch: every point read twice (its own cluster's r, then the per-point "
@@ -463,6 +470,8 @@ def run_arm(arm, args, cfg, x, z_np, rank, local, dist, L, clocks=False, shard=N
     else:
         check(L.dpmm_sampler_create(ctypes.byref(rd), N, D, ctypes.c_void_p(x.data_ptr()), 1, ctypes.byref(h)))
     ctx = L.dpmm_sampler_context(h)
+    if args.fuse:
+        check(L.dpmm_set_fused_sub_stats(ctx, 1))
     stream = torch.cuda.ExternalStream(L.dpmm_sampler_stream(h), device=f"cuda:{local}")
     t0 = time.perf_counter()
     check(L.dpmm_sampler_step(h, args.burnin + args.warmup))
@@ -540,6 +549,8 @@ def main():
                          "the per-cluster statistics with NCCL (default), or run N independent replicas")
     ap.add_argument("--ablation", action="store_true",
                     help="also time every intermediate arm (one change at a time) and report them")
+    ap.add_argument("--fuse", action="store_true",
+                    help="sub-labels and their statistics in one fused pass (k_sub_stats_tc) instead of two kernels")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--ref-points-per-core", type=int, default=600)
@@ -614,7 +625,7 @@ def main():
     if mult:
         kernels = mult_kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, pk, pk_src)
     else:
-        kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[4], pk, pk_src, tc)
+        kernels = kernel_rooflines(ph_ms, ph_calls, N, D, k_mean, prune[4], pk, pk_src, tc, tc and args.fuse)
     # the roofline of the kernel with the most device time in the timed region
     dominant = max(kernels, key=lambda k: kernels[k]["total_ms"]) if kernels else None
     roofline = dict(kernels[dominant], kernel=dominant) if dominant else None
@@ -649,6 +660,8 @@ def main():
                                                  "generating model has (the reference's default is 1)"
                                                  if args.initial_clusters > 1 else "the reference's default"),
                        "burnin_iterations": args.burnin,
+                       "sub_labels_and_statistics": ("one fused pass (--fuse)" if args.fuse else
+                                                     "two kernels (k_sub_labels_tc, k_slot_stats_tc)"),
                        "clusters_in_timed_steps": ks,
                        "l2": "inputs (N*D*4 = %.2f GB) larger than L2" % (N * D * 4 / 1e9),
                        "nmi_vs_generating_labels": r["nmi"],

@@ -154,6 +154,7 @@ SIGNATURES = {
     "dpmm_get_gaussian_params": (c_int, [_CTX, c_int, _PF, _PF, _PF, _PF]),
     "dpmm_get_multinomial_params": (c_int, [_CTX, c_int, _PF]),
     "dpmm_set_wait_test": (c_int, [_CTX, c_int32]),
+    "dpmm_set_fused_sub_stats": (c_int, [_CTX, c_int32]),
     "dpmm_set_label_pruning": (c_int, [_CTX, c_double]),
     "dpmm_label_pruning_stats": (c_int, [_CTX, _PD]),
     "dpmm_set_ground_truth": (c_int, [_CTX, _PI32]),

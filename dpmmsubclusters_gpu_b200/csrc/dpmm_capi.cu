@@ -512,6 +512,13 @@ extern "C" dpmm_status dpmm_set_wait_test(dpmm_ctx* c, int32_t stall)
     return DPMM_OK;
 }
 
+extern "C" dpmm_status dpmm_set_fused_sub_stats(dpmm_ctx* c, int32_t on)
+{
+    if (!c) return fail(DPMM_ERR_INVALID_ARG, "null context");
+    c->fuse_sub_stats = on != 0;
+    return DPMM_OK;
+}
+
 extern "C" dpmm_status dpmm_set_shard(dpmm_ctx* c, const dpmm_shard* sh)
 {
     if (!c || !sh) return fail(DPMM_ERR_INVALID_ARG, "null argument");

@@ -220,6 +220,7 @@ struct dpmm_ctx {
     size_t h_pinned_bytes = 0;
 
     int stall_tc_mma = 0;          // test seam (dpmm_set_wait_test): tensor-core label kernels issue no products
+    int fuse_sub_stats = 0;        // sub-labels and statistics in one pass (dpmm_set_fused_sub_stats)
 
     // sharding by points (dpmm_set_shard): the aggregates are summed over the ranks by `allreduce`
     int shard_world = 1, shard_rank = 0;
@@ -359,6 +360,8 @@ dpmm_status launch_prune_scan_tc(dpmm_ctx* c, int K, int32_t* d_err);
 // sub-cluster statistics (sub-labels given) on the tensor cores (dpmm_tc.cu; Dp = 32 or 64)
 bool tc_stats_supported(const dpmm_ctx* c);
 dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask);
+bool tc_sub_stats_supported(const dpmm_ctx* c);
+dpmm_status launch_sub_stats_tc(dpmm_ctx* c, RngArgs r, float* d_rout);
 
 RngArgs rng_args(dpmm_ctx* c, const float* d_ucaller);
 // In-place sum over the shards of `count` doubles at d_buf (device, written on the context's stream);

@@ -1687,6 +1687,11 @@ dpmm_status launch_sub_labels_and_stats(dpmm_ctx* c, int K, const float* d_u, fl
 {
     if (c->perm_K != K) DPMM_TRY(build_permutation(c, K));
     RngArgs r = rng_args(c, d_u);
+    if (draw && !d_mask && tc_sub_stats_supported(c)) {
+        // sub-labels and their statistics in one pass over the points (one gather of each row)
+        DPMM_TRY(launch_sub_stats_tc(c, r, d_rout));
+        return launch_stats_finalize(c, K, d_mask);
+    }
     if (draw && !d_mask && tc_sub_supported(c)) {
         // sub-labels on the tensor cores, then the statistics of the drawn sub-labels
         // its error word is read in the statistics launch's sync when that runs on the tensor cores

@@ -114,16 +114,35 @@ __device__ __forceinline__ bool mbar_test_wait(uint64_t* bar, uint32_t parity)
     return ok != 0;
 }
 
+// Potentially blocking probe: the thread may sleep until the phase completes, for at most about
+// `ns` nanoseconds (the suspend-time hint), instead of returning at once and spinning.
+__device__ __forceinline__ bool mbar_try_wait_sleep(uint64_t* bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
 // Single-thread bounded wait.  Gives up after WAIT_LIMIT_NS, or early when another CTA of the
-// launch has already reported an error (gerr != nullptr).
+// launch has already reported an error (gerr != nullptr).  Between non-blocking probes the thread
+// backs off with nanosleep (32 ns growing to 256 ns), so that waiting warps do not fill the issue
+// slots and the barrier / timer pipes that the working warps need.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, const volatile int32_t* gerr)
 {
     if (mbar_test_wait(bar, parity)) return true;
-    if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = global_ns();
+    uint32_t sleep = 32;
     for (uint32_t i = 1;; ++i) {
-        if (mbar_try_wait(bar, parity)) return true;
-        if ((i & 255) == 0) {
+        __nanosleep(sleep);
+        if (mbar_test_wait(bar, parity)) return true;
+        if (sleep < 256) sleep <<= 1;
+        if ((i & 63) == 0) {
             if (global_ns() - t0 > WAIT_LIMIT_NS) return false;
             if (gerr && *gerr) return false;
         }
@@ -210,6 +229,21 @@ __device__ __forceinline__ void bf16_split(float v, __nv_bfloat16& hi, __nv_bflo
 {
     hi = __float2bfloat16_rn(v);
     lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+}
+
+__device__ __forceinline__ uint32_t bf16x2_bits(__nv_bfloat162 v)
+{
+    return (uint32_t)__bfloat16_as_ushort(v.x) | ((uint32_t)__bfloat16_as_ushort(v.y) << 16);
+}
+
+// bf16_split of four values, packed: hi and lo as 4 x BF16 (8 bytes) each
+__device__ __forceinline__ void bf16_split4(float a, float b, float c, float d, uint2& hi, uint2& lo)
+{
+    const __nv_bfloat162 h01 = __floats2bfloat162_rn(a, b), h23 = __floats2bfloat162_rn(c, d);
+    const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+    hi = make_uint2(bf16x2_bits(h01), bf16x2_bits(h23));
+    lo = make_uint2(bf16x2_bits(__floats2bfloat162_rn(a - f01.x, b - f01.y)),
+                    bf16x2_bits(__floats2bfloat162_rn(c - f23.x, d - f23.y)));
 }
 
 // ------------------------------------------------------------------------- B packing
@@ -1441,11 +1475,17 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
 // Statistics of the two sub-clusters of one chunk (cluster k, sub-labels given) on the tensor
 // cores, Dp = 32 or 64: count, sum c and the upper triangle of sum c c^T over each sub-cluster's
 // points, c = x - mu_k (mu_k the cluster's mean parameter), the partial records of
-// k_gauss_slot_stats (dpmm_kernels.cu).  Per tile of 32 points:
-//   A (128 rows x 32 points, K-major TF32)  row i < Dp: c_i where the sub-label is 1, else 0;
-//                                           row 64 + i: c_i where it is 2
-//   B (Dp + 16 rows x 32 points)            row j < Dp: c_j; row Dp: ones; the rest zero
-//   D = A B^T (M = 128, N = Dp + 16)        D[64 s + i][j] = sum c_i c_j, D[64 s + i][Dp] = sum c_i
+// k_gauss_slot_stats (dpmm_kernels.cu).  Per tile of 32 points (the contraction dimension K):
+//   A (M = 128 x K, MN-major TF32)   column 64 s + i, point p: c_i(p) where p's sub-label is s + 1,
+//                                    else 0 (columns Dp .. 63 of each half stay 0)
+//   B (N = Dp + 32 x K, MN-major)    column j < Dp: c_j(p); column Dp: 1; the rest 0
+//   D = A B^T                        D[64 s + i][j] = sum c_i c_j, D[64 s + i][Dp] = sum c_i
+// MN-major means the operand is stored point by point: each point's row is its features, in
+// 128-byte rows of 32 features.  TF32 MN-major operands take the 128-byte swizzle with 32-byte
+// atomicity (the one MN-major layout the tensor cores accept for TF32): an atom is 4 points x 128 B,
+// its 32-byte pieces XOR-permuted by the point's row (0..3); atoms along M / N at 512 B, groups of 4
+// points at 4 x 512 B for A and (Dp + 32) / 32 x 512 B for B.  A row is built from the staged FP32
+// row with 16-byte stores.  The ones column lives in B's last atom, written once.
 // The operands are split TF32 (hi = rna(c), lo = rna(c - hi), |c - hi - lo| <= 2^-22 |c|) and
 // D = A_hi B_hi + A_lo B_hi + A_hi B_lo (12 tcgen05.mma of K = 8).  The accumulator runs over a
 // group of ST_G tiles (FP32 over 256 points: 96 accumulator roundings) and is then added into FP64
@@ -1454,10 +1494,10 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
 // totals moved to mu_k in FP64 at the end:
 //   sum (x-mu)(x-mu)^T = S_a + d S1^T + S1 d^T + n d d^T,  sum (x-mu) = S1 + n d,  d = a - mu.
 // Pipeline: tile t + 3's rows and sub-labels (gathered through permutation entries that were
-// staged three tiles earlier, all by cp.async) are in flight while tile t is split and transposed
-// into the operands; a group's accumulator is drained while the next group's MMAs run.  Every wait
-// is bounded.
-constexpr int ST_P = 32;                   // points per tile: one 128-byte TF32 K row
+// staged three tiles earlier, all by cp.async) are in flight while tile t is split into the
+// operands; a group's accumulator is drained while the next group's MMAs run.  Every wait is
+// bounded.
+constexpr int ST_P = 32;                   // points per tile (K of the contraction)
 constexpr int ST_STAGES = 4;               // staged tiles of rows (3 in flight)
 constexpr int ST_PERM = 8;                 // staged tiles of permutation entries
 constexpr int ST_G = 8;                    // tiles per accumulation group
@@ -1465,13 +1505,14 @@ constexpr uint32_t ST_TMEM_COLS = 256;     // two accumulators, at columns 0 and
 
 template <int DP>
 struct StatSmem {
-    static constexpr int N = DP + 16;                                   // B rows
+    static constexpr int NA = DP / 32 + 1;                              // B atoms: features, then ones
+    static constexpr int N = NA * 32;                                   // B columns (N of the MMA)
     static constexpr int SX = DP + 4;                                   // staged row stride (floats)
-    static constexpr size_t a_hi = 0;                                   // 128 rows x 128 B
-    static constexpr size_t a_lo = a_hi + 128 * 128;
-    static constexpr size_t b_hi = a_lo + 128 * 128;                    // N rows x 128 B
-    static constexpr size_t b_lo = b_hi + (size_t)N * 128;
-    static constexpr size_t stage = b_lo + (size_t)N * 128;             // [ST_STAGES][ST_P][SX] floats
+    static constexpr size_t a_hi = 0;                                   // 4 groups x 4 atoms x 1 KB
+    static constexpr size_t a_lo = a_hi + 16384;
+    static constexpr size_t b_hi = a_lo + 16384;                        // 4 groups x NA atoms x 1 KB
+    static constexpr size_t b_lo = b_hi + (size_t)NA * 4096;
+    static constexpr size_t stage = b_lo + (size_t)NA * 4096;           // [ST_STAGES][ST_P][SX] floats
     static constexpr size_t ssub = stage + (size_t)ST_STAGES * ST_P * SX * 4;   // [ST_STAGES][ST_P] ints
     static constexpr size_t sperm = ssub + (size_t)ST_STAGES * ST_P * 4;        // [ST_PERM][ST_P] ints
     static constexpr size_t shift = sperm + (size_t)ST_PERM * ST_P * 4;         // [DP] floats
@@ -1479,10 +1520,27 @@ struct StatSmem {
     static constexpr size_t total = bar + 32 + 1024;                    // + alignment slack
 };
 
-// byte offset of 4-byte element k of row r in a K-major tile with 128-byte swizzle
-__host__ __device__ constexpr uint32_t sw128_offset32(int row, int k)
+// Shared-memory descriptor of an MN-major TF32 operand with the 128-byte swizzle of 32-byte atomicity:
+// atoms of 4 rows (K) x 128 B (32 elements of M / N) 512 B apart along M / N (leading byte offset),
+// groups of 4 rows sbo bytes apart along K (stride byte offset).
+__device__ __forceinline__ uint64_t sw128b32_mn_desc(uint32_t saddr, uint32_t sbo)
 {
-    return (uint32_t)((row >> 3) * 1024 + (row & 7) * 128 + ((((k >> 2) ^ (row & 7)) & 7) << 4) + (k & 3) * 4);
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);
+    d |= (uint64_t)(512 >> 4) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    d |= (uint64_t)1 << 61;   // 128-byte swizzle, 32-byte atomicity
+    return d;
+}
+
+// byte offset of the 16-byte piece j4 (elements 4 j4 .. 4 j4 + 3 of M / N) of row p (K) in such an
+// operand whose groups of 4 rows hold `atoms` atoms; the piece's atom is (j4 >> 3) + atom0
+__device__ __forceinline__ uint32_t mn32_offset(int p, int j4, int atom0, int atoms)
+{
+    const int r = p & 3;
+    return (uint32_t)((p >> 2) * atoms * 512 + ((j4 >> 3) + atom0) * 512 + r * 128 + ((((j4 & 7) >> 1) ^ r) << 5) +
+                      ((j4 & 1) << 4));
 }
 
 // round to TF32 (10 explicit mantissa bits), nearest with ties away from zero: add half of the
@@ -1526,6 +1584,13 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
+// the barrier receives one arrival once every cp.async this thread issued so far has landed (its
+// expected count includes these arrivals)
+__device__ __forceinline__ void cp_async_mbar_arrive(uint64_t* bar)
+{
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 template <int DP>
 __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
@@ -1533,12 +1598,15 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     double* __restrict__ part, const uint8_t* __restrict__ mask, int32_t* __restrict__ err)
 {
     using L = StatSmem<DP>;
-    constexpr int N = L::N, SX = L::SX;
+    constexpr int N = L::N, NA = L::NA, SX = L::SX;
     constexpr int SL = 1 + DP + tri(DP);
     constexpr int C4 = DP / 4;                     // float4 per row
     constexpr int ITEMS = ST_P * C4 / 256;         // row pieces per thread per tile
-    static_assert(ITEMS >= 1 && ST_P * C4 % 256 == 0, "tile shape");
-    constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    static_assert(ITEMS >= 1 && ST_P * C4 % 256 == 0 && 256 % C4 == 0, "tile shape");
+    // F32 accumulator, TF32 A and B, both MN-major, M = 128
+    constexpr uint32_t IDESC = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+                               ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    constexpr uint32_t A_GROUP = 4096, B_GROUP = NA * 1024;   // bytes per 8 points (two groups of 4)
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     float* stage = reinterpret_cast<float*>(smem + L::stage);
@@ -1570,7 +1638,8 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     __syncthreads();
-    if (tid < ST_P) *reinterpret_cast<float*>(smem + L::b_hi + sw128_offset32(DP, tid)) = 1.0f;
+    if (tid < ST_P)   // the ones column: element 0 of B's last atom in every point's row (hi part)
+        *reinterpret_cast<float*>(smem + L::b_hi + mn32_offset(tid, 0, NA - 1, NA)) = 1.0f;
 
     // loader pieces (cp.async; the caller commits)
     auto issue_perm = [&](int t) {   // permutation entries of tile t (threads 0..31; 0 past the chunk)
@@ -1611,8 +1680,13 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = *tmem_slot;
-    const uint64_t da_h = sw128_desc(smem_u32(smem + L::a_hi)), da_l = sw128_desc(smem_u32(smem + L::a_lo));
-    const uint64_t db_h = sw128_desc(smem_u32(smem + L::b_hi)), db_l = sw128_desc(smem_u32(smem + L::b_lo));
+    const uint64_t da_h = sw128b32_mn_desc(smem_u32(smem + L::a_hi), A_GROUP / 2);
+    const uint64_t da_l = sw128b32_mn_desc(smem_u32(smem + L::a_lo), A_GROUP / 2);
+    const uint64_t db_h = sw128b32_mn_desc(smem_u32(smem + L::b_hi), B_GROUP / 2);
+    const uint64_t db_l = sw128b32_mn_desc(smem_u32(smem + L::b_lo), B_GROUP / 2);
+    // operand pieces of this thread: point tid / C4 + (256 / C4) u, features 4 (tid % C4) ..
+    const int j4 = tid % C4;
+    float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);   // its four centre coordinates (set at tile 0)
 
     // drain role: TMEM lane quarter q (accumulator rows 32 q ..), column half hc
     const int q = warp & 3, hc = warp >> 2;
@@ -1666,6 +1740,7 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
                 sshift[tid] = a / (float)nv;
             }
             __syncthreads();
+            s4 = *reinterpret_cast<const float4*>(sshift + 4 * j4);
         }
         tc_fence_after();
         issue_rows(t + 3);
@@ -1673,31 +1748,44 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
         cp_async_commit();
         {
             const float* sb = stage + (size_t)(t % ST_STAGES) * ST_P * SX;
-            const int sv = ssub[(t % ST_STAGES) * ST_P + lane];
-            const bool in_l = sv == 1, in_r = sv == 2;
+            const int32_t* sbs = ssub + (t % ST_STAGES) * ST_P;
             if (warp == 0) {
-                const unsigned bl = __ballot_sync(0xffffffffu, in_l), br = __ballot_sync(0xffffffffu, in_r);
+                const int sv = sbs[lane];
+                const unsigned bl = __ballot_sync(0xffffffffu, sv == 1), br = __ballot_sync(0xffffffffu, sv == 2);
                 cnt_l += __popc(bl);
                 cnt_r += __popc(br);
             }
+            // one 16-byte piece of a point's row per item: split, then stored into the side's half of
+            // A (zeros into the other half) and into B; a point past the chunk (sub-label 0) is all zero
 #pragma unroll
-            for (int g = 0; g < DP / 32; ++g) {
-                const float4 v4 = *reinterpret_cast<const float4*>(sb + lane * SX + 32 * g + 4 * warp);
-                const float4 s4 = *reinterpret_cast<const float4*>(sshift + 32 * g + 4 * warp);
+            for (int u = 0; u < ITEMS; ++u) {
+                const int p = tid / C4 + (256 / C4) * u;
+                const int sv = sbs[p];
+                const float4 v4 = *reinterpret_cast<const float4*>(sb + p * SX + 4 * j4);
                 const float cv[4] = {v4.x - s4.x, v4.y - s4.y, v4.z - s4.z, v4.w - s4.w};
+                float hi[4], lo[4];
+                const bool live = sv == 1 || sv == 2;
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
-                    const int f = 32 * g + 4 * warp + e;
-                    const float hi = tf32_rna(cv[e]);
-                    const float lo = tf32_rna(cv[e] - hi);
-                    const uint32_t ob = sw128_offset32(f, lane), orr = sw128_offset32(64 + f, lane);
-                    *reinterpret_cast<float*>(smem + L::b_hi + ob) = hi;
-                    *reinterpret_cast<float*>(smem + L::b_lo + ob) = lo;
-                    *reinterpret_cast<float*>(smem + L::a_hi + ob) = in_l ? hi : 0.f;
-                    *reinterpret_cast<float*>(smem + L::a_lo + ob) = in_l ? lo : 0.f;
-                    *reinterpret_cast<float*>(smem + L::a_hi + orr) = in_r ? hi : 0.f;
-                    *reinterpret_cast<float*>(smem + L::a_lo + orr) = in_r ? lo : 0.f;
+                    hi[e] = tf32_rna(cv[e]);
+                    lo[e] = tf32_rna(cv[e] - hi[e]);
+                    if (!live) hi[e] = lo[e] = 0.f;
                 }
+                const int side = sv == 2 ? 1 : 0;
+                const uint32_t a_c = mn32_offset(p, j4, 2 * side, 4);
+                const uint32_t a_z = mn32_offset(p, j4, 2 * (1 - side), 4);
+                const uint32_t b_o = mn32_offset(p, j4, 0, NA);
+                const uint4 h4 = make_uint4(__float_as_uint(hi[0]), __float_as_uint(hi[1]), __float_as_uint(hi[2]),
+                                            __float_as_uint(hi[3]));
+                const uint4 l4 = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
+                                            __float_as_uint(lo[3]));
+                const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+                *reinterpret_cast<uint4*>(smem + L::a_hi + a_c) = h4;
+                *reinterpret_cast<uint4*>(smem + L::a_lo + a_c) = l4;
+                *reinterpret_cast<uint4*>(smem + L::a_hi + a_z) = z4;
+                *reinterpret_cast<uint4*>(smem + L::a_lo + a_z) = z4;
+                *reinterpret_cast<uint4*>(smem + L::b_hi + b_o) = h4;
+                *reinterpret_cast<uint4*>(smem + L::b_lo + b_o) = l4;
             }
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1709,11 +1797,14 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
             const uint32_t td = tmem_base + (uint32_t)((grp & 1) * 128);
             const uint32_t first = (t % ST_G) == 0 ? 0u : 1u;   // a fresh accumulator per group
 #pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_h + 2 * ks, IDESC, ks != 0 ? 1u : first);
+            for (int ks = 0; ks < ST_P / 8; ++ks)   // one group of 8 points per MMA (K = 8)
+                umma_tf32(td, da_h + (A_GROUP >> 4) * ks, db_h + (B_GROUP >> 4) * ks, IDESC, ks != 0 ? 1u : first);
 #pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_l + 2 * ks, db_h + 2 * ks, IDESC, 1u);
+            for (int ks = 0; ks < ST_P / 8; ++ks)
+                umma_tf32(td, da_l + (A_GROUP >> 4) * ks, db_h + (B_GROUP >> 4) * ks, IDESC, 1u);
 #pragma unroll
-            for (int ks = 0; ks < ST_P / 8; ++ks) umma_tf32(td, da_h + 2 * ks, db_l + 2 * ks, IDESC, 1u);
+            for (int ks = 0; ks < ST_P / 8; ++ks)
+                umma_tf32(td, da_h + (A_GROUP >> 4) * ks, db_l + (B_GROUP >> 4) * ks, IDESC, 1u);
             umma_commit(bar);
         }
         pending = t;
@@ -1769,6 +1860,541 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     if (warp == 0) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(ST_TMEM_COLS));
+    }
+}
+
+
+// ------------------------------------------------------------------------- fused sub-labels + statistics
+// One pass over the points of a chunk (cluster k, label order) for both steps that follow the label
+// phase: the sub-cluster labels (cudaKernel.cu create_subclusters_labels, :1299-1398) and then the
+// sub-cluster statistics of the drawn labels (niw::create_sufficient_statistics per slot); each point's
+// row is gathered from HBM once.  Per super-tile of 128 points:
+//   sub-labels   the rows (split BF16, K-major, a point per row) times the cluster's [W_l | W_r] tile
+//                give z for both sub-clusters (the 12 tcgen05.mma of k_sub_labels_tc); one thread per
+//                point drains r_l and r_r and draws its sub-label;
+//   statistics   8 tiles of 16 points feed the split-TF32 Gram products of k_slot_stats_tc
+//                (MN-major operands, 6 tcgen05.mma of K = 8 per tile) into an FP32 accumulator of
+//                256 points, added into FP64 registers per group.
+// Warp roles (320 threads; the shared memory holds one CTA per SM), three chains that overlap:
+//   warp 0       loader: the permutation entries, then the rows into a three-slot stage by 16-byte
+//                cp.async (a warp instruction copies whole rows; per-row bulk copies measured several
+//                times slower for 256-byte rows); the cluster's B tile once per chunk;
+//   warp 1       MMA issuer (one thread): services whichever is ready, a super-tile's sub-label
+//                products first, then the statistics tiles in order;
+//   warps 2..5   sub-label group (a thread per point): the row -> the sub-label operand, then r and
+//                the draw; it runs up to two super-tiles ahead of
+//   warps 6..9   statistics group: the operand tiles of a super-tile whose sub-labels are drawn, from
+//                the same staged rows; it frees the stage slot.
+// Both groups drain the accumulation groups into FP64 (32 values per thread each).  Every wait is
+// bounded; on a failure every role stops, waits (bounded) for the copies or products it issued, and
+// the tensor memory is freed.  Output: the partial record per chunk of k_slot_stats_tc; sub[].
+constexpr int SS_T = 128;                        // points per super-tile (M of the sub-label products)
+constexpr int SS_SLOTS = 3;                      // staged super-tiles of rows (and of drawn sub-labels)
+constexpr int SS_PIDX = 4;                       // staged super-tiles of permutation entries
+constexpr int SS_KT = 16;                        // points per statistics tile (two groups of 8)
+constexpr int SS_TPS = SS_T / SS_KT;             // statistics tiles per super-tile
+constexpr int SS_G = 16;                         // statistics tiles per accumulation group (256 points)
+constexpr int SS_THREADS = 320;
+constexpr uint32_t SS_TMEM_COLS = 512;           // statistics accumulators at 0 and 128, sub-labels at 256
+constexpr uint32_t SS_SUBC = 256;
+
+enum : int {
+    SB_BFULL = 0, SB_FULL = 1, SB_EMPTY = SB_FULL + SS_SLOTS, SB_SUBREADY = SB_EMPTY + SS_SLOTS,
+    SB_AFULL = SB_SUBREADY + SS_SLOTS, SB_SUBDONE = SB_AFULL + 1, SB_STFULL = SB_SUBDONE + 1,
+    SB_STFREE = SB_STFULL + 2, SB_GRPDONE = SB_STFREE + 2, SB_ACCEMPTY = SB_GRPDONE + 2, SB_COUNT = SB_ACCEMPTY + 2
+};
+
+template <int DP>
+struct SubStatSmem {
+    static constexpr int NA = DP / 32 + 1;                     // statistics B atoms: features, then ones
+    static constexpr uint32_t A_GROUP = 4096, B_GROUP = NA * 1024;   // bytes per 8 points (two groups of 4)
+    static constexpr uint32_t OP_AH = 0, OP_AL = 2 * A_GROUP, OP_BH = 4 * A_GROUP, OP_BL = OP_BH + 2 * B_GROUP;
+    static constexpr uint32_t OP_BYTES = OP_BL + 2 * B_GROUP;        // one statistics operand buffer
+    static constexpr size_t sb = 0;                                  // 32 KB sub-label B tile (hi, lo)
+    static constexpr size_t sa = sb + STAGE_BYTES;                   // 32 KB sub-label A tile (hi, lo)
+    static constexpr size_t op = sa + A_TILE;                        // 2 statistics operand buffers
+    static constexpr size_t stage = op + 2 * (size_t)OP_BYTES;       // [SS_SLOTS][SS_T][DP] floats
+    static constexpr size_t pidx = stage + (size_t)SS_SLOTS * SS_T * DP * 4;   // [SS_PIDX][SS_T] ints
+    static constexpr size_t ssub = pidx + (size_t)SS_PIDX * SS_T * 4;          // [SS_SLOTS][SS_T] ints
+    static constexpr size_t bias = ssub + (size_t)SS_SLOTS * SS_T * 4;         // [2][KD] floats
+    static constexpr size_t shift = bias + (size_t)2 * KD * 4;                 // [64] floats
+    static constexpr size_t misc = shift + 64 * 4;                             // counts [2], abort flag
+    static constexpr size_t bar = misc + 16;
+    static constexpr size_t total = bar + SB_COUNT * 8 + 16 + 1024;           // + tmem slot, alignment
+    static_assert(stage % 1024 == 0 && OP_BH % 512 == 0 && OP_BL % 512 == 0 && OP_BYTES % 1024 == 0, "atoms");
+    static_assert(total <= 227 * 1024, "shared memory");
+};
+
+template <int DP>
+__global__ void __launch_bounds__(SS_THREADS, 1) k_sub_stats_tc(
+    const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
+    const int32_t* __restrict__ nchunks, const uint8_t* __restrict__ Bsub, const float* __restrict__ bvec,
+    const float* __restrict__ cvec, const float* __restrict__ lrw, const float* __restrict__ muv, RngArgs rng,
+    int32_t* __restrict__ sub, float* __restrict__ r_out, double* __restrict__ part, int32_t* __restrict__ err,
+    int stall)
+{
+    using L = SubStatSmem<DP>;
+    constexpr int NA = L::NA, N = NA * 32, C4 = DP / 4;
+    constexpr int SL = 1 + DP + tri(DP);
+    constexpr uint32_t A_GROUP = L::A_GROUP, B_GROUP = L::B_GROUP;
+    // F32 accumulator, TF32 A and B, both MN-major, M = 128, N = Dp + 32
+    constexpr uint32_t IDESC_ST = (1u << 4) | (2u << 7) | (2u << 10) | (1u << 15) | (1u << 16) |
+                                  ((uint32_t)(N >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* sB = smem + L::sb;
+    uint8_t* sA = smem + L::sa;
+    uint8_t* sop = smem + L::op;
+    float* stage = reinterpret_cast<float*>(smem + L::stage);
+    int32_t* spidx = reinterpret_cast<int32_t*>(smem + L::pidx);
+    int32_t* ssub = reinterpret_cast<int32_t*>(smem + L::ssub);
+    float* sbias = reinterpret_cast<float*>(smem + L::bias);
+    float* sshift = reinterpret_cast<float*>(smem + L::shift);
+    int* scnt = reinterpret_cast<int*>(smem + L::misc);
+    volatile int* abort_flag = reinterpret_cast<volatile int*>(scnt + 2);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + L::bar);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + SB_COUNT);
+
+    const int ch = blockIdx.x;
+    if (ch >= *nchunks) return;
+    const int k = chunk[3 * ch], start = chunk[3 * ch + 1], len = chunk[3 * ch + 2];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const volatile int32_t* gerr = err;
+    const int nst = (len + SS_T - 1) / SS_T;     // super-tiles
+    const int ntt = (len + SS_KT - 1) / SS_KT;   // statistics tiles
+    const int ngr = (ntt + SS_G - 1) / SS_G;     // accumulation groups
+
+    // statistics operands zeroed once: A's halves past Dp and B's ones atom rely on it
+    for (int e = tid; e < (int)(2 * L::OP_BYTES / 16); e += SS_THREADS)
+        reinterpret_cast<uint4*>(sop)[e] = make_uint4(0u, 0u, 0u, 0u);
+    if (tid < 2 * KD) {
+        const int side = tid / KD, j = tid % KD;
+        sbias[tid] = j < DP ? bvec[(size_t)(3 * k + 1 + side) * DP + j] : 0.f;
+    }
+    if (tid == 0) {
+        *abort_flag = *gerr ? 1 : 0;
+        scnt[0] = scnt[1] = 0;
+        mbar_init(&bars[SB_BFULL], 1);
+        for (int s = 0; s < SS_SLOTS; ++s) {
+            mbar_init(&bars[SB_FULL + s], 33);    // the loader's 32 lanes' copies, then its lane 0
+            mbar_init(&bars[SB_EMPTY + s], 4);    // the statistics group
+            mbar_init(&bars[SB_SUBREADY + s], 4); // the sub-label group
+        }
+        mbar_init(&bars[SB_AFULL], 4);
+        mbar_init(&bars[SB_SUBDONE], 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&bars[SB_STFULL + b], 4);
+            mbar_init(&bars[SB_STFREE + b], 1);
+            mbar_init(&bars[SB_GRPDONE + b], 1);
+            mbar_init(&bars[SB_ACCEMPTY + b], 8);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(SS_TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    __syncthreads();
+    if (tid < 2 * SS_KT)   // the ones column: element 0 of B's last atom in every row, both buffers (hi part)
+        *reinterpret_cast<float*>(sop + (tid / SS_KT) * L::OP_BYTES + L::OP_BH + mn32_offset(tid % SS_KT, 0, NA - 1, NA)) =
+            1.0f;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const bool run = *abort_flag == 0;
+
+    // group drain role of warps 2..9: TMEM lane quarter q, column half hc (0: sub-label group)
+    const int q = warp & 3, hc = (warp - 2) >> 2;
+    const int dslot = q >> 1, fi = (q & 1) * 32 + lane;   // sub-cluster, feature i of this lane's row
+    const bool row_live = (q & 1) * 32 < DP;
+    const bool do_s = row_live && (DP > 32 ? (q & 1) <= hc : hc == 0);
+    const bool do_sum = row_live && hc == 0;
+    double acc[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) acc[m] = 0.0;
+    double sacc = 0.0;
+    int cnt_l = 0, cnt_r = 0;
+    auto drain_group = [&](int g) -> bool {   // warps 2..9, each group once (both halves of the columns)
+        if (!warp_wait_bounded(&bars[SB_GRPDONE + (g & 1)], (uint32_t)((g >> 1) & 1), gerr)) {
+            if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+            return false;
+        }
+        tc_fence_after();
+        const uint32_t base = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)((g & 1) * 128);
+        if (do_s) {
+            uint32_t v[32];
+            tmem_ld32(base + (uint32_t)(32 * hc), v);
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] += (double)__uint_as_float(v[i]);
+        }
+        if (do_sum) {
+            uint32_t v1;
+            tmem_ld1(base + (uint32_t)DP, v1);
+            sacc += (double)__uint_as_float(v1);
+        }
+        tc_fence_before();
+        warp_arrive(&bars[SB_ACCEMPTY + (g & 1)]);
+        return true;
+    };
+
+    if (warp == 0) {
+        // ---------------- loader
+        if (run) {
+            if (lane == 0) {
+                mbar_arrive_expect_tx(&bars[SB_BFULL], STAGE_BYTES);
+                bulk_copy_g2s(sB, Bsub + (size_t)k * STAGE_BYTES, STAGE_BYTES, &bars[SB_BFULL]);
+            }
+            int pe[4];
+            auto load_pe = [&](int T) {
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int row = T * SS_T + 4 * lane + r;
+                    pe[r] = row < len ? __ldg(perm + start + row) : -1;
+                }
+            };
+            load_pe(0);
+            int issued = 0;
+            for (int T = 0; T < nst; ++T) {
+                const int slot = T % SS_SLOTS;
+                if (T >= SS_SLOTS &&
+                    !warp_wait_bounded(&bars[SB_EMPTY + slot], (uint32_t)((T / SS_SLOTS - 1) & 1), gerr)) {
+                    if (lane == 0) {
+                        atomicCAS(err, 0, ERR_TIMEOUT_EMPTY);
+                        *abort_flag = 1;
+                    }
+                    break;
+                }
+                if (__any_sync(0xffffffffu, *abort_flag != 0)) break;
+                const int nv = min(SS_T, len - T * SS_T);
+                int32_t* pix = spidx + (T % SS_PIDX) * SS_T;
+#pragma unroll
+                for (int r = 0; r < 4; ++r) pix[4 * lane + r] = pe[r];
+                __syncwarp();
+                // a warp instruction copies 32 / (Dp / 4) whole rows, 16 bytes per lane (zero past the chunk)
+                constexpr int RPI = 32 / C4;
+                float* sl = stage + (size_t)slot * SS_T * DP;
+                const int pc = lane % C4, pr = lane / C4;
+#pragma unroll 4
+                for (int i = 0; i < SS_T / RPI; ++i) {
+                    const int row = RPI * i + pr;
+                    const bool live = row < nv;
+                    cp_async16(sl + row * DP + 4 * pc, x + (size_t)(live ? pix[row] : 0) * DP + 4 * pc, live ? 16u : 0u);
+                }
+                cp_async_mbar_arrive(&bars[SB_FULL + slot]);
+                __syncwarp();
+                if (lane == 0) mbar_arrive(&bars[SB_FULL + slot]);   // orders the entries written above
+                ++issued;
+                if (T + 1 < nst) load_pe(T + 1);
+            }
+            // every copy issued has landed before the shared memory is released
+            if (lane == 0) {
+                mbar_wait_bounded(&bars[SB_BFULL], 0, nullptr);
+                for (int t = issued > SS_SLOTS ? issued - SS_SLOTS : 0; t < issued; ++t)
+                    mbar_wait_bounded(&bars[SB_FULL + t % SS_SLOTS], (uint32_t)((t / SS_SLOTS) & 1), nullptr);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer.  stall (test seam): nothing is issued, so the groups' waits run out
+        if (run && lane == 0 && !stall) {
+            uint64_t* last = nullptr;   // the barrier of the last commit and its phase parity
+            uint32_t last_par = 0;
+            bool ok = mbar_wait_bounded(&bars[SB_BFULL], 0, gerr);
+            if (!ok) atomicCAS(err, 0, ERR_TIMEOUT_BFULL);
+            const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
+            const uint64_t db_h = sw128_desc(smem_u32(sB)), db_l = sw128_desc(smem_u32(sB + B_BYTES));
+            int ts = 0, ti = 0;   // next super-tile for the sub-label products, next statistics tile
+            uint64_t t0 = global_ns();
+            uint32_t idle = 0;
+            while (ok && (ts < nst || ti < ntt)) {
+                bool did = false;
+                // a super-tile's sub-label products (the sub-label group has drained the previous ones)
+                if (ts < nst && mbar_test_wait(&bars[SB_AFULL], (uint32_t)(ts & 1))) {
+                    tc_fence_after();
+                    const uint32_t dsub = tmem_base + SS_SUBC;
+#pragma unroll
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
+#pragma unroll
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_l + 2 * ks, db_h + 2 * ks, 1u);
+#pragma unroll
+                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_l + 2 * ks, 1u);
+                    umma_commit(&bars[SB_SUBDONE]);
+                    last = &bars[SB_SUBDONE];
+                    last_par = (uint32_t)(ts & 1);
+                    ++ts;
+                    did = true;
+                }
+                // the next statistics tile, in order (its group's accumulator drained two groups ago)
+                if (ti < ntt) {
+                    const int b = ti & 1, g = ti / SS_G;
+                    const bool acc_free = !(ti % SS_G == 0 && g >= 2) ||
+                                          mbar_test_wait(&bars[SB_ACCEMPTY + (g & 1)], (uint32_t)(((g >> 1) - 1) & 1));
+                    if (acc_free && mbar_test_wait(&bars[SB_STFULL + b], (uint32_t)((ti >> 1) & 1))) {
+                        tc_fence_after();
+                        const uint32_t td = tmem_base + (uint32_t)((g & 1) * 128);
+                        const uint32_t ob = smem_u32(sop + (size_t)b * L::OP_BYTES);
+#pragma unroll
+                        for (int kg = 0; kg < SS_KT / 8; ++kg) {   // one group of 8 points per product (K = 8)
+                            const uint64_t adh = sw128b32_mn_desc(ob + L::OP_AH + kg * A_GROUP, A_GROUP / 2);
+                            const uint64_t adl = sw128b32_mn_desc(ob + L::OP_AL + kg * A_GROUP, A_GROUP / 2);
+                            const uint64_t bdh = sw128b32_mn_desc(ob + L::OP_BH + kg * B_GROUP, B_GROUP / 2);
+                            const uint64_t bdl = sw128b32_mn_desc(ob + L::OP_BL + kg * B_GROUP, B_GROUP / 2);
+                            umma_tf32(td, adh, bdh, IDESC_ST, (ti % SS_G == 0 && kg == 0) ? 0u : 1u);
+                            umma_tf32(td, adl, bdh, IDESC_ST, 1u);
+                            umma_tf32(td, adh, bdl, IDESC_ST, 1u);
+                        }
+                        umma_commit(&bars[SB_STFREE + b]);
+                        last = &bars[SB_STFREE + b];
+                        last_par = (uint32_t)((ti >> 1) & 1);
+                        if (ti % SS_G == SS_G - 1 || ti == ntt - 1) {
+                            umma_commit(&bars[SB_GRPDONE + (g & 1)]);
+                            last = &bars[SB_GRPDONE + (g & 1)];
+                            last_par = (uint32_t)((g >> 1) & 1);
+                        }
+                        ++ti;
+                        did = true;
+                    }
+                }
+                if (did) {
+                    t0 = global_ns();
+                    idle = 0;
+                } else {
+                    __nanosleep(32);
+                    if ((++idle & 63) == 0) {
+                        if (global_ns() - t0 > WAIT_LIMIT_NS) {
+                            atomicCAS(err, 0, ERR_TIMEOUT_FULL);
+                            ok = false;
+                        } else if (*gerr || *abort_flag) {
+                            ok = false;
+                        }
+                    }
+                }
+            }
+            if (!ok) *abort_flag = 1;
+            // the products issued have completed before the tensor memory is freed (a commit tracks
+            // every earlier product of this thread)
+            if (last) mbar_wait_bounded(last, last_par, nullptr);
+        }
+    } else if (warp < 6) {
+        // ---------------- sub-label group: point p of every super-tile
+        const int p = q * 32 + lane;
+        const float cl = cvec[3 * k + 1], cr = cvec[3 * k + 2], wl = lrw[2 * k], wr = lrw[2 * k + 1];
+        bool ok = run;
+        int drained = 0;   // accumulation groups drained (this group's half)
+        for (int T = 0; T < nst && ok; ++T) {
+            if (__any_sync(0xffffffffu, *abort_flag != 0)) { ok = false; break; }
+            // the accumulation group that ended two super-tiles ago (its products completed long since)
+            if ((T & 1) == 0 && T >= 4) {
+                if (!drain_group(T / 2 - 2)) { ok = false; break; }
+                drained = T / 2 - 1;
+            }
+            const int slot = T % SS_SLOTS, nv = min(SS_T, len - T * SS_T);
+            if (!warp_wait_bounded(&bars[SB_FULL + slot], (uint32_t)((T / SS_SLOTS) & 1), gerr)) {
+                if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_FULL);
+                ok = false;
+                break;
+            }
+            const float* row = stage + ((size_t)slot * SS_T + p) * DP;
+            if (T == 0 && p < DP) {   // centre of the statistics: mean of the chunk's first 32 points
+                const int n0 = min(32, len);
+                float a = 0.f;
+                for (int r = 0; r < n0; ++r) a += stage[(size_t)r * DP + p];
+                sshift[p] = a / (float)n0;
+            }
+            // the sub-label operand: this point's row split into BF16 hi / lo (zero past Dp and past the
+            // chunk: the stage's rows past the chunk are zero-filled); the lanes visit the 16 pieces in
+            // rotated order so that neither the row reads nor the operand stores share banks
+#pragma unroll 4
+            for (int i = 0; i < 16; ++i) {
+                const int c = (i + lane) & 15;   // features 4 c .. 4 c + 3
+                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (4 * c < DP) v = *reinterpret_cast<const float4*>(row + 4 * c);
+                uint2 hi, lo;
+                bf16_split4(v.x, v.y, v.z, v.w, hi, lo);
+                const uint32_t off = sw128_offset(p, 4 * c);
+                *reinterpret_cast<uint2*>(sA + off) = hi;
+                *reinterpret_cast<uint2*>(sA + A_BYTES + off) = lo;
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            warp_arrive(&bars[SB_AFULL]);
+            // r of both sub-clusters for this point (its TMEM lane), then the draw (cudaKernel.cu:352-372)
+            if (!warp_wait_bounded(&bars[SB_SUBDONE], (uint32_t)(T & 1), gerr)) {
+                if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_TFULL);
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            float rs[2];
+#pragma unroll
+            for (int side = 0; side < 2; ++side) {
+                const float* bs = sbias + side * KD;
+                float q0 = 0.f, q1 = 0.f, q2 = 0.f, q3 = 0.f;
+#pragma unroll
+                for (int hh = 0; hh < 2; ++hh) {
+                    if (hh == 1 && DP <= 32) break;   // columns past Dp are zero
+                    uint32_t v[32];
+                    tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + SS_SUBC + (uint32_t)(side * KD + 32 * hh), v);
+#pragma unroll
+                    for (int j4 = 0; j4 < 8; ++j4) {
+                        const float4 b4 = *reinterpret_cast<const float4*>(bs + 32 * hh + 4 * j4);
+                        const float z0 = __uint_as_float(v[4 * j4 + 0]) - b4.x;
+                        const float z1 = __uint_as_float(v[4 * j4 + 1]) - b4.y;
+                        const float z2 = __uint_as_float(v[4 * j4 + 2]) - b4.z;
+                        const float z3 = __uint_as_float(v[4 * j4 + 3]) - b4.w;
+                        q0 = fmaf(z0, z0, q0);
+                        q1 = fmaf(z1, z1, q1);
+                        q2 = fmaf(z2, z2, q2);
+                        q3 = fmaf(z3, z3, q3);
+                    }
+                }
+                rs[side] = (side ? cr : cl) - 0.5f * ((q0 + q1) + (q2 + q3));
+            }
+            tc_fence_before();   // the accumulator is read: the next super-tile's products may overwrite it
+            int lab = 0;
+            if (p < nv) {
+                const int64_t pt = spidx[(T % SS_PIDX) * SS_T + p];
+                float rl = rs[0], rr = rs[1];
+                if (r_out) {
+                    r_out[2 * pt] = rl;
+                    r_out[2 * pt + 1] = rr;
+                }
+                rl += wl;
+                rr += wr;
+                const float mx = fmaxf(rl, rr);
+                const float el = __expf(rl - mx), er = __expf(rr - mx);
+                const float s = el + er;
+                float u1, u2;
+                draw_uniform2(rng, pt, u1, u2);
+                lab = alias_draw2(el / s, er / s, u1, u2);
+                sub[pt] = lab;
+            }
+            ssub[slot * SS_T + p] = lab;
+            const unsigned bl = __ballot_sync(0xffffffffu, lab == 1), br = __ballot_sync(0xffffffffu, lab == 2);
+            cnt_l += __popc(bl);
+            cnt_r += __popc(br);
+            warp_arrive(&bars[SB_SUBREADY + slot]);
+        }
+        if (ok)
+            for (int g = drained; g < ngr && ok; ++g) ok = drain_group(g);
+        if (!ok) *abort_flag = 1;
+        if (lane == 0) {
+            atomicAdd(&scnt[0], cnt_l);
+            atomicAdd(&scnt[1], cnt_r);
+        }
+    } else {
+        // ---------------- statistics group: 16-point tiles of the super-tiles whose sub-labels are drawn
+        const int gt = tid - 192;                  // 0 .. 127
+        constexpr int ITEMS = SS_KT * C4 / 128;    // 16-byte pieces per thread per tile (2 or 1)
+        const int j4 = gt % C4;                    // the thread's piece of every row: features 4 j4 ..
+        bool ok = run;
+        int drained = 0;
+        float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int T = 0; T < nst && ok; ++T) {
+            if (__any_sync(0xffffffffu, *abort_flag != 0)) { ok = false; break; }
+            const int slot = T % SS_SLOTS;
+            if (!warp_wait_bounded(&bars[SB_SUBREADY + slot], (uint32_t)((T / SS_SLOTS) & 1), gerr)) {
+                if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_AFULL);
+                ok = false;
+                break;
+            }
+            if (T == 0) s4 = *reinterpret_cast<const float4*>(sshift + 4 * j4);
+            const float* sl = stage + (size_t)slot * SS_T * DP;
+            const int32_t* sbs = ssub + slot * SS_T;
+            const int nj = min(SS_TPS, ntt - T * SS_TPS);
+            for (int j = 0; j < nj; ++j) {
+                const int idx = T * SS_TPS + j, b = idx & 1, u = idx >> 1;
+                if (u >= 1 && !warp_wait_bounded(&bars[SB_STFREE + b], (uint32_t)((u - 1) & 1), gerr)) {
+                    if (lane == 0) atomicCAS(err, 0, ERR_TIMEOUT_EMPTY);
+                    ok = false;
+                    break;
+                }
+                uint8_t* ob = sop + (size_t)b * L::OP_BYTES;
+#pragma unroll
+                for (int it = 0; it < ITEMS; ++it) {
+                    const int pl = (gt + 128 * it) / C4;   // point of the tile; 8 lanes share a row
+                    const int pp = SS_KT * j + pl;
+                    const int sv = sbs[pp];
+                    const bool live = sv == 1 || sv == 2;
+                    const int side = sv == 2 ? 1 : 0;
+                    const float4 v4 = *reinterpret_cast<const float4*>(sl + (size_t)pp * DP + 4 * j4);
+                    const float cv[4] = {v4.x - s4.x, v4.y - s4.y, v4.z - s4.z, v4.w - s4.w};
+                    float hi[4], lo[4];
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        hi[e] = tf32_rna(cv[e]);
+                        lo[e] = tf32_rna(cv[e] - hi[e]);
+                        if (!live) hi[e] = lo[e] = 0.f;
+                    }
+                    const uint32_t a_c = mn32_offset(pl, j4, 2 * side, 4);
+                    const uint32_t a_z = mn32_offset(pl, j4, 2 * (1 - side), 4);
+                    const uint32_t b_o = mn32_offset(pl, j4, 0, NA);
+                    const uint4 h4 = make_uint4(__float_as_uint(hi[0]), __float_as_uint(hi[1]), __float_as_uint(hi[2]),
+                                                __float_as_uint(hi[3]));
+                    const uint4 l4 = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
+                                                __float_as_uint(lo[3]));
+                    const uint4 z4 = make_uint4(0u, 0u, 0u, 0u);
+                    *reinterpret_cast<uint4*>(ob + L::OP_AH + a_c) = h4;
+                    *reinterpret_cast<uint4*>(ob + L::OP_AL + a_c) = l4;
+                    *reinterpret_cast<uint4*>(ob + L::OP_AH + a_z) = z4;
+                    *reinterpret_cast<uint4*>(ob + L::OP_AL + a_z) = z4;
+                    *reinterpret_cast<uint4*>(ob + L::OP_BH + b_o) = h4;
+                    *reinterpret_cast<uint4*>(ob + L::OP_BL + b_o) = l4;
+                }
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                warp_arrive(&bars[SB_STFULL + b]);
+            }
+            if (!ok) break;
+            warp_arrive(&bars[SB_EMPTY + slot]);   // the rows and sub-labels of this slot are consumed
+            // the accumulation group that ended with the previous super-tile, while this one's products run
+            if ((T & 1) == 0 && T >= 2) {
+                if (!drain_group(T / 2 - 1)) { ok = false; break; }
+                drained = T / 2;
+            }
+        }
+        if (ok)
+            for (int g = drained; g < ngr && ok; ++g) ok = drain_group(g);
+        if (!ok) *abort_flag = 1;
+    }
+    tc_fence_before();
+    __syncthreads();   // every role is done: copies landed, products complete, accumulators drained
+    const bool good = *abort_flag == 0;
+    double* xs = reinterpret_cast<double*>(smem + L::stage);   // [2][DP] sums S1
+    double* xd = xs + 2 * DP;                                  // [DP] d = a - mu_k
+    double* xn = xd + DP;                                      // [2] counts
+    if (good) {
+        if (warp >= 2 && do_sum) xs[dslot * DP + fi] = sacc;
+        if (tid < DP) xd[tid] = (double)sshift[tid] - (double)muv[(size_t)3 * k * DP + tid];
+        if (tid == 0) {
+            xn[0] = (double)scnt[0];
+            xn[1] = (double)scnt[1];
+        }
+    }
+    __syncthreads();
+    if (good) {
+        double* out = part + (size_t)ch * 2 * SL;
+        if (tid < 2) out[(size_t)tid * SL] = xn[tid];
+        if (warp >= 2) {
+            const double n = xn[dslot];
+            if (do_s) {
+                double* po = out + (size_t)dslot * SL + 1 + DP;
+                const double di = xd[fi], si = xs[dslot * DP + fi];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const int j = 32 * hc + i;
+                    if (fi <= j && j < DP) {
+                        const double dj = xd[j], sj = xs[dslot * DP + j];
+                        po[tri_index(DP, fi, j)] = acc[i] + di * sj + si * dj + n * di * dj;
+                    }
+                }
+            }
+            if (do_sum) out[(size_t)dslot * SL + 1 + fi] = sacc + n * xd[fi];
+        }
+    }
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(SS_TMEM_COLS));
     }
 }
 
@@ -1963,6 +2589,42 @@ dpmm_status launch_slot_stats_tc(dpmm_ctx* c, const uint8_t* d_mask)
     if (h_err[1]) return fail(DPMM_ERR_TIMEOUT, "tensor-core sub-label kernel: bounded wait expired (code " +
                                                     std::to_string(h_err[1]) + ")");
     if (*h_err) return fail(DPMM_ERR_TIMEOUT, "tensor-core statistics: bounded wait expired (code " +
+                                                  std::to_string(*h_err) + ")");
+    return DPMM_OK;
+}
+
+template <int DP>
+static dpmm_status launch_sub_stats_tc_t(dpmm_ctx* c, RngArgs r, float* d_rout, int32_t* err)
+{
+    auto kern = tc::k_sub_stats_tc<DP>;
+    constexpr size_t sm = tc::SubStatSmem<DP>::total;
+    DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    kern<<<c->max_chunks, tc::SS_THREADS, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Bsub,
+                                                            c->d_b, c->d_c, c->d_lrw, c->d_mu, r, c->d_sub, d_rout,
+                                                            c->d_part, err, c->stall_tc_mma);
+    DPMM_LAUNCHED();
+    return DPMM_OK;
+}
+
+bool tc_sub_stats_supported(const dpmm_ctx* c)
+{
+    return c->fuse_sub_stats && tc_sub_supported(c) && tc_stats_supported(c);
+}
+
+dpmm_status launch_sub_stats_tc(dpmm_ctx* c, RngArgs r, float* d_rout)
+{
+    if (!tc_sub_stats_supported(c)) return fail(DPMM_ERR_INVALID_ARG, "fused sub-label statistics: unsupported shape");
+    int32_t* err = c->d_aux + 3;
+    DPMM_CUDA_TRY(cudaMemsetAsync(err, 0, sizeof(int32_t), c->stream));
+    {
+        KernelTimer kt(c, PH_SLOT_STATS);
+        if (c->Dp == 64) DPMM_TRY(launch_sub_stats_tc_t<64>(c, r, d_rout, err));
+        else DPMM_TRY(launch_sub_stats_tc_t<32>(c, r, d_rout, err));
+    }
+    int32_t* h_err = reinterpret_cast<int32_t*>(c->h_pinned);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(h_err, err, sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (*h_err) return fail(DPMM_ERR_TIMEOUT, "fused sub-label statistics kernel: bounded wait expired (code " +
                                                   std::to_string(*h_err) + ")");
     return DPMM_OK;
 }

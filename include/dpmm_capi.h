@@ -364,6 +364,14 @@ dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, 
  * for them runs out after its limit (2 s); the call then returns DPMM_ERR_TIMEOUT after the kernel has
  * waited for the copies it issued and freed its tensor memory, and the context stays usable. */
 dpmm_status dpmm_set_wait_test(dpmm_ctx* ctx, int32_t stall);
+/* Sub-cluster labels and their statistics in one pass over the points (no counterpart in the
+ * reference, whose create_subclusters_labels and statistics are separate passes): with on nonzero the
+ * NIW contexts at D = 17 .. 64 that run both on the tensor cores gather each point once for both
+ * (k_sub_stats_tc); with on = 0 (the default: on the B200 the two kernels are faster) they run as
+ * k_sub_labels_tc and then k_slot_stats_tc.  The sub-cluster log-likelihoods and sub-labels are
+ * bit-identical either way; the statistics agree to FP32 rounding (the same products accumulated in
+ * 16- instead of 32-point tiles). */
+dpmm_status dpmm_set_fused_sub_stats(dpmm_ctx* ctx, int32_t on);
 /* Test seam (no counterpart in the reference): log theta[3K][D] of the 3K slots of a multinomial context
  * as the label phases use them (FP32). */
 dpmm_status dpmm_get_multinomial_params(dpmm_ctx* ctx, int K, float* log_theta);

@@ -1,10 +1,11 @@
 """Time the reference's own GPU executable against this library on the same input (test infrastructure).
 
-    python oracle/compare_reference_gpu.py [--n 1000000] [--d 32] [--k 20] [--iters 20] [--out DIR]
+    python oracle/compare_reference_gpu.py [--n 1000000] [--d 32] [--k 20] [--iters 60] [--out DIR]
 
 Writes a seeded synthetic data set of the C2 shape (means U(-20, 20)^D, covariances A A^T / D + 0.5 I,
 Dirichlet(1) weights) as a float64 N x D .npy (the layout the reference's loader reads correctly) and a
-params JSON (NIW kappa 1, m 0, nu D + 3, Psi I; alpha 10), runs the reference executable built from its
+params JSON (NIW kappa 1, m 0, nu D + 3, Psi I; alpha 10; burn-out period 15, so that clusters split
+from the 16th iteration on), runs the reference executable built from its
 sources by oracle/Makefile (oracle/_ref/dpmm_ref, sm_100a) with --model_path / --params_path /
 --result_path, and this library's dp_parallel_from_file on the same two files, and prints one JSON line:
 seconds per iteration (the reference's own iter_count; this library's iteration times), points x
@@ -50,7 +51,7 @@ def main():
     ap.add_argument("--n", type=int, default=1_000_000)
     ap.add_argument("--d", type=int, default=32)
     ap.add_argument("--k", type=int, default=20)
-    ap.add_argument("--iters", type=int, default=20)
+    ap.add_argument("--iters", type=int, default=60)
     ap.add_argument("--seed", type=int, default=1102)
     ap.add_argument("--out", default="/tmp/dpmm_compare")
     args = ap.parse_args()
@@ -59,12 +60,12 @@ def main():
     npy, pj, rj = (os.path.join(args.out, f) for f in ("x.npy", "params.json", "result.json"))
     np.save(npy, x)
     with open(pj, "w") as f:
-        json.dump({"alpha": 10.0, "iterations": args.iters, "burnout_period": 20, "outlier_mod": 0.0,
+        json.dump({"alpha": 10.0, "iterations": args.iters, "burnout_period": 15, "outlier_mod": 0.0,
                    "randomSeed": 7, "initial_clusters": 1,
                    "hyper_params": {"k": 1.0, "m": [0.0] * args.d, "v": args.d + 3.0,
                                     "psi": np.eye(args.d).tolist()}}, f)
     out = {"workload": f"C2 shape: N={args.n}, D={args.d}, {args.k} true clusters, float64 .npy, "
-                       f"{args.iters} iterations from one cluster, alpha 10, NIW(1, 0, D+3, I)"}
+                       f"{args.iters} iterations from one cluster (burn-out 15), alpha 10, NIW(1, 0, D+3, I)"}
     if os.path.exists(REF_EXE):
         t0 = time.perf_counter()
         p = subprocess.run([REF_EXE, f"--model_path={npy}", f"--params_path={pj}", "--prior_type=Gaussian",
