@@ -1879,8 +1879,8 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
 //   warp 0       loader: the permutation entries, then the rows into a three-slot stage by 16-byte
 //                cp.async (a warp instruction copies whole rows; per-row bulk copies measured several
 //                times slower for 256-byte rows); the cluster's B tile once per chunk;
-//   warp 1       MMA issuer (one thread): services whichever is ready, a super-tile's sub-label
-//                products first, then the statistics tiles in order;
+//   warp 1       MMA issuer (one thread): sub-label products of super-tile T + 1, then the
+//                statistics tiles of T, the order in which the two groups produce their operands;
 //   warps 2..5   sub-label group (a thread per point): the row -> the sub-label operand, then r and
 //                the draw; it runs up to two super-tiles ahead of
 //   warps 6..9   statistics group: the operand tiles of a super-tile whose sub-labels are drawn, from
@@ -2105,72 +2105,66 @@ __global__ void __launch_bounds__(SS_THREADS, 1) k_sub_stats_tc(
             if (!ok) atomicCAS(err, 0, ERR_TIMEOUT_BFULL);
             const uint64_t da_h = sw128_desc(smem_u32(sA)), da_l = sw128_desc(smem_u32(sA + A_BYTES));
             const uint64_t db_h = sw128_desc(smem_u32(sB)), db_l = sw128_desc(smem_u32(sB + B_BYTES));
-            int ts = 0, ti = 0;   // next super-tile for the sub-label products, next statistics tile
-            uint64_t t0 = global_ns();
-            uint32_t idle = 0;
-            while (ok && (ts < nst || ti < ntt)) {
-                bool did = false;
-                // a super-tile's sub-label products (the sub-label group has drained the previous ones)
-                if (ts < nst && mbar_test_wait(&bars[SB_AFULL], (uint32_t)(ts & 1))) {
-                    tc_fence_after();
-                    const uint32_t dsub = tmem_base + SS_SUBC;
-#pragma unroll
-                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
-#pragma unroll
-                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_l + 2 * ks, db_h + 2 * ks, 1u);
-#pragma unroll
-                    for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_l + 2 * ks, 1u);
-                    umma_commit(&bars[SB_SUBDONE]);
-                    last = &bars[SB_SUBDONE];
-                    last_par = (uint32_t)(ts & 1);
-                    ++ts;
-                    did = true;
+            // issue order: sub(0), then per super-tile T: sub(T + 1), the statistics tiles of T -- the
+            // order in which the groups produce them (the sub-label group runs ahead); every wait sleeps
+            auto issue_sub = [&](int ts) -> bool {
+                if (!mbar_wait_bounded(&bars[SB_AFULL], (uint32_t)(ts & 1), gerr)) {
+                    atomicCAS(err, 0, ERR_TIMEOUT_AFULL);
+                    return false;
                 }
-                // the next statistics tile, in order (its group's accumulator drained two groups ago)
-                if (ti < ntt) {
-                    const int b = ti & 1, g = ti / SS_G;
-                    const bool acc_free = !(ti % SS_G == 0 && g >= 2) ||
-                                          mbar_test_wait(&bars[SB_ACCEMPTY + (g & 1)], (uint32_t)(((g >> 1) - 1) & 1));
-                    if (acc_free && mbar_test_wait(&bars[SB_STFULL + b], (uint32_t)((ti >> 1) & 1))) {
-                        tc_fence_after();
-                        const uint32_t td = tmem_base + (uint32_t)((g & 1) * 128);
-                        const uint32_t ob = smem_u32(sop + (size_t)b * L::OP_BYTES);
+                tc_fence_after();
+                const uint32_t dsub = tmem_base + SS_SUBC;
 #pragma unroll
-                        for (int kg = 0; kg < SS_KT / 8; ++kg) {   // one group of 8 points per product (K = 8)
-                            const uint64_t adh = sw128b32_mn_desc(ob + L::OP_AH + kg * A_GROUP, A_GROUP / 2);
-                            const uint64_t adl = sw128b32_mn_desc(ob + L::OP_AL + kg * A_GROUP, A_GROUP / 2);
-                            const uint64_t bdh = sw128b32_mn_desc(ob + L::OP_BH + kg * B_GROUP, B_GROUP / 2);
-                            const uint64_t bdl = sw128b32_mn_desc(ob + L::OP_BL + kg * B_GROUP, B_GROUP / 2);
-                            umma_tf32(td, adh, bdh, IDESC_ST, (ti % SS_G == 0 && kg == 0) ? 0u : 1u);
-                            umma_tf32(td, adl, bdh, IDESC_ST, 1u);
-                            umma_tf32(td, adh, bdl, IDESC_ST, 1u);
-                        }
-                        umma_commit(&bars[SB_STFREE + b]);
-                        last = &bars[SB_STFREE + b];
-                        last_par = (uint32_t)((ti >> 1) & 1);
-                        if (ti % SS_G == SS_G - 1 || ti == ntt - 1) {
-                            umma_commit(&bars[SB_GRPDONE + (g & 1)]);
-                            last = &bars[SB_GRPDONE + (g & 1)];
-                            last_par = (uint32_t)((g >> 1) & 1);
-                        }
-                        ++ti;
-                        did = true;
-                    }
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_l + 2 * ks, db_h + 2 * ks, 1u);
+#pragma unroll
+                for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(dsub, da_h + 2 * ks, db_l + 2 * ks, 1u);
+                umma_commit(&bars[SB_SUBDONE]);
+                last = &bars[SB_SUBDONE];
+                last_par = (uint32_t)(ts & 1);
+                return true;
+            };
+            auto issue_tile = [&](int ti) -> bool {
+                const int b = ti & 1, g = ti / SS_G;
+                if (ti % SS_G == 0 && g >= 2 &&
+                    !mbar_wait_bounded(&bars[SB_ACCEMPTY + (g & 1)], (uint32_t)(((g >> 1) - 1) & 1), gerr)) {
+                    atomicCAS(err, 0, ERR_TIMEOUT_TEMPTY);
+                    return false;
                 }
-                if (did) {
-                    t0 = global_ns();
-                    idle = 0;
-                } else {
-                    __nanosleep(32);
-                    if ((++idle & 63) == 0) {
-                        if (global_ns() - t0 > WAIT_LIMIT_NS) {
-                            atomicCAS(err, 0, ERR_TIMEOUT_FULL);
-                            ok = false;
-                        } else if (*gerr || *abort_flag) {
-                            ok = false;
-                        }
-                    }
+                if (!mbar_wait_bounded(&bars[SB_STFULL + b], (uint32_t)((ti >> 1) & 1), gerr)) {
+                    atomicCAS(err, 0, ERR_TIMEOUT_FULL);
+                    return false;
                 }
+                tc_fence_after();
+                const uint32_t td = tmem_base + (uint32_t)((g & 1) * 128);
+                const uint32_t ob = smem_u32(sop + (size_t)b * L::OP_BYTES);
+#pragma unroll
+                for (int kg = 0; kg < SS_KT / 8; ++kg) {   // one group of 8 points per product (K = 8)
+                    const uint64_t adh = sw128b32_mn_desc(ob + L::OP_AH + kg * A_GROUP, A_GROUP / 2);
+                    const uint64_t adl = sw128b32_mn_desc(ob + L::OP_AL + kg * A_GROUP, A_GROUP / 2);
+                    const uint64_t bdh = sw128b32_mn_desc(ob + L::OP_BH + kg * B_GROUP, B_GROUP / 2);
+                    const uint64_t bdl = sw128b32_mn_desc(ob + L::OP_BL + kg * B_GROUP, B_GROUP / 2);
+                    umma_tf32(td, adh, bdh, IDESC_ST, (ti % SS_G == 0 && kg == 0) ? 0u : 1u);
+                    umma_tf32(td, adl, bdh, IDESC_ST, 1u);
+                    umma_tf32(td, adh, bdl, IDESC_ST, 1u);
+                }
+                umma_commit(&bars[SB_STFREE + b]);
+                last = &bars[SB_STFREE + b];
+                last_par = (uint32_t)((ti >> 1) & 1);
+                if (ti % SS_G == SS_G - 1 || ti == ntt - 1) {
+                    umma_commit(&bars[SB_GRPDONE + (g & 1)]);
+                    last = &bars[SB_GRPDONE + (g & 1)];
+                    last_par = (uint32_t)((g >> 1) & 1);
+                }
+                return true;
+            };
+            if (ok) ok = issue_sub(0);
+            for (int T = 0; T < nst && ok; ++T) {
+                if (*abort_flag) { ok = false; break; }
+                if (T + 1 < nst && !issue_sub(T + 1)) { ok = false; break; }
+                const int nj = min(SS_TPS, ntt - T * SS_TPS);
+                for (int j = 0; j < nj && ok; ++j) ok = issue_tile(T * SS_TPS + j);
             }
             if (!ok) *abort_flag = 1;
             // the products issued have completed before the tensor memory is freed (a commit tracks
