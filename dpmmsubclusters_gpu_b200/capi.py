@@ -155,6 +155,9 @@ SIGNATURES = {
     "dpmm_get_multinomial_params": (c_int, [_CTX, c_int, _PF]),
     "dpmm_set_wait_test": (c_int, [_CTX, c_int32]),
     "dpmm_set_fused_sub_stats": (c_int, [_CTX, c_int32]),
+    "dpmm_set_outlier_prior_niw": (c_int, [_CTX, c_double, _PD, c_double, _PD]),
+    "dpmm_set_outlier_prior_multinomial": (c_int, [_CTX, _PD]),
+    "dpmm_set_cluster_priors": (c_int, [_CTX, c_int, ctypes.POINTER(ctypes.c_uint8)]),
     "dpmm_set_label_pruning": (c_int, [_CTX, c_double]),
     "dpmm_label_pruning_stats": (c_int, [_CTX, _PD]),
     "dpmm_set_ground_truth": (c_int, [_CTX, _PI32]),

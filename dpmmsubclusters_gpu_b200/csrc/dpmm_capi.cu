@@ -180,7 +180,8 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_prox, c->d_scr_score, c->d_scr_w, c->d_scr_wdep, c->d_scr_elig, c->d_scr_sel,
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
-                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg, c->d_Amult, c->d_Bmult};
+                    c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg, c->d_Amult, c->d_Bmult,
+                    c->d_prior2, c->d_prior_sel, c->d_cbase};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);
@@ -667,6 +668,7 @@ static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, con
     float* hc = hb + (size_t)3 * K * Dp;
     float* hmu = hc + 3 * K;
     std::vector<float> hlrw(2 * K, 0.f);
+    std::vector<double> hcb(3 * (size_t)K, 0.0);   // -log det Sigma / 2 per slot (kept for the outlier layout)
     DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));   // the pinned stage may still be in flight
     // every slot is independent: pack them in parallel, keep the first error
     int err_slot = -1;
@@ -697,6 +699,7 @@ static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, con
                 st = DPMM_ERR_NOT_PD;
             }
             double cval = -ld / 2;
+            hcb[q] = cval;
             if (!sub) cval += std::log(weights[k]);
             if (st == DPMM_OK && !std::isfinite(cval) && !(cval < 0)) st = DPMM_ERR_NUMERIC;
             if (st != DPMM_OK) {
@@ -722,6 +725,8 @@ static dpmm_status upload_gauss_params(dpmm_ctx* c, int K, const double* mu, con
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c, hc, sizeof(float) * 3 * K, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu, hmu, sizeof(float) * 3 * K * (size_t)Dp, cudaMemcpyHostToDevice, c->stream));
     DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hlrw.data(), sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
+    if (c->d_cbase)
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_cbase, hcb.data(), sizeof(double) * 3 * K, cudaMemcpyHostToDevice, c->stream));
     g_h2d_bytes += sizeof(float) * 3 * (size_t)K * ((size_t)Dp * Dp + 2 * Dp + 1) + sizeof(float) * 2 * K;
     {
         PhaseTimer pt(c, PH_PARAMS);
@@ -946,6 +951,32 @@ extern "C" dpmm_status dpmm_split_clusters(dpmm_ctx* c, int n, const int32_t* in
         invalidate_stats(c, index[i]);
         invalidate_stats(c, new_index[i]);
     }
+    if (c->outlier_layout) {
+        // create_splittable_from_params (local_clusters_actions.cpp:264-285): the new cluster starts
+        // from the parent's r sub-cluster parameters.  Drawn at the next iteration like every cluster,
+        // except when it is renumbered to index 1 before that, which is never redrawn (:348-351).
+        for (int i = 0; i < n; ++i) {
+            if (index[i] >= c->K_params) continue;
+            const size_t src = 3 * (size_t)index[i] + 2;
+            for (int s = 0; s < 3; ++s) {
+                const size_t dst = 3 * (size_t)new_index[i] + s;
+                if (c->prior == DPMM_PRIOR_GAUSSIAN) {
+                    const size_t m = (size_t)c->Dp * c->Dp;
+                    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_Wt + dst * m, c->d_Wt + src * m, sizeof(float) * m,
+                                                  cudaMemcpyDeviceToDevice, c->stream));
+                    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_b + dst * c->Dp, c->d_b + src * c->Dp, sizeof(float) * c->Dp,
+                                                  cudaMemcpyDeviceToDevice, c->stream));
+                    if (c->d_cbase)
+                        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_cbase + dst, c->d_cbase + src, sizeof(double),
+                                                      cudaMemcpyDeviceToDevice, c->stream));
+                }
+                DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu + dst * c->Dp, c->d_mu + src * c->Dp, sizeof(float) * c->Dp,
+                                              cudaMemcpyDeviceToDevice, c->stream));
+                DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c + dst, c->d_c + src, sizeof(float), cudaMemcpyDeviceToDevice,
+                                              c->stream));
+            }
+        }
+    }
     return DPMM_OK;
 }
 
@@ -1118,6 +1149,61 @@ extern "C" dpmm_status dpmm_set_prior_niw(dpmm_ctx* c, double k, const double* m
     std::memcpy(h.data() + D, psi, sizeof(double) * D * D);
     DPMM_CUDA_TRY(cudaMemcpy(c->d_prior, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
     c->prior_set = true;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_outlier_prior_niw(dpmm_ctx* c, double k, const double* m, double v, const double* psi)
+{
+    if (!c || !m || !psi) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_GAUSSIAN) return fail(DPMM_ERR_STATE, "context is not Gaussian");
+    const int D = c->D;
+    std::vector<double> L;
+    if (!la::cholesky(psi, D, L)) return fail(DPMM_ERR_NOT_PD, "outlier prior psi is not positive definite");
+    if (!c->d_prior2) DPMM_TRY(dev_alloc(&c->d_prior2, (size_t)D + (size_t)D * D));
+    if (!c->d_prior_sel) {
+        DPMM_TRY(dev_alloc(&c->d_prior_sel, (size_t)c->k_max));
+        DPMM_CUDA_TRY(cudaMemset(c->d_prior_sel, 0, (size_t)c->k_max));
+    }
+    std::vector<double> h((size_t)D + D * D);
+    std::memcpy(h.data(), m, sizeof(double) * D);
+    std::memcpy(h.data() + D, psi, sizeof(double) * D * D);
+    DPMM_CUDA_TRY(cudaMemcpy(c->d_prior2, h.data(), sizeof(double) * h.size(), cudaMemcpyHostToDevice));
+    c->prior2_logdet = la::logdet_from_chol(L, D);
+    c->prior2_k = k;
+    c->prior2_v = v;
+    if (!c->d_cbase) {
+        DPMM_TRY(dev_alloc(&c->d_cbase, 3 * (size_t)c->k_max));
+        DPMM_CUDA_TRY(cudaMemset(c->d_cbase, 0, sizeof(double) * 3 * (size_t)c->k_max));
+    }
+    c->outlier_layout = 1;
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_cluster_priors(dpmm_ctx* c, int K, const uint8_t* second)
+{
+    if (!c || (K > 0 && !second)) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (K < 0 || K > c->k_max) return fail(DPMM_ERR_INVALID_ARG, "K out of range [0, k_max]");
+    if (!c->outlier_layout) return fail(DPMM_ERR_STATE, "no outlier prior set");
+    if (K == 0) return DPMM_OK;
+    uint8_t* h = reinterpret_cast<uint8_t*>(c->h_pinned) + sizeof(double) * 3 * (size_t)c->k_max;
+    DPMM_CUDA_TRY(cudaStreamSynchronize(c->stream));   // the pinned stage may still be in flight
+    std::memcpy(h, second, (size_t)K);
+    DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_prior_sel, h, (size_t)K, cudaMemcpyHostToDevice, c->stream));
+    g_h2d_bytes.fetch_add((size_t)K, std::memory_order_relaxed);
+    return DPMM_OK;
+}
+
+extern "C" dpmm_status dpmm_set_outlier_prior_multinomial(dpmm_ctx* c, const double* alpha)
+{
+    if (!c || !alpha) return fail(DPMM_ERR_INVALID_ARG, "null argument");
+    if (c->prior != DPMM_PRIOR_MULTINOMIAL) return fail(DPMM_ERR_STATE, "context is not multinomial");
+    if (!c->d_prior2) DPMM_TRY(dev_alloc(&c->d_prior2, (size_t)c->D));
+    if (!c->d_prior_sel) {
+        DPMM_TRY(dev_alloc(&c->d_prior_sel, (size_t)c->k_max));
+        DPMM_CUDA_TRY(cudaMemset(c->d_prior_sel, 0, (size_t)c->k_max));
+    }
+    DPMM_CUDA_TRY(cudaMemcpy(c->d_prior2, alpha, sizeof(double) * c->D, cudaMemcpyHostToDevice));
+    c->outlier_layout = 1;
     return DPMM_OK;
 }
 

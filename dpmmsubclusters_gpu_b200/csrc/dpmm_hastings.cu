@@ -17,12 +17,21 @@
 namespace dpmm {
 
 // one block per slot (3K): log marginal likelihood of each cluster / sub-cluster
+// sel (nullable): clusters whose slots use the second prior (k1, v1, ld1, prior1), the outlier layout
 template <int DP>
 __global__ void __launch_bounds__(RegChol<DP>::T) k_slot_lml(const double* __restrict__ stats, int stat_len, int D,
                                                              int gauss, double k0, double v0, double ld0,
-                                                             const double* __restrict__ prior, double* __restrict__ lml)
+                                                             const double* __restrict__ prior, double k1, double v1,
+                                                             double ld1, const double* __restrict__ prior1,
+                                                             const uint8_t* __restrict__ sel, double* __restrict__ lml)
 {
     __shared__ double sh[RegChol<DP>::SMEM];
+    if (sel && sel[blockIdx.x / 3]) {
+        k0 = k1;
+        v0 = v1;
+        ld0 = ld1;
+        prior = prior1;
+    }
     const double* st = stats + (size_t)blockIdx.x * stat_len;
     double v;
     if (gauss)
@@ -41,10 +50,13 @@ __global__ void k_split_hr(const double* __restrict__ stats, int stat_len, const
 }
 
 // one block per pair i < j: statistics aggregated (niw.cpp:140-148), posterior, lml, ratio
+// the merged cluster takes cluster i's prior (shared_actions.cpp:88-95): the second one where sel[i]
 template <int DP>
 __global__ void __launch_bounds__(RegChol<DP>::T) k_merge_hr(const double* __restrict__ stats, int stat_len, int D,
                                                              int gauss, double k0, double v0, double ld0,
-                                                             const double* __restrict__ prior,
+                                                             const double* __restrict__ prior, double k1, double v1,
+                                                             double ld1, const double* __restrict__ prior1,
+                                                             const uint8_t* __restrict__ sel,
                                                              const double* __restrict__ lml, int K, double alpha,
                                                              double* __restrict__ hr)
 {
@@ -55,6 +67,12 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_merge_hr(const double* __res
     long long rowlen = K - 1;
     while (b >= rowlen) { b -= rowlen; ++i; --rowlen; }
     const int j = i + 1 + (int)b;
+    if (sel && sel[i]) {
+        k0 = k1;
+        v0 = v1;
+        ld0 = ld1;
+        prior = prior1;
+    }
     const double v = merge_log_hr_reg<DP>(stats, stat_len, D, gauss, k0, v0, ld0, prior, lml, i, j, alpha, sh);
     if (threadIdx.x == 0) hr[(size_t)i * K + j] = v;
 }
@@ -65,9 +83,11 @@ static int chol_dp(const dpmm_ctx* c) { return c->prior == DPMM_PRIOR_GAUSSIAN ?
 static dpmm_status launch_slot_lml(dpmm_ctx* c, int K)
 {
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    const bool out = c->outlier_layout != 0;
     DPMM_WITH_DP(chol_dp(c), (k_slot_lml<DP><<<3 * K, RegChol<DP>::T, 0, c->stream>>>(
                                  c->d_stats, c->stat_len, c->D, gauss, c->prior_k, c->prior_v, c->prior_logdet,
-                                 c->d_prior, c->d_lml)));
+                                 c->d_prior, c->prior2_k, c->prior2_v, c->prior2_logdet,
+                                 out ? c->d_prior2 : c->d_prior, out ? c->d_prior_sel : nullptr, c->d_lml)));
     DPMM_LAUNCHED();
     return DPMM_OK;
 }
@@ -102,9 +122,11 @@ dpmm_status launch_merge_hastings(dpmm_ctx* c, int K, double alpha)
     const long long pairs = (long long)K * (K - 1) / 2;
     if (pairs == 0) return DPMM_OK;
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    const bool out = c->outlier_layout != 0;
     DPMM_WITH_DP(chol_dp(c), (k_merge_hr<DP><<<(unsigned)pairs, RegChol<DP>::T, 0, c->stream>>>(
                                  c->d_stats, c->stat_len, c->D, gauss, c->prior_k, c->prior_v, c->prior_logdet,
-                                 c->d_prior, c->d_lml, K, alpha, c->d_merge_hr)));
+                                 c->d_prior, c->prior2_k, c->prior2_v, c->prior2_logdet, out ? c->d_prior2 : c->d_prior,
+                                 out ? c->d_prior_sel : nullptr, c->d_lml, K, alpha, c->d_merge_hr)));
     DPMM_LAUNCHED();
     return DPMM_OK;
 }

@@ -176,6 +176,13 @@ struct dpmm_ctx {
     double prior_logdet = 0;       // log det psi0 (NIW)
     bool prior_identity = false;   // NIW prior with m0 = 0 and psi0 = I
     double* d_prior = nullptr;     // NIW: m[D], psi[D*D]; multinomial: alpha[D]
+    // runs with an outlier cluster (local_clusters_actions.cpp:48-79, 341-371): cluster 0 has its own
+    // prior (its slots are drawn from this one's posterior), cluster 1's parameters are not redrawn
+    int outlier_layout = 0;
+    double prior2_k = 0, prior2_v = 0, prior2_logdet = 0;
+    double* d_prior2 = nullptr;    // like d_prior
+    uint8_t* d_prior_sel = nullptr;  // [k_max] 1: the cluster's slots use the second prior
+    double* d_cbase = nullptr;     // [3*k_max] -log det Sigma / 2 of each slot's current parameters (NIW)
     double* d_lml = nullptr;       // [3*k_max]
     double* d_split_hr = nullptr;  // [k_max]
     double* d_merge_hr = nullptr;  // [k_max*k_max]

@@ -87,10 +87,18 @@ __device__ double chi2_draw(double k, uint64_t seed, uint64_t draw, uint32_t s, 
 
 // element ids of the random streams of one slot: A(i, j) below the diagonal uses e = j D + i; the
 // diagonal i uses 256 ids from D*D + 256 i; z uses D*D + 256 D + i
+// Outlier layout (sel != nullptr): the slots of clusters with sel[k] = 1 (the outlier cluster and the
+// clusters split from it) use the second prior (k1, v1, ld1, prior1); slots [skip_lo, skip_hi)
+// (cluster 1, local_clusters_actions.cpp:348-351) keep their parameters: only their log marginal
+// likelihood and the cluster slot's weight term are refreshed (cbase[s] = -log det Sigma / 2 of the
+// slot's current parameters, written by every draw).
 template <int DP>
 __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __restrict__ stats, int stat_len, int D,
                                                               int Dp, double k0, double v0, double ld0,
-                                                              const double* __restrict__ prior,
+                                                              const double* __restrict__ prior, double k1, double v1,
+                                                              double ld1, const double* __restrict__ prior1,
+                                                              const uint8_t* __restrict__ sel, int skip_lo,
+                                                              int skip_hi, double* __restrict__ cbase,
                                                               const double* __restrict__ shift,
                                                               const double* __restrict__ logw, uint64_t seed,
                                                               uint64_t draw, float* __restrict__ Wt,
@@ -106,6 +114,12 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __res
     double* Am = Lm + (size_t)D * D;       // D*AL: Bartlett factor (lower)
     double* red = sh + 3 * DP;
     const int s = blockIdx.x, t = threadIdx.x;
+    if (sel && sel[s / 3]) {   // the outlier prior
+        k0 = k1;
+        v0 = v1;
+        ld0 = ld1;
+        prior = prior1;
+    }
     const double* st = stats + (size_t)s * stat_len;
     const double n = st[0];
     const double kp = k0 + n, vp = v0 + n;
@@ -114,6 +128,13 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __res
     NiwExtras ex;
     const double L = niw_lml_reg<DP>(D, n, st + 1, st + 1 + D, nullptr, nullptr, k0, v0, prior, prior + D, ld0, sh,
                                      &ex, Lm, true);
+    if (s >= skip_lo && s < skip_hi) {   // parameters kept (uniform over the block)
+        if (t == 0) {
+            lml[s] = n > 0 ? L : 0.0;
+            if (s % 3 == 0) cv[s] = (float)(cbase[s] + logw[s / 3]);
+        }
+        return;
+    }
     const double* mp = sh + 2 * DP;        // posterior mean, left by niw_lml_reg
     const uint32_t us = (uint32_t)s;
     for (int e = t; e < D * D; e += blockDim.x) {
@@ -177,6 +198,7 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __res
     }
     if (t == 0) {
         const double cval = -logdet_sigma / 2 + (s % 3 == 0 ? logw[s / 3] : 0.0);
+        if (cbase) cbase[s] = -logdet_sigma / 2;
         cv[s] = (float)cval;
         lml[s] = n > 0 ? L : 0.0;
         if (isnan(cval) || cval == INFINITY || !isfinite(ex.ld)) atomicCAS(err, 0, s + 1);
@@ -191,20 +213,27 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_draw_niw(const double* __res
 // posterior is the prior) for the splittable test.  One block per slot; element d draws from the
 // Philox streams 256 d .. 256 d + 201 of (slot, draw).
 __global__ void __launch_bounds__(256) k_draw_dirichlet(const double* __restrict__ stats, int stat_len, int D, int Dp,
-                                                        const double* __restrict__ alpha0, uint64_t seed,
-                                                        uint64_t draw, float* __restrict__ lt,
-                                                        float* __restrict__ cv, double* __restrict__ lml)
+                                                        const double* __restrict__ alpha0,
+                                                        const double* __restrict__ alpha1,
+                                                        const uint8_t* __restrict__ sel, int skip_lo, int skip_hi,
+                                                        uint64_t seed, uint64_t draw,
+                                                        float* __restrict__ lt, float* __restrict__ cv,
+                                                        double* __restrict__ lml)
 {
     __shared__ double red[33];
     const int s = blockIdx.x, t = threadIdx.x;
+    if (sel && sel[s / 3]) alpha0 = alpha1;   // the outlier prior
+    const bool keep = s >= skip_lo && s < skip_hi;   // parameters kept: the marginal likelihood only
     const double* st = stats + (size_t)s * stat_len;
     const double n = st[0];
     double gsum = 0, a0 = 0, ap = 0, lg = 0;
     for (int d = t; d < D; d += blockDim.x) {
         const double a = alpha0[d], a1 = a + st[1 + d];
-        const double g = fmax(0.5 * chi2_draw(2.0 * a1, seed, draw, (uint32_t)s, (uint32_t)(256 * d)), 1e-300);
-        lt[(size_t)s * Dp + d] = (float)log(g);   // log g for now: the normalisation follows
-        gsum += g;
+        if (!keep) {
+            const double g = fmax(0.5 * chi2_draw(2.0 * a1, seed, draw, (uint32_t)s, (uint32_t)(256 * d)), 1e-300);
+            lt[(size_t)s * Dp + d] = (float)log(g);   // log g for now: the normalisation follows
+            gsum += g;
+        }
         a0 += a;
         ap += a1;
         lg += lgamma(a1) - lgamma(a);
@@ -213,10 +242,12 @@ __global__ void __launch_bounds__(256) k_draw_dirichlet(const double* __restrict
     a0 = block_sum(a0, red);
     ap = block_sum(ap, red);
     lg = block_sum(lg, red);
-    const float lz = (float)log(gsum);
-    for (int d = t; d < Dp; d += blockDim.x) lt[(size_t)s * Dp + d] = d < D ? lt[(size_t)s * Dp + d] - lz : 0.f;
+    if (!keep) {
+        const float lz = (float)log(gsum);
+        for (int d = t; d < Dp; d += blockDim.x) lt[(size_t)s * Dp + d] = d < D ? lt[(size_t)s * Dp + d] - lz : 0.f;
+    }
     if (t == 0) {
-        cv[s] = 0.f;       // the multinomial cluster log-likelihood has no weight term (cudaKernel_multinomial.cu:60-76)
+        if (!keep) cv[s] = 0.f;   // the multinomial cluster log-likelihood has no weight term (cudaKernel_multinomial.cu:60-76)
         lml[s] = n > 0 ? lgamma(a0) - lgamma(ap) + lg : 0.0;
     }
 }
@@ -255,9 +286,12 @@ static dpmm_status launch_draw_niw(dpmm_ctx* c, int K, uint64_t seed, uint64_t d
     } else {
         const size_t sm = sizeof(double) * ((size_t)c->D * c->D + (size_t)c->D * (c->D + 1));
         DPMM_TRY(allow_smem(k_draw_niw<DP>, sm));
+        const bool out = c->outlier_layout != 0;
         k_draw_niw<DP><<<3 * K, RegChol<DP>::T, sm, c->stream>>>(
-            c->d_stats, c->stat_len, c->D, c->Dp, c->prior_k, c->prior_v, c->prior_logdet, c->d_prior, c->d_gshift,
-            c->d_logw, seed, draw, c->d_Wt, c->d_b, c->d_c, c->d_mu, c->d_lml, c->d_aux + 6);
+            c->d_stats, c->stat_len, c->D, c->Dp, c->prior_k, c->prior_v, c->prior_logdet, c->d_prior, c->prior2_k,
+            c->prior2_v, c->prior2_logdet, out ? c->d_prior2 : c->d_prior, out ? c->d_prior_sel : nullptr,
+            out ? 3 : 0, out && K > 1 ? 6 : 0, c->d_cbase, c->d_gshift, c->d_logw, seed, draw, c->d_Wt, c->d_b, c->d_c, c->d_mu,
+            c->d_lml, c->d_aux + 6);
         return DPMM_OK;
     }
 }
@@ -331,7 +365,11 @@ extern "C" dpmm_status dpmm_sample_multinomial_params(dpmm_ctx* c, int K, uint64
         PhaseTimer pt(c, PH_PARAMS);
         DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw, hl, sizeof(float) * 2 * K, cudaMemcpyHostToDevice, c->stream));
         g_h2d_bytes.fetch_add(sizeof(float) * 2 * K, std::memory_order_relaxed);
-        k_draw_dirichlet<<<3 * K, 256, 0, c->stream>>>(c->d_stats, c->stat_len, c->D, c->Dp, c->d_prior, seed, draw,
+        const bool out = c->outlier_layout != 0;
+        k_draw_dirichlet<<<3 * K, 256, 0, c->stream>>>(c->d_stats, c->stat_len, c->D, c->Dp, c->d_prior,
+                                                        out ? c->d_prior2 : c->d_prior,
+                                                        out ? c->d_prior_sel : nullptr, out ? 3 : 0,
+                                                        out && K > 1 ? 6 : 0, seed, draw,
                                                        c->d_mu, c->d_c, c->d_lml);
         DPMM_LAUNCHED();
         c->K_params = K;
@@ -381,6 +419,27 @@ extern "C" dpmm_status dpmm_compact_statistics(dpmm_ctx* c, int n_keep, const in
     k_compact_stats<<<n_keep, 256, 0, c->stream>>>(c->d_stats, c->d_stats_tmp, c->stat_len, c->d_remap);
     DPMM_LAUNCHED();
     std::swap(c->d_stats, c->d_stats_tmp);
+    if (c->outlier_layout && n_keep > 1 && keep[1] != 1 && c->K_params > keep[1]) {
+        // cluster 1's parameters are not redrawn (local_clusters_actions.cpp:348-351): the cluster that
+        // moves into index 1 brings its current ones (device to device, the 3 slots are contiguous)
+        const size_t s0 = 3 * (size_t)keep[1], s1 = 3;
+        if (c->prior == DPMM_PRIOR_GAUSSIAN) {
+            const size_t m = (size_t)c->Dp * c->Dp;
+            DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_Wt + s1 * m, c->d_Wt + s0 * m, sizeof(float) * 3 * m,
+                                          cudaMemcpyDeviceToDevice, c->stream));
+            DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_b + s1 * c->Dp, c->d_b + s0 * c->Dp, sizeof(float) * 3 * c->Dp,
+                                          cudaMemcpyDeviceToDevice, c->stream));
+            if (c->d_cbase)
+                DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_cbase + s1, c->d_cbase + s0, sizeof(double) * 3,
+                                              cudaMemcpyDeviceToDevice, c->stream));
+        }
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_mu + s1 * c->Dp, c->d_mu + s0 * c->Dp, sizeof(float) * 3 * c->Dp,
+                                      cudaMemcpyDeviceToDevice, c->stream));
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_c + s1, c->d_c + s0, sizeof(float) * 3, cudaMemcpyDeviceToDevice,
+                                      c->stream));
+        DPMM_CUDA_TRY(cudaMemcpyAsync(c->d_lrw + 2, c->d_lrw + 2 * (size_t)keep[1], sizeof(float) * 2,
+                                      cudaMemcpyDeviceToDevice, c->stream));
+    }
     std::vector<uint8_t> ok(c->k_max, 0);
     for (int k = 0; k < n_keep; ++k) ok[k] = c->stats_ok[keep[k]];
     c->stats_ok = ok;

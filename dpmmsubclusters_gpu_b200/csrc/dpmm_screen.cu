@@ -687,15 +687,25 @@ __global__ void __launch_bounds__(kTopThreads) k_screen_topk(const float* __rest
 
 // ------------------------------------------------------------------------------ exact ratios of a list
 // log marginal likelihood of the listed slots (the arithmetic of k_slot_lml), one block per slot
+// (sel, nullable: clusters whose slots use the second prior k1, v1, ld1, prior1 -- the outlier layout)
 template <int DP>
 __global__ void __launch_bounds__(RegChol<DP>::T) k_slot_lml_list(const double* __restrict__ stats, int stat_len, int D,
                                                                    int gauss, double k0, double v0, double ld0,
-                                                                   const double* __restrict__ prior,
+                                                                   const double* __restrict__ prior, double k1,
+                                                                   double v1, double ld1,
+                                                                   const double* __restrict__ prior1,
+                                                                   const uint8_t* __restrict__ sel,
                                                                    const int32_t* __restrict__ slots,
                                                                    double* __restrict__ lml)
 {
     __shared__ double sh[RegChol<DP>::SMEM];
     const int s = slots[blockIdx.x];
+    if (sel && sel[s / 3]) {
+        k0 = k1;
+        v0 = v1;
+        ld0 = ld1;
+        prior = prior1;
+    }
     const double* st = stats + (size_t)s * stat_len;
     double v;
     if (gauss)
@@ -705,17 +715,27 @@ __global__ void __launch_bounds__(RegChol<DP>::T) k_slot_lml_list(const double* 
     if (threadIdx.x == 0) lml[s] = v;
 }
 
-// exact merge ratios of the listed pairs (the arithmetic of k_merge_hr), one block per pair
+// exact merge ratios of the listed pairs (the arithmetic of k_merge_hr), one block per pair; the merged
+// cluster takes cluster i's prior (shared_actions.cpp:88-95)
 template <int DP>
 __global__ void __launch_bounds__(RegChol<DP>::T) k_merge_hr_list(const double* __restrict__ stats, int stat_len, int D,
                                                                    int gauss, double k0, double v0, double ld0,
-                                                                   const double* __restrict__ prior,
+                                                                   const double* __restrict__ prior, double k1,
+                                                                   double v1, double ld1,
+                                                                   const double* __restrict__ prior1,
+                                                                   const uint8_t* __restrict__ sel,
                                                                    const double* __restrict__ lml,
                                                                    const int32_t* __restrict__ pairs, double alpha,
                                                                    double* __restrict__ out)
 {
     __shared__ double sh[RegChol<DP>::SMEM];
     const int i = pairs[2 * blockIdx.x], j = pairs[2 * blockIdx.x + 1];
+    if (sel && sel[i]) {
+        k0 = k1;
+        v0 = v1;
+        ld0 = ld1;
+        prior = prior1;
+    }
     const double v = merge_log_hr_reg<DP>(stats, stat_len, D, gauss, k0, v0, ld0, prior, lml, i, j, alpha, sh);
     if (threadIdx.x == 0) out[blockIdx.x] = v;
 }
@@ -965,14 +985,18 @@ dpmm_status launch_hastings_list(dpmm_ctx* c, int K, int kind, double alpha, int
     const int gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     if (n == 0) return DPMM_OK;
     const int dp = gauss ? c->Dp : 4;
+    const bool out2 = c->outlier_layout != 0;
+    const double* p2 = out2 ? c->d_prior2 : c->d_prior;
+    const uint8_t* sel = out2 ? c->d_prior_sel : nullptr;
     DPMM_WITH_DP(dp, (k_slot_lml_list<DP><<<nslots, RegChol<DP>::T, 0, c->stream>>>(
                          c->d_stats, c->stat_len, c->D, gauss, c->prior_k, c->prior_v, c->prior_logdet, c->d_prior,
-                         c->d_scr_slots, c->d_lml)));
+                         c->prior2_k, c->prior2_v, c->prior2_logdet, p2, sel, c->d_scr_slots, c->d_lml)));
     DPMM_LAUNCHED();
     if (kind == DPMM_SCREEN_MERGE) {
         DPMM_WITH_DP(dp, (k_merge_hr_list<DP><<<n, RegChol<DP>::T, 0, c->stream>>>(
                              c->d_stats, c->stat_len, c->D, gauss, c->prior_k, c->prior_v, c->prior_logdet, c->d_prior,
-                             c->d_lml, c->d_scr_list, alpha, c->d_scr_hr)));
+                             c->prior2_k, c->prior2_v, c->prior2_logdet, p2, sel, c->d_lml, c->d_scr_list, alpha,
+                             c->d_scr_hr)));
     } else {
         k_split_hr_list<<<(n + 127) / 128, 128, 0, c->stream>>>(c->d_stats, c->stat_len, c->d_lml, c->d_scr_list, n,
                                                                 alpha, c->d_scr_hr);

@@ -33,6 +33,7 @@ namespace dpmm {
 namespace host {
 
 struct Hyper {               // niw_hyperparams {k, m, v, psi} / multinomial_hyper {alpha}
+    bool outlier = false;        // the outlier cluster's prior (outlier_hyper_params)
     double k = 0, v = 0;
     std::vector<double> m, psi;
     std::vector<double> chol;    // lower Cholesky factor of psi (NIW)
@@ -99,9 +100,15 @@ public:
     Sampler(const Config& cfg, dpmm_ctx* ctx, int64_t N, int D)
         : cfg_(cfg), ctx_(ctx), N_(N), Ntot_(ctx->n_total), D_(D), gen_((unsigned long)cfg.seed)
     {
-        // device-resident parameters: the NIW draws run on the device from the device statistics,
-        // the host keeps counts only (the outlier cluster's own prior stays on the host path)
-        dev_ = !(cfg.outlier_mod > 0) && !cfg.host_param_draws && (cfg.prior == DPMM_PRIOR_MULTINOMIAL || D <= 64);
+        // device-resident parameters: the draws run on the device from the device statistics, the
+        // host keeps counts only (and the outlier cluster's full statistics, for its split ratio)
+        dev_ = device_draws(cfg, D);
+        cfg_.outlier_hyper.outlier = true;
+    }
+
+    static bool device_draws(const Config& cfg, int D)
+    {
+        return !cfg.host_param_draws && (cfg.prior == DPMM_PRIOR_MULTINOMIAL || D <= 64);
     }
 
     // init_model + init_first_clusters, then iterations first..first+n-1 of run_model
@@ -314,6 +321,8 @@ private:
     // ----------------------------------------------------------------- device glue
     dpmm_status upload_params(const std::vector<double>& weights);
     dpmm_status update_suff_stats_posterior(const std::vector<int32_t>& indices);
+    dpmm_status host_stats_posterior(const std::vector<int32_t>& indices);
+    dpmm_status sync_prior_select();
     void sample_cluster_params_all();
     dpmm_status sample_clusters();
     dpmm_status sample_clusters_device();
@@ -406,6 +415,18 @@ dpmm_status Sampler::upload_params(const std::vector<double>& weights)
                                      ld_lr.data(), lrw.data());
 }
 
+// runs with an outlier cluster: which clusters carry the outlier prior (the outlier cluster and the
+// clusters split from it, as their host bookkeeping does), before every device launch that reads the
+// priors (draws, marginal likelihoods, split and merge ratios: each cluster's own prior, as
+// should_split_local and should_merge use, local_clusters_actions.cpp:215-239, shared_actions.cpp:88-95)
+dpmm_status Sampler::sync_prior_select()
+{
+    if (!(cfg_.outlier_mod > 0) || clusters_.empty()) return DPMM_OK;
+    std::vector<uint8_t> sel(clusters_.size());
+    for (size_t k = 0; k < clusters_.size(); ++k) sel[k] = clusters_[k].c.prior.outlier ? 1 : 0;
+    return dpmm_set_cluster_priors(ctx_, (int)sel.size(), sel.data());
+}
+
 // local_clusters_actions::update_suff_stats_posterior (local_clusters_actions.cpp:103-168)
 dpmm_status Sampler::update_suff_stats_posterior(const std::vector<int32_t>& indices)
 {
@@ -414,15 +435,27 @@ dpmm_status Sampler::update_suff_stats_posterior(const std::vector<int32_t>& ind
     if (dev_) {   // the statistics stay on the device; the host bookkeeping needs the counts
         std::vector<int64_t> cnt(3 * (size_t)n);
         DPMM_TRY(dpmm_statistics_counts(ctx_, n, indices.data(), cnt.data()));
+        bool outlier_listed = false;
         for (int q = 0; q < n; ++q) {
             Splittable& sc = clusters_[indices[q]];
             sc.c.stats.N = cnt[3 * (size_t)q];
             sc.l.stats.N = cnt[3 * (size_t)q + 1];
             sc.r.stats.N = cnt[3 * (size_t)q + 2];
             sc.points_count = sc.c.stats.N;
+            outlier_listed |= cfg_.outlier_mod > 0 && indices[q] == 0;
         }
+        // the outlier cluster's split ratio is evaluated on the host (its own prior): its full
+        // statistics and posteriors
+        if (outlier_listed) return host_stats_posterior({0});
         return DPMM_OK;
     }
+    return host_stats_posterior(indices);
+}
+
+// the statistics of the listed clusters downloaded, and their posteriors
+dpmm_status Sampler::host_stats_posterior(const std::vector<int32_t>& indices)
+{
+    const int n = (int)indices.size();
     const int D = D_;
     const bool gauss = cfg_.prior == DPMM_PRIOR_GAUSSIAN;
     std::vector<int64_t> cnt(3 * (size_t)n);
@@ -529,14 +562,19 @@ void Sampler::mixture_weights()
 dpmm_status Sampler::sample_clusters_device()
 {
     const int K = (int)clusters_.size();
+    const bool outlier = cfg_.outlier_mod > 0;
+    DPMM_TRY(sync_prior_select());
     std::vector<double> lrw(2 * (size_t)K);
     for (int i = 0; i < K; ++i) {
         Splittable& sc = clusters_[i];
-        std::vector<double> w = dirichlet({(double)sc.l.stats.N + cfg_.alpha / 2, (double)sc.r.stats.N + cfg_.alpha / 2});
-        sc.lrw[0] = w[0];
-        sc.lrw[1] = w[1];
-        lrw[2 * i] = w[0];
-        lrw[2 * i + 1] = w[1];
+        if (!(outlier && i == 1)) {   // cluster 1 is not redrawn with an outlier cluster (:348-351)
+            std::vector<double> w =
+                dirichlet({(double)sc.l.stats.N + cfg_.alpha / 2, (double)sc.r.stats.N + cfg_.alpha / 2});
+            sc.lrw[0] = w[0];
+            sc.lrw[1] = w[1];
+        }
+        lrw[2 * i] = sc.lrw[0];
+        lrw[2 * i + 1] = sc.lrw[1];
     }
     mixture_weights();
     std::vector<double> w(K, 0.0), lml(3 * (size_t)K);
@@ -548,6 +586,7 @@ dpmm_status Sampler::sample_clusters_device()
     draw_ctr_ += 3 * (uint64_t)K;
     const int B = cfg_.burnout;
     for (int i = 0; i < K; ++i) {
+        if (outlier && i == 1) continue;
         Splittable& sc = clusters_[i];
         for (int q = 0; q < B - 1; ++q) sc.hist[q] = sc.hist[q + 1];
         sc.hist[B - 1] = std::make_pair(true, lml[3 * (size_t)i + 1] + lml[3 * (size_t)i + 2]);
@@ -606,6 +645,7 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
     std::vector<double> hr(K, NAN);
     std::vector<uint8_t> in_sel(K, 0);
     const ScreenUse use = screen_use(ncand, cfg_.screen_split_min);
+    DPMM_TRY(sync_prior_select());
     if (use != USE_FULL && ncand > 0) {
         std::vector<int32_t> sel(kScrMaxTop);
         int32_t nsel = 0;
@@ -713,6 +753,7 @@ dpmm_status Sampler::check_and_merge(bool final_)
         m += elig[i];
     }
     const int64_t ncand = m * (m - 1) / 2;
+    DPMM_TRY(sync_prior_select());
     const ScreenUse use = screen_use(ncand);
     // proposals in (i, j) order with their ratios
     struct Prop {
@@ -944,6 +985,12 @@ dpmm_status Sampler::init_first_clusters()
     std::vector<int32_t> all(clusters_.size());
     std::iota(all.begin(), all.end(), 0);
     DPMM_TRY(update_suff_stats_posterior(all));
+    if (dev_ && cfg_.outlier_mod > 0) {
+        // cluster 1 keeps its initial draw (it is not redrawn with an outlier cluster): the host's
+        // initial parameters go to the device once, the device draws then replace the others
+        std::vector<double> w(clusters_.size(), 1.0 / (double)clusters_.size());
+        DPMM_TRY(upload_params(w));
+    }
     return sample_clusters();
 }
 
@@ -955,6 +1002,7 @@ dpmm_status Sampler::calculate_posterior(double* out)
     std::vector<double> dl;
     if (dev_ && !clusters_.empty()) {
         dl.resize(3 * clusters_.size());
+        DPMM_TRY(sync_prior_select());
         DPMM_TRY(slot_lml_as_is(ctx_, (int)clusters_.size(), dl.data()));
     }
     for (size_t k = 0; k < clusters_.size(); ++k) {
@@ -1109,6 +1157,11 @@ dpmm_status make_sampler(const Config& cfg_in, int64_t N, int D, const void* poi
         DPMM_TRY(dpmm_set_prior_niw(h->ctx, cfg.hyper.k, cfg.hyper.m.data(), cfg.hyper.v, cfg.hyper.psi.data()));
     else
         DPMM_TRY(dpmm_set_prior_multinomial(h->ctx, cfg.hyper.alpha.data()));
+    if (cfg.outlier_mod > 0) {   // the outlier prior on the device: its clusters' draws and ratios
+        const host::Hyper& o = cfg.outlier_hyper;
+        if (cfg.prior == DPMM_PRIOR_GAUSSIAN) DPMM_TRY(dpmm_set_outlier_prior_niw(h->ctx, o.k, o.m.data(), o.v, o.psi.data()));
+        else DPMM_TRY(dpmm_set_outlier_prior_multinomial(h->ctx, o.alpha.data()));
+    }
     if (h->ctx->d_prune_rh) DPMM_TRY(dpmm_set_label_pruning(h->ctx, cfg.label_prune_margin));
     if (cfg.verbose && !cfg.gt.empty()) {
         if ((int64_t)cfg.gt.size() != N) return fail(DPMM_ERR_INVALID_ARG, "ground truth needs one value per point");

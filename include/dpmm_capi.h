@@ -248,6 +248,16 @@ dpmm_status dpmm_sample_log_cat_array_sub_cluster(dpmm_ctx* ctx, int m, const do
  * multinomial_hyper{alpha} (priors/multinomial_hyper.h:9-29). */
 dpmm_status dpmm_set_prior_niw(dpmm_ctx* ctx, double k, const double* m, double v, const double* psi);
 dpmm_status dpmm_set_prior_multinomial(dpmm_ctx* ctx, const double* alpha);
+/* Runs with an outlier cluster (outlier_mod > 0: create_outlier_local_cluster and sample_clusters,
+ * local_clusters_actions.cpp:48-79, 341-371) with device draws: the outlier cluster's own prior
+ * (outlier_hyper_params) for the clusters that carry it, chosen per cluster by
+ * dpmm_set_cluster_priors (second[k] != 0: cluster k uses it; the outlier cluster and the clusters
+ * split from it), in the device draws and the device marginal likelihoods; and, as the reference,
+ * cluster 1's parameters are not redrawn (its marginal likelihood and weight term are refreshed),
+ * and move with it when dpmm_compact_statistics renumbers the clusters. */
+dpmm_status dpmm_set_outlier_prior_niw(dpmm_ctx* ctx, double k, const double* m, double v, const double* psi);
+dpmm_status dpmm_set_outlier_prior_multinomial(dpmm_ctx* ctx, const double* alpha);
+dpmm_status dpmm_set_cluster_priors(dpmm_ctx* ctx, int K, const uint8_t* second);
 
 /* For the K clusters whose statistics the last dpmm_create_subclusters_labels /
  * dpmm_create_sufficient_statistics left on the device: the posterior of the cluster and
