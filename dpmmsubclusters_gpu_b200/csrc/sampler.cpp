@@ -106,9 +106,13 @@ public:
         cfg_.outlier_hyper.outlier = true;
     }
 
+    // device draws for NIW at D <= 64 and the multinomial prior; runs with an outlier cluster draw on
+    // the host (the device supports them -- dpmm_set_outlier_prior_*, dpmm_set_cluster_priors -- but
+    // whole runs were not shown to match the host draws' outcomes: their course is dominated by the
+    // reference's never-redrawn cluster 1)
     static bool device_draws(const Config& cfg, int D)
     {
-        return !cfg.host_param_draws && (cfg.prior == DPMM_PRIOR_MULTINOMIAL || D <= 64);
+        return !cfg.host_param_draws && !(cfg.outlier_mod > 0) && (cfg.prior == DPMM_PRIOR_MULTINOMIAL || D <= 64);
     }
 
     // init_model + init_first_clusters, then iterations first..first+n-1 of run_model
