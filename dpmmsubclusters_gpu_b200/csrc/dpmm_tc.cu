@@ -1684,8 +1684,12 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     const uint64_t da_l = sw128b32_mn_desc(smem_u32(smem + L::a_lo), A_GROUP / 2);
     const uint64_t db_h = sw128b32_mn_desc(smem_u32(smem + L::b_hi), B_GROUP / 2);
     const uint64_t db_l = sw128b32_mn_desc(smem_u32(smem + L::b_lo), B_GROUP / 2);
-    // operand pieces of this thread: point tid / C4 + (256 / C4) u, features 4 (tid % C4) ..
+    // operand pieces of this thread: point tid / C4 + (256 / C4) u, features 4 (tid % C4) ..; their
+    // offsets in the operands (side l's half of A, then + 1024 for side r; B) for u = 0, and the step
+    // to the next u (whole groups of 4 points)
     const int j4 = tid % C4;
+    const uint32_t a_off0 = mn32_offset(tid / C4, j4, 0, 4), b_off0 = mn32_offset(tid / C4, j4, 0, NA);
+    constexpr uint32_t A_STEP = (256 / C4) / 4 * 4 * 512, B_STEP = (256 / C4) / 4 * NA * 512;
     float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);   // its four centre coordinates (set at tile 0)
 
     // drain role: TMEM lane quarter q (accumulator rows 32 q ..), column half hc
@@ -1771,10 +1775,8 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
                     lo[e] = tf32_rna(cv[e] - hi[e]);
                     if (!live) hi[e] = lo[e] = 0.f;
                 }
-                const int side = sv == 2 ? 1 : 0;
-                const uint32_t a_c = mn32_offset(p, j4, 2 * side, 4);
-                const uint32_t a_z = mn32_offset(p, j4, 2 * (1 - side), 4);
-                const uint32_t b_o = mn32_offset(p, j4, 0, NA);
+                const uint32_t a0 = a_off0 + A_STEP * u, b_o = b_off0 + B_STEP * u;
+                const uint32_t a_c = sv == 2 ? a0 + 1024 : a0, a_z = sv == 2 ? a0 : a0 + 1024;
                 const uint4 h4 = make_uint4(__float_as_uint(hi[0]), __float_as_uint(hi[1]), __float_as_uint(hi[2]),
                                             __float_as_uint(hi[3]));
                 const uint4 l4 = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
@@ -2282,6 +2284,10 @@ __global__ void __launch_bounds__(SS_THREADS, 1) k_sub_stats_tc(
         const int gt = tid - 192;                  // 0 .. 127
         constexpr int ITEMS = SS_KT * C4 / 128;    // 16-byte pieces per thread per tile (2 or 1)
         const int j4 = gt % C4;                    // the thread's piece of every row: features 4 j4 ..
+        // offsets of its pieces in an operand buffer (side l's half of A, + 1024 for side r; B) for
+        // item 0, and the step to the next item (whole groups of 4 points)
+        const uint32_t a_off0 = mn32_offset(gt / C4, j4, 0, 4), b_off0 = mn32_offset(gt / C4, j4, 0, NA);
+        constexpr uint32_t A_STEP = (128 / C4) / 4 * 4 * 512, B_STEP = (128 / C4) / 4 * NA * 512;
         bool ok = run;
         int drained = 0;
         float4 s4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -2311,7 +2317,6 @@ __global__ void __launch_bounds__(SS_THREADS, 1) k_sub_stats_tc(
                     const int pp = SS_KT * j + pl;
                     const int sv = sbs[pp];
                     const bool live = sv == 1 || sv == 2;
-                    const int side = sv == 2 ? 1 : 0;
                     const float4 v4 = *reinterpret_cast<const float4*>(sl + (size_t)pp * DP + 4 * j4);
                     const float cv[4] = {v4.x - s4.x, v4.y - s4.y, v4.z - s4.z, v4.w - s4.w};
                     float hi[4], lo[4];
@@ -2321,9 +2326,8 @@ __global__ void __launch_bounds__(SS_THREADS, 1) k_sub_stats_tc(
                         lo[e] = tf32_rna(cv[e] - hi[e]);
                         if (!live) hi[e] = lo[e] = 0.f;
                     }
-                    const uint32_t a_c = mn32_offset(pl, j4, 2 * side, 4);
-                    const uint32_t a_z = mn32_offset(pl, j4, 2 * (1 - side), 4);
-                    const uint32_t b_o = mn32_offset(pl, j4, 0, NA);
+                    const uint32_t a0 = a_off0 + A_STEP * it, b_o = b_off0 + B_STEP * it;
+                    const uint32_t a_c = sv == 2 ? a0 + 1024 : a0, a_z = sv == 2 ? a0 : a0 + 1024;
                     const uint4 h4 = make_uint4(__float_as_uint(hi[0]), __float_as_uint(hi[1]), __float_as_uint(hi[2]),
                                                 __float_as_uint(hi[3]));
                     const uint4 l4 = make_uint4(__float_as_uint(lo[0]), __float_as_uint(lo[1]), __float_as_uint(lo[2]),
