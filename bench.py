@@ -68,7 +68,7 @@ def peaks():
 NCU_TRAFFIC = {
     "k_gauss_labels_tc": {"dram_bytes": 619413504, "points": 1_000_000, "clusters": 95},
     "k_prune_scan1_tc": {"dram_bytes": 270950144, "points": 1_000_000},
-    "k_slot_stats_tc": {"dram_bytes": 290109952, "points": 1_000_000},
+    "k_slot_stats_tc": {"dram_bytes": 288693760, "points": 1_000_000},
     "k_mult_labels_tc": {"dram_bytes": 417898240, "points": 200_000},
 }
 
