@@ -26,6 +26,11 @@ constexpr int kChunkMax = 4096;
 // Pruned label phase: at most kMaxKForPrune clusters; a chunk keeps at most kPrMaxCand other
 // clusters before it is evaluated against every cluster.
 constexpr int kMaxKForPrune = 256;
+// Pruned label phase against the tensor-core dense phase (N = 1e7, D = 64 on the B200): the scan alone
+// costs about as much as the dense phase at 7 clusters, and a kept cluster per point about as much as
+// 30 clusters of the dense phase.
+constexpr int kMinKForPruneTc = 8;
+constexpr double kPruneTcRatio = 30.0;
 constexpr int kPrMaxCand = 16;
 
 // Learned split/merge screen (dpmm_screen.cu): 32 features per candidate, a 32 -> 64 -> 64 -> 1 MLP

@@ -754,7 +754,7 @@ __global__ void __launch_bounds__(kPrTh) k_prune_draw(const float* __restrict__ 
 static size_t prune_draw_smem(int DP, int K) { return sizeof(float) * ((size_t)DP * DP + DP + (size_t)K * kPrTh); }
 
 template <int DP>
-static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float* d_u, bool* used)
+static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float* d_u, bool tc_dense, bool* used)
 {
     DPMM_TRY(build_permutation(c, K));
     k_prune_prep<DP><<<K, kPrTh, 0, c->stream>>>(c->d_Wt, c->d_mu, K, c->d_prune_lam, c->d_prune_M, c->d_prune_V,
@@ -794,9 +794,13 @@ static dpmm_status launch_pruned_dp(dpmm_ctx* c, int K, int final_, const float*
     const double extra = (double)h[0] / (double)c->N;   // kept other clusters per point
     c->prune_last_extra = extra;
     c->prune_last_over = (int64_t)h[1];
-    // each kept cluster costs about one more exact r per point; beyond 2 per point the dense phase
-    // (tensor cores where available) is the cheaper one: run it, and wait before the next attempt
-    if (extra > 2.0 || *outside != 0) {
+    // each kept cluster costs about one more exact r per point (FP32, in k_prune_draw).  Against the
+    // SIMT dense phase that is the cheaper path up to about 2 per point; the tensor-core dense phase
+    // costs about 1/30 of a kept cluster per point and cluster (N = 1e7, D = 64 on the B200: 0.21 ms
+    // per cluster against 3-6 ms per kept cluster per point), so there the limit is K / 30.  Beyond
+    // it run the dense phase, and wait before the next attempt
+    const double limit = tc_dense ? (double)K / kPruneTcRatio : 2.0;
+    if (extra > limit || *outside != 0) {
         c->prune_wait = 2;
         return DPMM_OK;
     }
@@ -829,17 +833,20 @@ dpmm_status launch_cluster_labels_pruned(dpmm_ctx* c, int K, int final_, const f
     *used = false;
     if (c->prior != DPMM_PRIOR_GAUSSIAN || c->Dp > 64 || c->prune_margin <= 0 || K < 2 || K > kMaxKForPrune)
         return DPMM_OK;
+    // below kMinKForPruneTc clusters the tensor-core dense phase costs less than the scan alone
+    const bool tc_dense = c->ll_mode != DPMM_LL_FP32 && tc_supported(c, K);
+    if (tc_dense && K < kMinKForPruneTc) return DPMM_OK;
     if (prune_draw_smem(c->Dp, K) > 220 * 1024) return DPMM_OK;
     if (c->prune_wait > 0) {
         --c->prune_wait;
         return DPMM_OK;
     }
     switch (c->Dp) {
-        case 4: return launch_pruned_dp<4>(c, K, final_, d_u, used);
-        case 8: return launch_pruned_dp<8>(c, K, final_, d_u, used);
-        case 16: return launch_pruned_dp<16>(c, K, final_, d_u, used);
-        case 32: return launch_pruned_dp<32>(c, K, final_, d_u, used);
-        default: return launch_pruned_dp<64>(c, K, final_, d_u, used);
+        case 4: return launch_pruned_dp<4>(c, K, final_, d_u, tc_dense, used);
+        case 8: return launch_pruned_dp<8>(c, K, final_, d_u, tc_dense, used);
+        case 16: return launch_pruned_dp<16>(c, K, final_, d_u, tc_dense, used);
+        case 32: return launch_pruned_dp<32>(c, K, final_, d_u, tc_dense, used);
+        default: return launch_pruned_dp<64>(c, K, final_, d_u, tc_dense, used);
     }
 }
 

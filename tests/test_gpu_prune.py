@@ -74,6 +74,31 @@ def test_pruned_labels_equal_dense_labels(D, mode):
                      final=True)
 
 
+def test_dense_phase_chosen_where_it_costs_less():
+    # tensor-core dense phase (D = 64): no attempt below 8 clusters (the scan alone costs more).  At 12
+    # heavily overlapping clusters the points keep most other clusters, far more than 12 / 30 per
+    # point, so the attempt falls back to the dense phase.  Labels equal the dense phase's either way.
+    N, D = 60000, 64
+    for K, spread, tried, used in ((4, 6.0, 0, 0), (12, 0.3, 1, 0)):
+        x, z, mus, covs, rng = _mixture(29 + K, N, D, K, spread)
+        kern = CudaKernel(prior_type.Gaussian, k_max=16).init(N, x.T, seed=1)
+        kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
+                                 np.array([np.linalg.slogdet(c)[1] for c in covs]), np.full(K, 1.0 / K))
+        u = uniforms(2 * N, 11)
+        lab = {}
+        for margin in (30.0, 0.0):
+            check(lib().dpmm_set_label_pruning(kern.ctx, margin))
+            kern.set_labels((z + 1).astype(np.int32))
+            kern.create_clusters_labels(K, False, u)
+            lab[margin] = kern.get_labels()
+        st = _stats(kern)
+        assert st[0] == tried and st[1] == used, (K, st)
+        if tried:
+            assert st[4] > K / 30.0, st
+        np.testing.assert_array_equal(lab[30.0], lab[0.0])
+        kern.release()
+
+
 def test_unprunable_state_falls_back_to_dense():
     K, N, D = 6, 30000, 8
     x, z, mus, covs, rng = _mixture(3, N, D, K, 0.5)    # overlapping clusters
@@ -92,13 +117,15 @@ def test_unprunable_state_falls_back_to_dense():
     np.testing.assert_array_equal(lab[30.0], lab[0.0])
 
 
-@pytest.mark.parametrize("K,N,D,planted", [(30, 200000, 8, 3000), (30, 200000, 64, 3000), (150, 150000, 32, 600),
+@pytest.mark.parametrize("K,N,D,planted", [(30, 200000, 8, 3000), (60, 200000, 64, 1500), (150, 150000, 32, 600),
                                            (200, 200000, 32, 500)])
 def test_chunk_over_capacity_is_evaluated_against_every_cluster(K, N, D, planted):
     # separated clusters; points drawn from all of them carry label 1, so the chunk(s) of cluster 0
     # keep more than 16 clusters: those points get every cluster, the rest stay pruned.  At D = 32 / 64
     # the scan runs on the tensor cores: in one pass up to 193 clusters (150: two B tiles), in two
-    # passes above (200: the chunk bound first, then more than 128 candidates in two tiles).
+    # passes above (200: the chunk bound first, then more than 128 candidates in two tiles).  With the
+    # tensor-core dense phase the pruned one is kept while fewer than K / 30 other clusters per point
+    # are kept: cluster 1's chunks (all of them over capacity) hold under N / 30 points.
     x, z, mus, covs, rng = _mixture(17, N, D, K, 8.0)
     kern = CudaKernel(prior_type.Gaussian, k_max=K + 2).init(N, x.T, seed=1)
     kern.set_gaussian_params(mus, np.array([np.linalg.inv(c) for c in covs]),
