@@ -231,7 +231,7 @@ struct dpmm_ctx {
     double* h_pinned = nullptr;    // pinned staging for D2H of results
     size_t h_pinned_bytes = 0;
 
-    int stall_tc_mma = 0;          // test seam (dpmm_set_wait_test): tensor-core label kernels issue no products
+    int stall_tc_mma = 0;          // test seam (dpmm_set_wait_test): tensor-core kernels issue no products
     int fuse_sub_stats = 0;        // sub-labels and statistics in one pass (dpmm_set_fused_sub_stats)
 
     // sharding by points (dpmm_set_shard): the aggregates are summed over the ranks by `allreduce`

@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const uint8_t* __restrict__ Bsub, const float* __restrict__ bvec,
     const float* __restrict__ cvec, const float* __restrict__ lrw, RngArgs rng, int32_t* __restrict__ sub,
-    float* __restrict__ r_out, int32_t* __restrict__ err)
+    float* __restrict__ r_out, int32_t* __restrict__ err, int stall)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -770,7 +770,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !stall) {   // stall: the wait-test seam issues nothing
             tc_fence_after();
 #pragma unroll
             for (int ks = 0; ks < KD / 16; ++ks) umma_bf16(tmem_base, da_h + 2 * ks, db_h + 2 * ks, ks != 0 ? 1u : 0u);
@@ -835,7 +835,7 @@ __global__ void __launch_bounds__(256, 2) k_sub_labels_tc(
             sub[pt] = alias_draw2(el / s, er / s, u1, u2);
         }
     }
-    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    if (failed && tid == 0 && !stall) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -878,7 +878,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
     const float* __restrict__ cvec, const float* __restrict__ mu, const float* __restrict__ lam,
     const float* __restrict__ M, const float* __restrict__ V, const float* __restrict__ beta, int K, float margin,
     float* __restrict__ rh, int32_t* __restrict__ cand, unsigned long long* __restrict__ cnt,
-    int32_t* __restrict__ err)
+    int32_t* __restrict__ err, int stall)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -988,7 +988,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !stall) {   // stall: the wait-test seam issues nothing
             tc_fence_after();
             for (int nb = 0; nb < nbt; ++nb) {
                 const uint8_t* bt = sB + (size_t)nb * STAGE_BYTES;
@@ -1178,7 +1178,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan_tc(
         atomicAdd(&cnt[0], (unsigned long long)n * (unsigned long long)len);
         if (n > kPrMaxCand) atomicAdd(&cnt[1], 1ull);
     }
-    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    if (failed && tid == 0 && !stall) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -1202,7 +1202,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
     const float* __restrict__ cvec, const float* __restrict__ mu, const float* __restrict__ lam,
     const float* __restrict__ M, const float* __restrict__ V, const float* __restrict__ beta, int K, float margin,
     float* __restrict__ rh, int32_t* __restrict__ cand, unsigned long long* __restrict__ cnt,
-    int32_t* __restrict__ err)
+    int32_t* __restrict__ err, int stall)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -1342,7 +1342,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         tc_fence_before();
         __syncthreads();
-        if (tid == 0) {
+        if (tid == 0 && !stall) {   // stall: the wait-test seam issues nothing
             tc_fence_after();
             for (int nb = 0; nb < nbt; ++nb) {
                 const uint8_t* bt = sB + (size_t)nb * STAGE_BYTES;
@@ -1462,7 +1462,7 @@ __global__ void __launch_bounds__(256, 2) k_prune_scan1_tc(
         atomicAdd(&cnt[0], (unsigned long long)n * (unsigned long long)len);
         if (n > kPrMaxCand) atomicAdd(&cnt[1], 1ull);
     }
-    if (failed && tid == 0) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
+    if (failed && tid == 0 && !stall) mbar_wait_bounded(bar, (phase - 1) & 1, nullptr);   // nothing in flight at dealloc
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
@@ -1595,7 +1595,7 @@ template <int DP>
 __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
     const float* __restrict__ x, const int32_t* __restrict__ perm, const int32_t* __restrict__ chunk,
     const int32_t* __restrict__ nchunks, const float* __restrict__ muv, const int32_t* __restrict__ sub,
-    double* __restrict__ part, const uint8_t* __restrict__ mask, int32_t* __restrict__ err)
+    double* __restrict__ part, const uint8_t* __restrict__ mask, int32_t* __restrict__ err, int stall)
 {
     using L = StatSmem<DP>;
     constexpr int N = L::N, NA = L::NA, SX = L::SX;
@@ -1794,7 +1794,7 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
         tc_fence_before();
         __syncthreads();
         const int grp = t / ST_G;
-        if (tid == 0) {
+        if (tid == 0 && !stall) {   // stall: the wait-test seam issues nothing
             tc_fence_after();
             const uint32_t td = tmem_base + (uint32_t)((grp & 1) * 128);
             const uint32_t first = (t % ST_G) == 0 ? 0u : 1u;   // a fresh accumulator per group
@@ -1855,7 +1855,7 @@ __global__ void __launch_bounds__(256, 2) k_slot_stats_tc(
         }
         if (do_sum) out[(size_t)slot * SL + 1 + fi] = sacc + n * xd[fi];
     }
-    if (failed && tid == 0 && pending >= 0)   // nothing in flight at dealloc
+    if (failed && tid == 0 && pending >= 0 && !stall)   // nothing in flight at dealloc
         mbar_wait_bounded(bar, (uint32_t)(pending & 1), nullptr);
     tc_fence_before();
     __syncthreads();
@@ -2501,7 +2501,8 @@ static dpmm_status launch_sub_labels_tc_t(dpmm_ctx* c, RngArgs r, float* d_rout,
     auto kern = tc::k_sub_labels_tc<DP>;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::SubSmem::total));
     kern<<<c->max_chunks, 256, tc::SubSmem::total, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Bsub,
-                                                              c->d_b, c->d_c, c->d_lrw, r, c->d_sub, d_rout, err);
+                                                              c->d_b, c->d_c, c->d_lrw, r, c->d_sub, d_rout, err,
+                                                              c->stall_tc_mma);
     DPMM_LAUNCHED();
     return DPMM_OK;
 }
@@ -2537,7 +2538,8 @@ static dpmm_status launch_prune_scan_tc_t(dpmm_ctx* c, int K, int32_t* err)
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc::ScanSmem::total));
     kern<<<c->max_chunks, 256, tc::ScanSmem::total, c->stream>>>(
         c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_Btc, c->d_b, c->d_c, c->d_mu, c->d_prune_lam, c->d_prune_M,
-        c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand, c->d_prune_cnt, err);
+        c->d_prune_V, c->d_prune_beta, K, c->prune_margin, c->d_prune_rh, c->d_prune_cand, c->d_prune_cnt, err,
+        c->stall_tc_mma);
     DPMM_LAUNCHED();
     return DPMM_OK;
 }
@@ -2562,7 +2564,7 @@ static dpmm_status launch_slot_stats_tc_t(dpmm_ctx* c, const uint8_t* d_mask, in
     constexpr size_t sm = tc::StatSmem<DP>::total;
     DPMM_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     kern<<<c->max_chunks, 256, sm, c->stream>>>(c->d_x, c->d_perm, c->d_chunk, c->d_nchunks, c->d_mu, c->d_sub,
-                                                c->d_part, d_mask, err);
+                                                c->d_part, d_mask, err, c->stall_tc_mma);
     DPMM_LAUNCHED();
     return DPMM_OK;
 }

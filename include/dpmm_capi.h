@@ -369,8 +369,9 @@ dpmm_status dpmm_statistics_counts(dpmm_ctx* ctx, int n, const int32_t* indices,
  * (+ log w for cluster slots), mu[3K][Dp] = mu - shift, where shift is the data mean the points are
  * stored relative to.  Any output may be NULL. */
 dpmm_status dpmm_get_gaussian_params(dpmm_ctx* ctx, int K, float* wt, float* b, float* c, float* mu);
-/* Test seam (no counterpart in the reference) for the bounded device waits: with stall nonzero the
- * tensor-core label kernels (Gaussian and multinomial) issue no tensor-core products, so every wait
+/* Test seam (no counterpart in the reference) for the bounded device waits: with stall nonzero every
+ * tensor-core kernel issues no tensor-core products (the dense Gaussian and multinomial label kernels,
+ * the pruned phase's scans, the sub-label and statistics kernels and their fused pass), so every wait
  * for them runs out after its limit (2 s); the call then returns DPMM_ERR_TIMEOUT after the kernel has
  * waited for the copies it issued and freed its tensor memory, and the context stays usable. */
 dpmm_status dpmm_set_wait_test(dpmm_ctx* ctx, int32_t stall);

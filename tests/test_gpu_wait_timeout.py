@@ -1,11 +1,13 @@
 """Bounded device waits: a wait that runs out ends the kernel with an error status, not a hang.
 
-dpmm_set_wait_test makes the tensor-core label kernels issue no products, so the waits for them (the
-drain warps' and the producer's mbarrier waits, each bounded by a 2 s limit read from %globaltimer)
-run out: the call must return DPMM_ERR_TIMEOUT after about that limit, with the kernel having waited
-for the copies it issued and freed its tensor memory -- the next call on the same context, with the
-test switched off, must run and give correct labels (it allocates the same tensor memory again).
+dpmm_set_wait_test makes the tensor-core kernels issue no products, so the waits for them (the
+drain warps' and the producer's mbarrier waits of the label kernels, the single waiting thread of the
+scan, sub-label and statistics kernels, each bounded by a 2 s limit read from %globaltimer) run out:
+the call must return DPMM_ERR_TIMEOUT after about that limit, with the kernel having waited for the
+copies it issued and freed its tensor memory -- the next calls on the same context, with the test
+switched off, must run and give correct results (they allocate the same tensor memory again).
 """
+import ctypes
 import time
 
 import numpy as np
@@ -70,3 +72,80 @@ def test_multinomial_tensor_core_wait_runs_out_and_the_context_stays_usable():
     r64 = np.stack([O.mult_loglik(x, lt[k]) for k in range(K)], 1)
     assert (np.abs(r - r64) / np.maximum(x @ np.abs(lt).T, 1)).max() <= 1e-5
     ck.release()
+
+
+def _separated(seed, N, D, K):
+    rng = np.random.default_rng(seed)
+    mus = rng.normal(size=(K, D)) * 3
+    z = rng.integers(0, K, size=N)
+    x = mus[z] + rng.normal(size=(N, D))
+    inv = np.repeat(np.eye(D)[None], K, 0)
+    mu_lr = mus[:, None, :] + 0.5 * rng.normal(size=(K, 2, D))
+    params = (mus, inv, np.zeros(K), np.full(K, 1.0 / K), mu_lr, np.repeat(inv[:, None], 2, 1), np.zeros((K, 2)),
+              np.full((K, 2), 0.5))
+    return rng, x, (z + 1).astype(np.int32), params
+
+
+def _context(x, labels, params, K):
+    N = x.shape[0]
+    ck = CudaKernel(prior_type.Gaussian, loglik_mode=LL_TC_BF16X3, k_max=16).init(N, x, 1, points_major=True)
+    ck.set_gaussian_params(*params)
+    ck.set_labels(labels)
+    return ck
+
+
+def _stalled(ck, call):
+    check(lib().dpmm_set_wait_test(ck.ctx, 1))
+    t0 = time.perf_counter()
+    with pytest.raises(DpmmError) as e:
+        call()
+    dt = time.perf_counter() - t0
+    check(lib().dpmm_set_wait_test(ck.ctx, 0))
+    assert e.value.status == DPMM_ERR_TIMEOUT, e.value
+    assert 1.0 <= dt <= 60.0, dt
+    return dt
+
+
+@pytest.mark.parametrize("step", ["pruned_scan", "sub_labels", "statistics"])
+def test_block_synchronous_kernel_wait_runs_out_and_the_context_stays_usable(step):
+    # the kernels where one thread waits for the block's products (k_prune_scan1_tc, k_sub_labels_tc,
+    # k_slot_stats_tc): with the seam on the wait runs out, the call reports DPMM_ERR_TIMEOUT, and the
+    # same context then gives the results of a context that never stalled
+    N, D, K = 30000, 64, 10
+    rng, x, labels, params = _separated(5, N, D, K)
+    u = uniforms(2 * N, 6)
+    sub = rng.integers(1, 3, size=N).astype(np.int32)
+    ck = _context(x, labels, params, K)
+    fresh = _context(x, labels, params, K)
+    if step == "pruned_scan":
+        for c in (ck, fresh):
+            check(lib().dpmm_set_label_pruning(c.ctx, 30.0))
+
+        def run(c):
+            c.set_labels(labels)
+            c.create_clusters_labels(K, uniforms=u)   # no log-likelihood output: the pruned phase runs
+            return [c.get_labels()]
+    elif step == "sub_labels":
+        def run(c):
+            r = c.create_subclusters_labels(K, uniforms=u, return_loglik=True)
+            return [np.asarray(r), c.get_sub_labels()]
+    else:
+        def run(c):
+            c.set_sub_labels(sub)
+            return list(c.create_sufficient_statistics(np.arange(K)))
+    _stalled(ck, lambda: run(ck))
+    want = run(fresh)
+    for _ in range(2):
+        got = run(ck)
+        for a, b in zip(got, want):
+            np.testing.assert_array_equal(a, b)
+    if step == "pruned_scan":
+        out = (ctypes.c_double * 6)()
+        check(lib().dpmm_label_pruning_stats(ck.ctx, out))
+        assert out[1] == 2, list(out)   # both runs after the stall ran pruned
+    if step == "statistics":
+        cnt, sm, S = O.suff_stats(x, labels, sub, K)
+        np.testing.assert_array_equal(want[0], cnt)
+        np.testing.assert_allclose(want[2], S, atol=1e-6 * (np.abs(S).max() + 1), rtol=1e-6)
+    ck.release()
+    fresh.release()
