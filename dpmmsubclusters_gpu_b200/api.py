@@ -363,6 +363,31 @@ class CudaKernel:
         check(lib().dpmm_get_sub_labels_count(self.ctx, byref(l), byref(r)))
         return l.value, r.value
 
+    # -------------------------------------------------------------- matrix helpers
+    def inverse_matrix(self, A) -> np.ndarray:
+        """cudaKernel::inverse_matrix (cudaKernel.cu:1558-1598): A^-1 of a square FP64 matrix,
+        computed on the device."""
+        A = np.asfortranarray(A, np.float64)
+        n = A.shape[0]
+        if A.ndim != 2 or A.shape[1] != n:
+            raise ValueError("inverse_matrix: A must be square")
+        B = np.empty((n, n), np.float64, order="F")
+        check(lib().dpmm_inverse_matrix(self.ctx, n, _dptr(A), _dptr(B)))
+        return B
+
+    def multiplie_matrix_for_inverseWishart(self, A, B) -> np.ndarray:
+        """cudaKernel::multiplie_matrix_for_inverseWishart (cudaKernel.cu:980-1016): (A B)(A B)^T,
+        computed on the device."""
+        A = np.asfortranarray(A, np.float64)
+        B = np.asfortranarray(B, np.float64)
+        if A.ndim != 2 or B.ndim != 2 or A.shape[1] != B.shape[0]:
+            raise ValueError("multiplie_matrix_for_inverseWishart: A (m, n) and B (n, k) required")
+        m, n = A.shape
+        k = B.shape[1]
+        C = np.empty((m, m), np.float64, order="F")
+        check(lib().dpmm_multiply_for_inverse_wishart(self.ctx, m, n, k, _dptr(A), _dptr(B), _dptr(C)))
+        return C
+
     # -------------------------------------------------------------- parameters
     def set_gaussian_params(self, mu, inv_sigma, logdet_sigma, weights, mu_lr=None, inv_sigma_lr=None,
                             logdet_sigma_lr=None, lr_weights=None, factors=False):

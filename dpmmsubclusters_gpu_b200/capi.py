@@ -85,6 +85,8 @@ SIGNATURES = {
     "dpmm_get_labels": (c_int, [_CTX, _PI32]),
     "dpmm_get_sub_labels": (c_int, [_CTX, _PI32]),
     "dpmm_get_sub_labels_count": (c_int, [_CTX, _PI32, _PI32]),
+    "dpmm_inverse_matrix": (c_int, [_CTX, c_int, _PD, _PD]),
+    "dpmm_multiply_for_inverse_wishart": (c_int, [_CTX, c_int, c_int, c_int, _PD, _PD, _PD]),
     "dpmm_set_gaussian_params": (c_int, [_CTX, c_int, _PD, _PD, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dpmm_set_gaussian_factors": (c_int, [_CTX, c_int, _PD, _PD, _PD, _PD, _PD, _PD, _PD, _PD]),
     "dpmm_set_multinomial_params": (c_int, [_CTX, c_int, _PD, _PD, _PD, _PD]),

@@ -181,7 +181,7 @@ static void free_ctx(dpmm_ctx* c)
                     c->d_scr_list, c->d_scr_slots, c->d_scr_hr, c->d_stats_tmp, c->d_logw, c->d_prune_rh,
                     c->d_prune_cand, c->d_prune_lam, c->d_prune_M, c->d_prune_cnt, c->d_prune_V,
                     c->d_prune_beta, c->d_prune_list, c->d_gt, c->d_ctab, c->d_xchg, c->d_Amult, c->d_Bmult,
-                    c->d_prior2, c->d_prior_sel, c->d_cbase};
+                    c->d_prior2, c->d_prior_sel, c->d_cbase, c->d_linalg};
     for (void* p : bufs)
         if (p) cudaFree(p);
     if (c->h_pinned) cudaFreeHost(c->h_pinned);

@@ -188,6 +188,8 @@ struct dpmm_ctx {
     double* d_prior2 = nullptr;    // like d_prior
     uint8_t* d_prior_sel = nullptr;  // [k_max] 1: the cluster's slots use the second prior
     double* d_cbase = nullptr;     // [3*k_max] -log det Sigma / 2 of each slot's current parameters (NIW)
+    double* d_linalg = nullptr;    // scratch of dpmm_inverse_matrix / dpmm_multiply_for_inverse_wishart
+    size_t linalg_bytes = 0;       // (grown on demand)
     double* d_lml = nullptr;       // [3*k_max]
     double* d_split_hr = nullptr;  // [k_max]
     double* d_merge_hr = nullptr;  // [k_max*k_max]

@@ -160,6 +160,19 @@ dpmm_status dpmm_get_sub_labels(dpmm_ctx* ctx, int32_t* sub_labels);
 /* cudaKernel::get_sub_labels_count (cudaKernel.cu:1237-1257) */
 dpmm_status dpmm_get_sub_labels_count(dpmm_ctx* ctx, int32_t* l, int32_t* r);
 
+/* cudaKernel::inverse_matrix (cudaKernel.cu:1558-1598), used by niw::sample_distribution
+ * (priors/niw.cpp:61-107): B = A^-1 for an n x n FP64 matrix, 1 <= n <= 2048, host arrays in either
+ * layout (column-major in, column-major out; row-major likewise), computed on the device.  The
+ * reference inverts by Gauss-Jordan without pivoting; this uses partial pivoting (the same inverse to
+ * FP64 rounding) and returns DPMM_ERR_NUMERIC for a singular matrix or a non-finite inverse. */
+dpmm_status dpmm_inverse_matrix(dpmm_ctx* ctx, int n, const double* A, double* B);
+
+/* cudaKernel::multiplie_matrix_for_inverseWishart (cudaKernel.cu:980-1016), used by
+ * niw::sample_distribution: C = (A B)(A B)^T with A m x n, B n x k, C m x m, FP64 column-major host
+ * arrays (sizes 1 .. 2048), computed on the device (C exactly symmetric). */
+dpmm_status dpmm_multiply_for_inverse_wishart(dpmm_ctx* ctx, int m, int n, int k, const double* A,
+                                              const double* B, double* C);
+
 /* Cluster parameters for the next label / sub-label phase: the thin_cluster_params
  * broadcast (local_clusters_actions.cpp:373-382, 449-458) plus the per-cluster H2D copies
  * the reference makes inside cudaKernel_gaussian::log_likelihood_labels / _sub_labels

@@ -53,6 +53,18 @@ def test_create_validates_arguments():
     assert not h.value
 
 
+def test_matrix_helpers_validate_arguments():
+    # checked before any device call: no context, a size outside 1 .. 2048, null arrays
+    L = capi.lib()
+    a = np.eye(3)
+    P = ctypes.POINTER(ctypes.c_double)
+    pa = a.ctypes.data_as(P)
+    assert L.dpmm_inverse_matrix(None, 3, pa, pa) == 1
+    assert L.dpmm_multiply_for_inverse_wishart(None, 3, 3, 3, pa, pa, pa) == 1
+    assert L.dpmm_inverse_matrix(None, 0, pa, pa) == 1
+    assert L.dpmm_inverse_matrix(None, 4096, None, None) == 1
+
+
 @pytest.mark.skipif(HAVE_GPU, reason="checks the no-device path")
 def test_no_device_status():
     L = capi.lib()
