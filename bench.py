@@ -818,6 +818,16 @@ def run_study(args, rank, local):
         z_np = z.cpu().numpy()
         res = {}
         for arm in ("mixed", "plain"):
+            # one untimed short run first: the process's first sampler teardown carries a one-time cost
+            # of the driver (about 0.9 s on the B200) that is no part of a run
+            keep = []
+            a = argparse.Namespace(initial_clusters=1, multi_gpu="replicas")
+            rd = make_run_desc(cfg, a, arm, 5, 0, local, keep)
+            h = ctypes.c_void_p()
+            check(L.dpmm_sampler_create(ctypes.byref(rd), cfg["N"], cfg["D"], ctypes.c_void_p(x.data_ptr()), 1,
+                                        ctypes.byref(h)))
+            check(L.dpmm_sampler_step(h, 5))
+            check(L.dpmm_sampler_destroy(h))
             rows = []
             for seed in range(args.study_seeds):
                 keep = []
