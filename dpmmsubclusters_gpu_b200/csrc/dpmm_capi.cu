@@ -60,15 +60,17 @@ static dpmm_status dev_alloc(T** p, size_t count)
 }
 
 // ----------------------------------------------------------------- point conversion kernels
+// column sums of the sampled rows i0 + q * stride, q < ns: block b sums samples [b*R, (b+1)*R) for
+// every column, then atomically adds (FP64)
 template <typename T>
-__global__ void k_col_sums(const T* __restrict__ x, int64_t N, int D, double* __restrict__ out)
+__global__ void k_col_sums(const T* __restrict__ x, int64_t i0, int64_t stride, int64_t ns, int D,
+                           double* __restrict__ out)
 {
-    // block b sums rows [b*R, (b+1)*R) for every column, then atomically adds (FP64)
     const int64_t R = 4096;
-    const int64_t r0 = (int64_t)blockIdx.x * R;
+    const int64_t q0 = (int64_t)blockIdx.x * R;
     for (int d = threadIdx.x; d < D; d += blockDim.x) {
         double s = 0;
-        for (int64_t r = r0; r < min(N, r0 + R); ++r) s += (double)x[r * D + d];
+        for (int64_t q = q0; q < min(ns, q0 + R); ++q) s += (double)x[(i0 + q * stride) * D + d];
         atomicAdd(&out[d], s);
     }
 }
@@ -382,43 +384,104 @@ extern "C" dpmm_status dpmm_synchronize(dpmm_ctx* c)
 }
 
 // ----------------------------------------------------------------- points
-// Pageable host memory is copied through two pinned staging buffers: host threads fill one while
-// the copy engine drains the other (a single pageable cudaMemcpy is staged by the driver through
-// a small bounce buffer, one piece at a time).
-static cudaError_t copy_pageable_staged(void* dst, const void* src, size_t bytes, cudaStream_t st)
+
+// the shift keeps 20 significant bits of the mean: any value near the mean serves, and the rounding
+// makes it the same whatever order the sums were added in (one context or shards)
+static double round_shift(double m)
 {
-    constexpr size_t kChunk = (size_t)64 << 20;
-    void* hb[2] = {nullptr, nullptr};
+    int ex = 0;
+    std::frexp(m, &ex);
+    return m == 0.0 ? 0.0 : std::ldexp(std::nearbyint(std::ldexp(m, 20 - ex)), ex - 20);
+}
+
+// Points in pageable host memory.  The shift (Gaussian prior) is the mean of a strided sample: the
+// points whose global index is a multiple of n_total / 65536, so the shards of one data set sample
+// the same points as one context would.  Host threads then write the FP32 rows relative to it, padded
+// to Dp, straight into two pinned staging buffers that the copy engine drains into d_x in turn: half
+// the bytes of FP64 points cross PCIe, the host writes half as much, and no FP64 copy is made on the
+// device.
+constexpr int64_t kShiftSample = 65536;
+
+template <typename T>
+static dpmm_status upload_host_points_t(dpmm_ctx* c, const T* points)
+{
+    const int64_t N = c->N;
+    const int D = c->D, Dp = c->Dp;
+    const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
+    if (gauss) {
+        const int64_t stride = std::max<int64_t>(1, c->n_total / kShiftSample);
+        const int64_t i0 = (stride - c->pt_offset % stride) % stride;
+        std::vector<double> sums(D + 1, 0.0);
+        const int64_t ns = i0 < N ? (N - 1 - i0) / stride + 1 : 0;
+#pragma omp parallel
+        {
+            std::vector<double> part(D, 0.0);
+#pragma omp for schedule(static) nowait
+            for (int64_t q = 0; q < ns; ++q) {
+                const T* row = points + (size_t)(i0 + q * stride) * D;
+                for (int d = 0; d < D; ++d) part[d] += (double)row[d];
+            }
+#pragma omp critical
+            for (int d = 0; d < D; ++d) sums[d] += part[d];
+        }
+        sums[D] = (double)ns;
+        if (c->shard_world > 1) {   // the sample of the whole data set
+            DPMM_CUDA_TRY(cudaMemcpy(c->d_xchg, sums.data(), sizeof(double) * (D + 1), cudaMemcpyHostToDevice));
+            DPMM_TRY(shard_allreduce(c, c->d_xchg, D + 1));
+            DPMM_CUDA_TRY(cudaMemcpy(sums.data(), c->d_xchg, sizeof(double) * (D + 1), cudaMemcpyDeviceToHost));
+        }
+        for (int d = 0; d < D; ++d) c->shift[d] = sums[D] > 0 ? round_shift(sums[d] / sums[D]) : 0.0;
+        DPMM_CUDA_TRY(cudaMemcpy(c->d_gshift, c->shift.data(), sizeof(double) * D, cudaMemcpyHostToDevice));
+    }
+    const std::vector<double> shift = gauss ? c->shift : std::vector<double>(D, 0.0);
+    constexpr size_t kChunkBytes = (size_t)64 << 20;
+    const int64_t rows = std::max<int64_t>(1, (int64_t)(kChunkBytes / (sizeof(float) * (size_t)Dp)));
+    float* hb[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaError_t e = cudaSuccess;
     for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
-        e = cudaMallocHost(&hb[b], kChunk);
+        e = cudaMallocHost(&hb[b], sizeof(float) * (size_t)rows * Dp);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
     }
-    size_t off = 0;
-    for (int i = 0; e == cudaSuccess && off < bytes; ++i, off += kChunk) {
-        const int b = i & 1;
-        const size_t n = std::min(kChunk, bytes - off);
+    int64_t bad = 0;
+    for (int64_t r0 = 0, i = 0; e == cudaSuccess && r0 < N; r0 += rows, ++i) {
+        const int b = (int)(i & 1);
+        const int64_t n = std::min(rows, N - r0);
         if (i >= 2) e = cudaEventSynchronize(ev[b]);   // its previous copy has left the buffer
         if (e != cudaSuccess) break;
-        const char* s = static_cast<const char*>(src) + off;
-        char* d = static_cast<char*>(hb[b]);
-        constexpr int64_t kParts = 16;
-#pragma omp parallel for schedule(static)
-        for (int64_t q = 0; q < kParts; ++q) {
-            const size_t a = n * (size_t)q / kParts, z = n * (size_t)(q + 1) / kParts;
-            std::memcpy(d + a, s + a, z - a);
+        float* dst = hb[b];
+        int64_t nb = 0;
+#pragma omp parallel for schedule(static) reduction(+ : nb)
+        for (int64_t r = 0; r < n; ++r) {
+            const T* src = points + (size_t)(r0 + r) * D;
+            float* out = dst + (size_t)r * Dp;
+            for (int d = 0; d < D; ++d) {
+                const float v = (float)((double)src[d] - shift[d]);
+                nb += std::isfinite(v) ? 0 : 1;
+                out[d] = v;
+            }
+            for (int d = D; d < Dp; ++d) out[d] = 0.f;
         }
-        e = cudaMemcpyAsync(static_cast<char*>(dst) + off, hb[b], n, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaEventRecord(ev[b], st);
+        bad += nb;
+        e = cudaMemcpyAsync(c->d_x + (size_t)r0 * Dp, dst, sizeof(float) * (size_t)n * Dp, cudaMemcpyHostToDevice,
+                            c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[b], c->stream);
     }
-    const cudaError_t es = cudaStreamSynchronize(st);   // nothing reads the buffers after this
+    const cudaError_t es = cudaStreamSynchronize(c->stream);   // nothing reads the buffers after this
     if (e == cudaSuccess) e = es;
     for (int b = 0; b < 2; ++b) {
         if (ev[b]) cudaEventDestroy(ev[b]);
         if (hb[b]) cudaFreeHost(hb[b]);
     }
-    return e;
+    if (e != cudaSuccess) return cuda_status(e, "dpmm_upload_points (host staging)");
+    g_h2d_bytes += sizeof(float) * (size_t)N * Dp;
+    if (bad) return fail(DPMM_ERR_NUMERIC, "points contain NaN or Inf");
+    DPMM_TRY(pack_tc_points(c));
+    DPMM_TRY(pack_mult_tc_points(c));
+    c->points_ready = true;
+    c->perm_K = -1;
+    invalidate_stats(c);
+    return DPMM_OK;
 }
 
 template <typename T>
@@ -428,28 +491,32 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
     DPMM_CUDA_TRY(cudaSetDevice(c->device));
     const int64_t N = c->N;
     const int D = c->D;
-    T* tmp = nullptr;
-    DPMM_TRY(dev_alloc(&tmp, (size_t)N * D));
     // the points may live in pageable or pinned host memory or in device memory
-    const size_t bytes = sizeof(T) * (size_t)N * D;
     cudaPointerAttributes pa{};
     const bool attr_ok = cudaPointerGetAttributes(&pa, points) == cudaSuccess;
     cudaGetLastError();
-    cudaError_t e = attr_ok && pa.type == cudaMemoryTypeUnregistered
-                        ? copy_pageable_staged(tmp, points, bytes, c->stream)
-                        : cudaMemcpyAsync(tmp, points, bytes, cudaMemcpyDefault, c->stream);
+    if (attr_ok && pa.type == cudaMemoryTypeUnregistered) return upload_host_points_t(c, points);
+    T* tmp = nullptr;
+    DPMM_TRY(dev_alloc(&tmp, (size_t)N * D));
+    const size_t bytes = sizeof(T) * (size_t)N * D;
+    cudaError_t e = cudaMemcpyAsync(tmp, points, bytes, cudaMemcpyDefault, c->stream);
     if (attr_ok && pa.type != cudaMemoryTypeDevice) g_h2d_bytes += bytes;
     const bool gauss = c->prior == DPMM_PRIOR_GAUSSIAN;
     if (e == cudaSuccess && gauss) {
         // FP64 column means (the shift)
+        // the same strided sample as host points (upload_host_points_t)
+        const int64_t stride = std::max<int64_t>(1, c->n_total / kShiftSample);
+        const int64_t i0 = (stride - c->pt_offset % stride) % stride;
+        const int64_t ns = i0 < N ? (N - 1 - i0) / stride + 1 : 0;
         cudaMemsetAsync(c->d_gshift, 0, sizeof(double) * D, c->stream);
-        k_col_sums<T><<<(unsigned)((N + 4095) / 4096), 128, 0, c->stream>>>(tmp, N, D, c->d_gshift);
+        if (ns > 0)
+            k_col_sums<T><<<(unsigned)((ns + 4095) / 4096), 128, 0, c->stream>>>(tmp, i0, stride, ns, D, c->d_gshift);
         e = cudaStreamSynchronize(c->stream);
         if (e == cudaSuccess) {
             std::vector<double> sums(D);
             e = cudaMemcpy(sums.data(), c->d_gshift, sizeof(double) * D, cudaMemcpyDeviceToHost);
-            double n = (double)N;
-            if (e == cudaSuccess && c->shard_world > 1) {   // the mean of the whole data set
+            double n = (double)ns;
+            if (e == cudaSuccess && c->shard_world > 1) {   // the sample of the whole data set
                 sums.push_back(n);
                 e = cudaMemcpy(c->d_xchg, sums.data(), sizeof(double) * (D + 1), cudaMemcpyHostToDevice);
                 if (e == cudaSuccess) {
@@ -462,14 +529,7 @@ static dpmm_status upload_points_t(dpmm_ctx* c, const T* points)
                     n = sums[D];
                 }
             }
-            // the shift keeps 20 significant bits of the mean: any value near the mean serves, and the
-            // rounding makes it the same whatever order the sums were added in (one context or shards)
-            for (int d = 0; d < D; ++d) {
-                const double m = sums[d] / n;
-                int ex = 0;
-                std::frexp(m, &ex);
-                c->shift[d] = m == 0.0 ? 0.0 : std::ldexp(std::nearbyint(std::ldexp(m, 20 - ex)), ex - 20);
-            }
+            for (int d = 0; d < D; ++d) c->shift[d] = n > 0 ? round_shift(sums[d] / n) : 0.0;
             if (e == cudaSuccess)
                 e = cudaMemcpy(c->d_gshift, c->shift.data(), sizeof(double) * D, cudaMemcpyHostToDevice);
         }
