@@ -708,10 +708,12 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
         if (!split[i]) continue;
         idx.push_back(i);
         nidx.push_back(new_index);
-        // split_cluster_local: the new cluster takes r, cluster i keeps l
+        // split_cluster_local: the new cluster takes r, cluster i keeps l.  Every field of both is
+        // rewritten here, so the parameters move rather than copy (a D x D NIW cluster holds several
+        // D x D matrices per sub-cluster)
         Splittable& sc = clusters_[i];
-        Splittable ns = sc;
-        auto make = [&](const ClusterParams& p, Splittable& out) {   // create_splittable_from_params
+        Splittable ns;
+        auto make = [&](ClusterParams&& p, Splittable& out) {   // create_splittable_from_params
             out.l = p;
             out.r = p;
             if (!dev_) {   // (device mode: every slot is drawn on the device before the next label phase)
@@ -722,13 +724,13 @@ dpmm_status Sampler::check_and_split(bool final_, std::vector<int32_t>& all_indi
             std::vector<double> w = dirichlet({cfg_.alpha / 2, cfg_.alpha / 2});
             out.lrw[0] = w[0];
             out.lrw[1] = w[1];
-            out.c = p;
+            out.c = std::move(p);
             out.hist = fresh_hist();
             out.splittable = false;
         };
-        ClusterParams r = sc.r, l = sc.l;
-        make(r, ns);
-        make(l, sc);
+        ClusterParams r = std::move(sc.r), l = std::move(sc.l);
+        make(std::move(r), ns);
+        make(std::move(l), sc);
         ns.points_count = ns.c.stats.N;
         sc.points_count = sc.c.stats.N;
         clusters_[new_index] = std::move(ns);
@@ -834,7 +836,7 @@ dpmm_status Sampler::check_and_merge(bool final_)
         a.lrw[0] = w[0];
         a.lrw[1] = w[1];
         a.l = a.c;
-        a.r = b.c;
+        a.r = std::move(b.c);   // b is emptied below and skipped by every later candidate
         a.splittable = false;
         a.hist = fresh_hist();
         a.points_count += b.points_count;
