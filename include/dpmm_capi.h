@@ -130,7 +130,10 @@ dpmm_status dpmm_create(const dpmm_desc* desc, dpmm_ctx** out);
 dpmm_status dpmm_destroy(dpmm_ctx* ctx);
 
 /* The H2D copy of the points inside cudaKernel::init (cudaKernel.cu:622-626).
- * points: N*D values, point-major. */
+ * points: N*D values, point-major, in host (pageable or pinned) or device memory.  The device keeps
+ * them as FP32 relative to a shift (NIW prior: the mean of every (n_total / 65536)-th point by global
+ * index, rounded to 20 significant bits); pageable host points are converted on host threads, so
+ * only the FP32 rows cross PCIe.  NaN or Inf in the points gives DPMM_ERR_NUMERIC. */
 dpmm_status dpmm_upload_points(dpmm_ctx* ctx, const double* points);
 dpmm_status dpmm_upload_points_f32(dpmm_ctx* ctx, const float* points);
 /* Makes the context one shard of a data set split by points (see dpmm_shard); call it before the
