@@ -435,7 +435,8 @@ static dpmm_status upload_host_points_t(dpmm_ctx* c, const T* points)
     }
     const std::vector<double> shift = gauss ? c->shift : std::vector<double>(D, 0.0);
     constexpr size_t kChunkBytes = (size_t)64 << 20;
-    const int64_t rows = std::max<int64_t>(1, (int64_t)(kChunkBytes / (sizeof(float) * (size_t)Dp)));
+    // staging rows: 64 MB worth, or the whole data set when smaller (small data sets pin little)
+    const int64_t rows = std::min<int64_t>(N, std::max<int64_t>(1, (int64_t)(kChunkBytes / (sizeof(float) * (size_t)Dp))));
     float* hb[2] = {nullptr, nullptr};
     cudaEvent_t ev[2] = {nullptr, nullptr};
     cudaError_t e = cudaSuccess;
